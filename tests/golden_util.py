@@ -1,0 +1,21 @@
+"""Load the committed golden fixtures (made by tests/golden/make_golden.py)."""
+import glob
+import os
+
+import numpy as np
+
+from pyscfad_b200.synthetic import TriplesInputs
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+KEYS = ("mo_energy", "t1", "t2", "ovoo", "ovov", "ovvv", "fvo")
+
+
+def names():
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
+
+
+def load(name):
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    inp = TriplesInputs(*[np.ascontiguousarray(z["in_" + k]) for k in KEYS])
+    grads = {k: z["grad_" + k] for k in KEYS}
+    return inp, float(z["e"]), grads, z

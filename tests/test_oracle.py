@@ -1,0 +1,82 @@
+"""The CPU oracle, pinned against the reference's own C kernels.
+
+Golden fixtures come from the reference library compiled unchanged from
+pyscfadlib/pyscfadlib/vjp/cc/*.c (tests/golden/make_golden.py).  Tolerances
+are FP64 summation-order level.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from pyscfad_b200.synthetic import make_inputs
+from tests import golden_util as G
+
+
+def _relerr(a, b):
+    # exact cancellations (nocc == 1 gives E = 0) leave ~1e-22 rounding noise
+    scale = max(np.abs(b).max(), 1e-7)
+    return np.abs(a - b).max() / scale
+
+
+@pytest.mark.parametrize("name", G.names())
+def test_oracle_matches_reference_golden(name):
+    inp, e_ref, g_ref, _ = G.load(name)
+    e, g = O.oracle_energy_vjp(inp, ybar=1.0)
+    assert abs(e - e_ref) <= 1e-12 * max(1.0, abs(e_ref))
+    for k in G.KEYS:
+        if np.abs(g_ref[k]).max() == 0:
+            assert np.abs(g[k]).max() < 1e-14
+        else:
+            assert _relerr(g[k], g_ref[k]) < 1e-11, k
+
+
+@pytest.mark.parametrize("name", ["o3v4_fvo", "o4v9_fvo", "o6v2"])
+def test_numpy_restatement_matches_golden(name):
+    inp, e_ref, _, _ = G.load(name)
+    assert abs(O.np_energy(inp) - e_ref) <= 1e-12 * max(1.0, abs(e_ref))
+
+
+@pytest.mark.parametrize("name", G.names())
+def test_packed_ovvv_cotangent_fold(name):
+    _, _, g_ref, z = G.load(name)
+    assert np.allclose(O.fold_ovvv_tril(g_ref["ovvv"]), z["cot_ovvv_tril"], rtol=0, atol=1e-15)
+
+
+def test_reference_library_reproduces_golden():
+    if not O.ref_available():
+        pytest.skip("reference library not built on this machine")
+    inp, e_ref, g_ref, _ = G.load("o4v9_fvo")
+    e, g = O.ref_energy_vjp(inp)
+    assert abs(e - e_ref) < 1e-13
+    for k in G.KEYS:
+        assert _relerr(g[k], g_ref[k]) < 1e-12
+
+
+def test_slices_sum_to_total():
+    inp, e_ref, g_ref, _ = G.load("o5v19_fvo")
+    parts = [O.oracle_energy_vjp(inp, a0=a0, a1=a1) for a0, a1 in [(0, 7), (7, 15), (15, 19)]]
+    assert abs(sum(p[0] for p in parts) - e_ref) < 1e-12 * abs(e_ref)
+    for k in G.KEYS:
+        tot = sum(p[1][k] for p in parts)
+        assert _relerr(tot, g_ref[k]) < 1e-11
+
+
+def test_oracle_gradient_central_differences():
+    """Central FD (h=1e-4, relative) on a few entries of every input."""
+    inp = make_inputs(4, 7, 24, seed=11, fvo_sigma=1e-3)
+    _, g = O.oracle_energy_vjp(inp)
+    rng = np.random.default_rng(0)
+    for k in G.KEYS:
+        arr = getattr(inp, k)
+        flat = arr.reshape(-1)
+        for idx in rng.choice(flat.size, size=3, replace=False):
+            x0 = flat[idx]
+            h = 1e-4 * max(abs(x0), 1e-2)
+            flat[idx] = x0 + h
+            ep, _ = O.oracle_energy_vjp(inp, want_grad=False)
+            flat[idx] = x0 - h
+            em, _ = O.oracle_energy_vjp(inp, want_grad=False)
+            flat[idx] = x0
+            fd = (ep - em) / (2 * h)
+            an = g[k].reshape(-1)[idx]
+            assert abs(fd - an) <= 1e-6 * max(abs(an), np.abs(g[k]).max() * 1e-3), (k, idx, fd, an)

@@ -1,0 +1,105 @@
+/*
+ * pyscfad_b200 -- C ABI of the B200 (sm_100a) CCSD(T) perturbative-triples
+ * energy and its adjoint.
+ *
+ * Every entry point takes plain device pointers, sizes and a cudaStream_t
+ * (passed as void*), allocates nothing itself unless stated, never
+ * synchronises the stream, and returns a triples_status (0 = success).
+ *
+ * Array layouts are the reference's canonical ones (C order, FP64), i.e. the
+ * leaves of pyscfad's ERI pytree and the CCSD amplitudes:
+ *   mo_energy[n]          n = nocc + nvir      (eris.mo_energy)
+ *   t1[o,v], t2[o,o,v,v]                       (mycc.t1, mycc.t2)
+ *   ovoo[o,v,o,o]                              (eris.ovoo)
+ *   ovov[o,v,o,v]                              (eris.ovov)
+ *   ovvv[o,v,v(v+1)/2]  when ovvv_packed != 0  (eris.ovvv of DF ERIs,
+ *                                               pyscfad/cc/dfccsd.py:88)
+ *   ovvv[o,v,v,v]       when ovvv_packed == 0
+ *   fvo[v,o]            = fock[o:,:o]          (pyscfad/cc/ccsd_t.py:93)
+ *
+ * Reference interfaces replaced (pyscfadlib, ctypes-bound through
+ * pyscfadlib/pyscfadlib/lib.py:3-12):
+ *   - the forward, pyscf.cc.ccsd_t.kernel called at pyscfad/cc/ccsd_t.py:41
+ *     (and lnoccsdt_contract, pyscfadlib/pyscfadlib/vjp/cc/lno_ccsd_t.c:96-100,
+ *     with mat = identity);
+ *   - the adjoint, ccsd_t_energy_vjp
+ *     (pyscfadlib/pyscfadlib/vjp/cc/ccsd_t_vjp.c:332-346) together with the
+ *     host-side preparation and fold of _ccsd_t_energy_vjp
+ *     (pyscfad/cc/ccsd_t.py:82-192).
+ */
+#ifndef PYSCFAD_B200_H
+#define PYSCFAD_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum triples_status {
+    TRIPLES_OK = 0,
+    TRIPLES_ERR_INVALID_ARGUMENT = 1,  /* bad size, null pointer, bad enum */
+    TRIPLES_ERR_WORKSPACE = 2,         /* workspace smaller than triples_workspace_size() */
+    TRIPLES_ERR_CUDA = 3,              /* a CUDA call failed; see triples_last_cuda_error() */
+    TRIPLES_ERR_UNSUPPORTED = 4,       /* precision / device not supported */
+    TRIPLES_ERR_DEVICE_TIMEOUT = 5     /* a bounded device-side wait gave up */
+};
+
+enum triples_precision {
+    TRIPLES_PRECISION_FP64 = 0,   /* all contractions in FP64 */
+    TRIPLES_PRECISION_MIXED = 1   /* tcgen05 split-operand contractions, FP32 accumulate;
+                                     FP64 denominators and energy sums */
+};
+
+/* Bytes of device workspace the calls below need for this problem.
+ * want_grad = 0 sizes triples_energy, 1 sizes triples_energy_vjp. */
+size_t triples_workspace_size(int precision, int nocc, int nvir, int ovvv_packed,
+                              int want_grad);
+
+/* E(T) into *e_out (device FP64 scalar).
+ * Replaces the forward of pyscfad/cc/ccsd_t.py:37-42 (pyscf's ccsd_t.kernel). */
+int triples_energy(void *stream, int precision, int nocc, int nvir, int ovvv_packed,
+                   const double *mo_energy, const double *t1, const double *t2,
+                   const double *ovoo, const double *ovov, const double *ovvv,
+                   const double *fvo,
+                   void *workspace, size_t workspace_bytes,
+                   double *e_out);
+
+/* E(T) and its vector-Jacobian product for adjoint seed ybar.
+ * Gradient outputs are OVERWRITTEN (the reference accumulates into
+ * caller-zeroed buffers, ccsd_t.py:89-106; the result is the same).
+ * Each gradient has the layout of its input; ovvv_bar is packed
+ * [o,v,v(v+1)/2] exactly as pyscfad/cc/ccsd_t.py:184-191 folds it when
+ * ovvv_packed != 0, and the unsymmetrised [o,v,v,v] gradient otherwise.
+ * fvo_bar is the vo block of fock_bar (ccsd_t.py:181-182).
+ * Replaces ccsd_t_energy_vjp (pyscfadlib/pyscfadlib/vjp/cc/ccsd_t_vjp.c:332)
+ * plus _ccsd_t_energy_vjp's blocking and fold (pyscfad/cc/ccsd_t.py:82-192). */
+int triples_energy_vjp(void *stream, int precision, int nocc, int nvir, int ovvv_packed,
+                       const double *mo_energy, const double *t1, const double *t2,
+                       const double *ovoo, const double *ovov, const double *ovvv,
+                       const double *fvo, double ybar,
+                       void *workspace, size_t workspace_bytes,
+                       double *e_out,
+                       double *mo_energy_bar, double *t1_bar, double *t2_bar,
+                       double *ovoo_bar, double *ovov_bar, double *ovvv_bar,
+                       double *fvo_bar);
+
+/* Human-readable text for a triples_status value. */
+const char *triples_status_string(int status);
+
+/* The cudaError_t of the most recent failing CUDA call on this thread. */
+int triples_last_cuda_error(void);
+
+/* Tuning: virtual block size of the chunk decomposition (0 = default 16;
+ * clamped to [1,16] and to nocc*Tv <= 1024).  Affects workspace size and
+ * performance, not results beyond FP64 summation order. */
+void triples_set_block_size(int tv);
+
+/* Version of this library, e.g. "0.1.0". */
+const char *triples_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PYSCFAD_B200_H */

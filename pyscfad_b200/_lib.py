@@ -1,0 +1,62 @@
+"""ctypes binding of the C ABI in include/pyscfad_b200.h.
+
+The CUDA library is mandatory: there is no CPU fallback.  Loading fails
+loudly if pyscfad_b200/libpyscfad_b200.so is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpyscfad_b200.so")
+
+PRECISION = {"fp64": 0, "mixed": 1}
+STATUS_OK = 0
+
+_lib = None
+
+_c_int, _c_size, _c_double, _vp = ctypes.c_int, ctypes.c_size_t, ctypes.c_double, ctypes.c_void_p
+
+
+class TriplesError(RuntimeError):
+    """A C-ABI entry point returned a non-zero triples_status."""
+
+    def __init__(self, status: int, where: str):
+        lib = load()
+        msg = lib.triples_status_string(status).decode()
+        if status == 3:
+            msg += f" (cudaError {lib.triples_last_cuda_error()})"
+        super().__init__(f"{where}: {msg}")
+        self.status = status
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -m pyscfad_b200.build` "
+            "(the (T) path has no CPU fallback)")
+    lib = ctypes.CDLL(LIB_PATH)
+    lib.triples_workspace_size.restype = _c_size
+    lib.triples_workspace_size.argtypes = [_c_int] * 5
+    lib.triples_energy.restype = _c_int
+    lib.triples_energy.argtypes = [_vp, _c_int, _c_int, _c_int, _c_int] + [_vp] * 7 + [_vp, _c_size, _vp]
+    lib.triples_energy_vjp.restype = _c_int
+    lib.triples_energy_vjp.argtypes = ([_vp, _c_int, _c_int, _c_int, _c_int] + [_vp] * 7 +
+                                       [_c_double, _vp, _c_size, _vp] + [_vp] * 7)
+    lib.triples_status_string.restype = ctypes.c_char_p
+    lib.triples_status_string.argtypes = [_c_int]
+    lib.triples_last_cuda_error.restype = _c_int
+    lib.triples_version.restype = ctypes.c_char_p
+    lib.triples_set_block_size.restype = None
+    lib.triples_set_block_size.argtypes = [_c_int]
+    _lib = lib
+    return lib
+
+
+def check(status: int, where: str):
+    if status != STATUS_OK:
+        raise TriplesError(status, where)

@@ -1,0 +1,164 @@
+// FP64 SIMT GEMM tile with multi-index operand maps.  This is the "plain FP64
+// GPU form" of the (T) contractions: the same chunked algorithm as the
+// tensor-core path, computed with DFMA.
+//
+//   C(m,n) = alpha * [ sum_k A(m,k) B(n,k) + alpha2 * sum_k A2(m,k) B2(n,k) ]
+//            (+ C(m,n) when accumulate)
+//   A(m,k) = A.p[apply(A.mn, m) + apply(A.k, k)], likewise B, A2, B2, C.
+//
+// 128x128 output tile, 256 threads, 8x8 outputs per thread, K tiles of 8,
+// register-staged double buffering.
+#pragma once
+#include "common.cuh"
+
+namespace tb {
+
+struct GOp {
+    const double *p;
+    Map4 mn;
+    Map4 k;
+    int kfast;  // 1: operand contiguous along k -> load along k
+};
+
+struct GemmArgs {
+    int M, N, K, K2;
+    GOp A, B, A2, B2;
+    double *C;
+    Map4 cm, cn;
+    double alpha, alpha2;
+    int accumulate;
+};
+
+constexpr int kGBM = 128, kGBN = 128, kGBK = 8;
+
+struct GemmSmem {
+    double As[2][kGBK][kGBM + 1];
+    double Bs[2][kGBK][kGBN + 1];
+    long long rowA[kGBM], rowB[kGBN], rowA2[kGBM], rowB2[kGBN];
+};
+
+__device__ __forceinline__ void gemm_load_tile(const GOp &op, const long long *rows, int K, int k0,
+                                               int tid, double scale, double (&r)[4]) {
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        int e = tid + 256 * i;
+        int ml, kl;
+        if (op.kfast) {
+            kl = e & 7;
+            ml = e >> 3;
+        } else {
+            ml = e & 127;
+            kl = e >> 7;
+        }
+        int k = k0 + kl;
+        long long ro = rows[ml];
+        double val = 0.0;
+        if (ro >= 0 && k < K) val = op.p[ro + apply(op.k, k)] * scale;
+        r[i] = val;
+    }
+}
+
+__device__ __forceinline__ void gemm_store_tile(double (*S)[kGBM + 1], int kfast, int tid,
+                                                const double (&r)[4]) {
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        int e = tid + 256 * i;
+        int ml, kl;
+        if (kfast) {
+            kl = e & 7;
+            ml = e >> 3;
+        } else {
+            ml = e & 127;
+            kl = e >> 7;
+        }
+        S[kl][ml] = r[i];
+    }
+}
+
+__device__ void gemm_fp64_tile(const GemmArgs &g, int m0, int n0, GemmSmem &sm) {
+    const int tid = threadIdx.x;
+    const int tx = tid & 15, ty = tid >> 4;
+    if (tid < 128) {
+        int m = m0 + tid;
+        bool ok = m < g.M;
+        sm.rowA[tid] = ok ? apply(g.A.mn, m) : -1;
+        sm.rowA2[tid] = (ok && g.K2 > 0) ? apply(g.A2.mn, m) : -1;
+    } else {
+        int t = tid - 128;
+        int n = n0 + t;
+        bool ok = n < g.N;
+        sm.rowB[t] = ok ? apply(g.B.mn, n) : -1;
+        sm.rowB2[t] = (ok && g.K2 > 0) ? apply(g.B2.mn, n) : -1;
+    }
+    __syncthreads();
+
+    double acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[i][j] = 0.0;
+
+    const int kt1 = (g.K + kGBK - 1) / kGBK;
+    const int kt2 = (g.K2 > 0) ? (g.K2 + kGBK - 1) / kGBK : 0;
+    const int kt_total = kt1 + kt2;
+    double ra[4], rb[4];
+
+    auto load = [&](int kt) {
+        if (kt < kt1) {
+            gemm_load_tile(g.A, sm.rowA, g.K, kt * kGBK, tid, 1.0, ra);
+            gemm_load_tile(g.B, sm.rowB, g.K, kt * kGBK, tid, 1.0, rb);
+        } else {
+            int k0 = (kt - kt1) * kGBK;
+            gemm_load_tile(g.A2, sm.rowA2, g.K2, k0, tid, g.alpha2, ra);
+            gemm_load_tile(g.B2, sm.rowB2, g.K2, k0, tid, 1.0, rb);
+        }
+    };
+    auto kfA = [&](int kt) { return kt < kt1 ? g.A.kfast : g.A2.kfast; };
+    auto kfB = [&](int kt) { return kt < kt1 ? g.B.kfast : g.B2.kfast; };
+
+    if (kt_total > 0) {
+        load(0);
+        gemm_store_tile(sm.As[0], kfA(0), tid, ra);
+        gemm_store_tile(sm.Bs[0], kfB(0), tid, rb);
+    }
+    __syncthreads();
+    for (int kt = 0; kt < kt_total; kt++) {
+        const int buf = kt & 1;
+        if (kt + 1 < kt_total) load(kt + 1);
+#pragma unroll
+        for (int kk = 0; kk < kGBK; kk++) {
+            double a[8], b[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++) a[i] = sm.As[buf][kk][ty + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 8; j++) b[j] = sm.Bs[buf][kk][tx + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 8; i++)
+#pragma unroll
+                for (int j = 0; j < 8; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        }
+        if (kt + 1 < kt_total) {
+            gemm_store_tile(sm.As[buf ^ 1], kfA(kt + 1), tid, ra);
+            gemm_store_tile(sm.Bs[buf ^ 1], kfB(kt + 1), tid, rb);
+        }
+        __syncthreads();
+    }
+
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        int m = m0 + ty + 16 * i;
+        if (m >= g.M) continue;
+        long long cmo = apply(g.cm, m);
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            int n = n0 + tx + 16 * j;
+            if (n >= g.N) continue;
+            long long off = cmo + apply(g.cn, n);
+            double val = g.alpha * acc[i][j];
+            if (g.accumulate) val += g.C[off];
+            g.C[off] = val;
+        }
+    }
+}
+
+}  // namespace tb

@@ -1,0 +1,965 @@
+// (T) energy and adjoint on B200: planner, layout kernels, chunk epilogue,
+// FP64 contraction drivers and the C ABI (include/pyscfad_b200.h).
+//
+// Reference path replaced: pyscfad/cc/ccsd_t.py:28-192 (forward through
+// pyscf's ccsd_t.kernel, backward through ccsd_t_energy_vjp,
+// pyscfadlib/pyscfadlib/vjp/cc/ccsd_t_vjp.c:332-497).
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "gemm_fp64.cuh"
+#include "pyscfad_b200.h"
+#include "triples_internal.h"
+
+namespace tb {
+
+static thread_local int g_last_cuda_error = 0;
+static int g_tv_override = 0;
+
+#define TB_CUDA(call)                                     \
+    do {                                                  \
+        cudaError_t _e = (call);                          \
+        if (_e != cudaSuccess) {                          \
+            g_last_cuda_error = (int)_e;                  \
+            return TRIPLES_ERR_CUDA;                      \
+        }                                                 \
+    } while (0)
+
+#define TB_LAUNCH_CHECK() TB_CUDA(cudaGetLastError())
+
+// ---------------------------------------------------------------------------
+// planning
+// ---------------------------------------------------------------------------
+static int choose_tv(int o, int v) {
+    int tv = g_tv_override > 0 ? g_tv_override : 16;
+    if (tv > kMaxTv) tv = kMaxTv;
+    if (tv * o > kMaxCols) tv = kMaxCols / o;
+    return tv < v ? tv : v;
+}
+
+static inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static void make_chunk(const Dims &d, int A, int B, int C, ChunkDesc &ch) {
+    const int blks[3] = {A, B, C};
+    auto bsize = [&](int b) { int lo = b * d.Tv; int hi = lo + d.Tv; if (hi > d.v) hi = d.v; return hi - lo; };
+    for (int t = 0; t < 3; t++) {
+        ch.blk[t] = blks[t];
+        ch.nabc[t] = bsize(blks[t]);
+        ch.base[t] = blks[t] * d.Tv;
+    }
+    ch.nperm = 0;
+    long long off = 0;
+    const long long o3 = (long long)d.o * d.o * d.o;
+    for (int s = 0; s < 6; s++) {
+        int ps[3];
+        perm_of(s, ps);
+        int bx = blks[ps[0]], by = blks[ps[1]], bz = blks[ps[2]];
+        bool dup = false;
+        for (int t = 0; t < ch.nperm; t++)
+            if (ch.pb[t].bx == bx && ch.pb[t].by == by && ch.pb[t].bz == bz) dup = true;
+        if (dup) continue;
+        PermBlock &pb = ch.pb[ch.nperm++];
+        pb.bx = bx; pb.by = by; pb.bz = bz;
+        pb.X0 = bx * d.Tv; pb.Tx = bsize(bx);
+        pb.Y0 = by * d.Tv; pb.Ty = bsize(by);
+        pb.Z0 = bz * d.Tv; pb.Tz = bsize(bz);
+        pb.soff = off;
+        off += o3 * pb.Tx * pb.Ty * pb.Tz;
+    }
+}
+
+static long long chunk_stage_elems(const ChunkDesc &ch, const Dims &d) {
+    long long o3 = (long long)d.o * d.o * d.o, s = 0;
+    for (int t = 0; t < ch.nperm; t++) s += o3 * ch.pb[t].Tx * ch.pb[t].Ty * ch.pb[t].Tz;
+    return s;
+}
+
+int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan &P) {
+    if (nocc < 1 || nvir < 1 || nocc > kMaxCols || nvir > 32767) return TRIPLES_ERR_INVALID_ARGUMENT;
+    if (precision != TRIPLES_PRECISION_FP64 && precision != TRIPLES_PRECISION_MIXED)
+        return TRIPLES_ERR_INVALID_ARGUMENT;
+    P = Plan{};
+    P.prec = precision;
+    P.want_grad = want_grad ? 1 : 0;
+    P.packed = packed ? 1 : 0;
+    Dims &d = P.d;
+    d.o = nocc;
+    d.v = nvir;
+    d.n = nocc + nvir;
+    d.Tv = choose_tv(nocc, nvir);
+    d.Kp = nvir;
+    P.nb = (nvir + d.Tv - 1) / d.Tv;
+    P.n_ijk = nocc * (nocc + 1) * (nocc + 2) / 6;
+    long long maxst = 0;
+    int maxitems = 0;
+    for (int A = 0; A < P.nb; A++)
+        for (int B = 0; B <= A; B++)
+            for (int C = 0; C <= B; C++) {
+                ChunkDesc ch;
+                make_chunk(d, A, B, C, ch);
+                long long s = chunk_stage_elems(ch, d);
+                if (s > maxst) maxst = s;
+                int it = ch.nabc[0] * ch.nabc[1] * ch.nabc[2];
+                if (it > maxitems) maxitems = it;
+            }
+    P.stage_elems = (size_t)maxst;
+    P.max_items = maxitems;
+    P.f2_gy = (maxitems + kF2Threads - 1) / kF2Threads;
+
+    const size_t o = nocc, v = nvir, Kp = d.Kp;
+    const size_t el = sizeof(double);
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t at = off; off = align256(off + bytes); return at; };
+    P.off_A1 = take(v * o * v * Kp * el);
+    P.off_B1 = take(o * o * v * Kp * el);
+    P.off_A2 = take(o * o * v * o * el);
+    P.off_B2 = take(v * o * v * o * el);
+    P.off_S = take(P.stage_elems * el);
+    if (want_grad) {
+        P.off_SV = take(P.stage_elems * el);
+        P.off_GA1 = take(v * o * v * Kp * el);
+        P.off_GB1 = take(o * o * v * Kp * el);
+        P.off_GA2 = take(o * o * v * o * el);
+        P.off_GB2 = take(v * o * v * o * el);
+    }
+    P.off_ijk = take((size_t)P.n_ijk * 3 * sizeof(int));
+    P.off_epart = take((size_t)P.n_ijk * P.f2_gy * el);
+    P.off_eacc = take(2 * el);
+    P.off_counter = take(sizeof(unsigned));
+    P.total = off;
+    return TRIPLES_OK;
+}
+
+// ---------------------------------------------------------------------------
+// layout kernels
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ long long tri_index(int f, int y) {
+    return f >= y ? (long long)f * (f + 1) / 2 + y : (long long)y * (y + 1) / 2 + f;
+}
+
+// A1[y][p][x][f] = ovvv[p,x,f,y]  (packed: unpacked symmetric [f,y] block)
+__global__ void k_prep_A1(const double *__restrict__ ovvv, int packed, Dims d,
+                          double *__restrict__ A1) {
+    __shared__ double tile[32][33];
+    const long long px = blockIdx.z;  // p*v + x
+    const int f0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+    const long long npair = (long long)d.v * (d.v + 1) / 2;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        int f = f0 + r, y = y0 + threadIdx.x;
+        double val = 0.0;
+        if (f < d.v && y < d.v)
+            val = packed ? ovvv[px * npair + tri_index(f, y)] : ovvv[(px * d.v + f) * d.v + y];
+        tile[r][threadIdx.x] = val;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        int y = y0 + r, f = f0 + threadIdx.x;
+        if (y < d.v && f < d.Kp)
+            A1[((long long)y * d.o * d.v + px) * d.Kp + f] = tile[threadIdx.x][r];
+    }
+}
+
+// B1[q][r][z][f] = t2[r,q,z,f]
+__global__ void k_prep_B1(const double *__restrict__ t2, Dims d, double *__restrict__ B1) {
+    const long long row = blockIdx.x;  // (q*o + r)*v + z
+    const int z = row % d.v;
+    const int qr = row / d.v;
+    const int r = qr % d.o, q = qr / d.o;
+    const double *src = t2 + (((long long)r * d.o + q) * d.v + z) * d.v;
+    for (int f = threadIdx.x; f < d.Kp; f += blockDim.x)
+        B1[row * d.Kp + f] = f < d.v ? src[f] : 0.0;
+}
+
+// A2[q][p][x][m] = ovoo[p,x,m,q]
+__global__ void k_prep_A2(const double *__restrict__ ovoo, Dims d, double *__restrict__ A2) {
+    const long long total = (long long)d.o * d.o * d.v * d.o;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        int m = e % d.o;
+        long long t = e / d.o;
+        int x = t % d.v;
+        t /= d.v;
+        int p = t % d.o;
+        int q = t / d.o;
+        A2[e] = ovoo[(((long long)p * d.v + x) * d.o + m) * d.o + q];
+    }
+}
+
+// B2[y][r][z][m] = t2[r,m,z,y]
+__global__ void k_prep_B2(const double *__restrict__ t2, Dims d, double *__restrict__ B2) {
+    const long long total = (long long)d.v * d.o * d.v * d.o;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        int m = e % d.o;
+        long long t = e / d.o;
+        int z = t % d.v;
+        t /= d.v;
+        int r = t % d.o;
+        int y = t / d.o;
+        B2[e] = t2[(((long long)r * d.o + m) * d.v + z) * d.v + y];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// FP64 contraction kernels (one GEMM problem per blockIdx.z)
+// ---------------------------------------------------------------------------
+struct GemmLaunch {
+    Dims d;
+    ChunkDesc ch;
+    int cum[7];      // prefix sums used to decode blockIdx.z
+    int tau_only;    // >= 0: restrict to this ordering
+    const double *A1, *B1, *A2, *B2;
+    double *S, *G;   // staging, gradient target
+};
+
+__device__ __forceinline__ int find_tau(const GemmLaunch &L, int b) {
+    int t = 0;
+    while (t + 1 < L.ch.nperm && b >= L.cum[t + 1]) t++;
+    return t;
+}
+
+// F1: S_tau[p][q][y][x][r][z] = W for all (tau, y, q)
+__global__ void __launch_bounds__(256) k_f1_fp64(GemmLaunch L) {
+    __shared__ GemmSmem sm;
+    const int b = blockIdx.z;
+    const int t = find_tau(L, b);
+    const PermBlock &pb = L.ch.pb[t];
+    const Dims &d = L.d;
+    const int o = d.o, v = d.v, Kp = d.Kp;
+    const int rem = b - L.cum[t];
+    const int y = rem / o, q = rem % o;
+    const long long yg = pb.Y0 + y;
+    const long long oTz = (long long)o * pb.Tz;
+    GemmArgs g;
+    g.M = o * pb.Tx;
+    g.N = o * pb.Tz;
+    g.K = v;
+    g.K2 = o;
+    g.A = GOp{L.A1 + (yg * o * v + pb.X0) * Kp, map2(pb.Tx, Kp, (long long)v * Kp), map1(1), 1};
+    g.B = GOp{L.B1 + ((long long)q * o * v + pb.Z0) * Kp, map2(pb.Tz, Kp, (long long)v * Kp), map1(1), 1};
+    g.A2 = GOp{L.A2 + ((long long)q * o * v + pb.X0) * o, map2(pb.Tx, o, (long long)v * o), map1(1), 1};
+    g.B2 = GOp{L.B2 + (yg * o * v + pb.Z0) * o, map2(pb.Tz, o, (long long)v * o), map1(1), 1};
+    g.C = L.S + pb.soff + (long long)q * pb.Ty * pb.Tx * oTz + (long long)y * pb.Tx * oTz;
+    g.cm = map2(pb.Tx, oTz, (long long)o * pb.Ty * pb.Tx * oTz);
+    g.cn = map1(1);
+    g.alpha = 1.0;
+    g.alpha2 = -1.0;
+    g.accumulate = 0;
+    const int m0 = blockIdx.x * kGBM, n0 = blockIdx.y * kGBN;
+    if (m0 >= g.M || n0 >= g.N) return;
+    gemm_fp64_tile(g, m0, n0, sm);
+}
+
+// ovvv gradient: G_A1[y][p][x][f] += sum_{q,r,z} Wbar * B1[q][r][z][f]; z = (tau, y)
+__global__ void __launch_bounds__(256) k_b1a_fp64(GemmLaunch L) {
+    __shared__ GemmSmem sm;
+    const int b = blockIdx.z;
+    const int t = find_tau(L, b);
+    const PermBlock &pb = L.ch.pb[t];
+    const Dims &d = L.d;
+    const int o = d.o, v = d.v, Kp = d.Kp;
+    const int y = b - L.cum[t];
+    const long long oTz = (long long)o * pb.Tz;
+    const long long sq = (long long)pb.Ty * pb.Tx * oTz;   // stride of q in S
+    GemmArgs g;
+    g.M = o * pb.Tx;
+    g.N = v;
+    g.K = o * o * pb.Tz;
+    g.K2 = 0;
+    g.A = GOp{L.S + pb.soff + (long long)y * pb.Tx * oTz, map2(pb.Tx, oTz, (long long)o * sq),
+              map2((int)oTz, 1, sq), 1};
+    g.B = GOp{L.B1 + (long long)pb.Z0 * Kp, map1(1),
+              map3(pb.Tz, o, Kp, (long long)v * Kp, (long long)o * v * Kp), 0};
+    g.C = L.G + (((long long)pb.Y0 + y) * o * v + pb.X0) * Kp;
+    g.cm = map2(pb.Tx, Kp, (long long)v * Kp);
+    g.cn = map1(1);
+    g.alpha = 1.0;
+    g.alpha2 = 0.0;
+    g.accumulate = 1;
+    const int m0 = blockIdx.x * kGBM, n0 = blockIdx.y * kGBN;
+    if (m0 >= g.M || n0 >= g.N) return;
+    gemm_fp64_tile(g, m0, n0, sm);
+}
+
+// t2 gradient (ovvv term): G_B1[q][r][z][f] += sum_{y,p,x} Wbar * A1[y][p][x][f]; z = q
+__global__ void __launch_bounds__(256) k_b1b_fp64(GemmLaunch L) {
+    __shared__ GemmSmem sm;
+    const int q = blockIdx.z;
+    const PermBlock &pb = L.ch.pb[L.tau_only];
+    const Dims &d = L.d;
+    const int o = d.o, v = d.v, Kp = d.Kp;
+    const long long oTz = (long long)o * pb.Tz;
+    const long long sq = (long long)pb.Ty * pb.Tx * oTz;
+    GemmArgs g;
+    g.M = o * pb.Tz;
+    g.N = v;
+    g.K = pb.Ty * o * pb.Tx;
+    g.K2 = 0;
+    g.A = GOp{L.S + pb.soff + (long long)q * sq, map1(1),
+              map3(pb.Tx, o, oTz, (long long)o * sq, (long long)pb.Tx * oTz), 0};
+    g.B = GOp{L.A1 + ((long long)pb.Y0 * o * v + pb.X0) * Kp, map1(1),
+              map3(pb.Tx, o, Kp, (long long)v * Kp, (long long)o * v * Kp), 0};
+    g.C = L.G + ((long long)q * o * v + pb.Z0) * Kp;
+    g.cm = map2(pb.Tz, Kp, (long long)v * Kp);
+    g.cn = map1(1);
+    g.alpha = 1.0;
+    g.alpha2 = 0.0;
+    g.accumulate = 1;
+    const int m0 = blockIdx.x * kGBM, n0 = blockIdx.y * kGBN;
+    if (m0 >= g.M || n0 >= g.N) return;
+    gemm_fp64_tile(g, m0, n0, sm);
+}
+
+// ovoo gradient: G_A2[q][p][x][m] -= sum_{y,r,z} Wbar * B2[y][r][z][m]; z = q
+__global__ void __launch_bounds__(256) k_b1c_fp64(GemmLaunch L) {
+    __shared__ GemmSmem sm;
+    const int q = blockIdx.z;
+    const PermBlock &pb = L.ch.pb[L.tau_only];
+    const Dims &d = L.d;
+    const int o = d.o, v = d.v;
+    const long long oTz = (long long)o * pb.Tz;
+    const long long sq = (long long)pb.Ty * pb.Tx * oTz;
+    GemmArgs g;
+    g.M = o * pb.Tx;
+    g.N = o;
+    g.K = pb.Ty * o * pb.Tz;
+    g.K2 = 0;
+    g.A = GOp{L.S + pb.soff + (long long)q * sq, map2(pb.Tx, oTz, (long long)o * sq),
+              map2((int)oTz, 1, (long long)pb.Tx * oTz), 1};
+    g.B = GOp{L.B2 + ((long long)pb.Y0 * o * v + pb.Z0) * o, map1(1),
+              map3(pb.Tz, o, o, (long long)v * o, (long long)o * v * o), 0};
+    g.C = L.G + ((long long)q * o * v + pb.X0) * o;
+    g.cm = map2(pb.Tx, o, (long long)v * o);
+    g.cn = map1(1);
+    g.alpha = -1.0;
+    g.alpha2 = 0.0;
+    g.accumulate = 1;
+    const int m0 = blockIdx.x * kGBM, n0 = blockIdx.y * kGBN;
+    if (m0 >= g.M || n0 >= g.N) return;
+    gemm_fp64_tile(g, m0, n0, sm);
+}
+
+// t2 gradient (ooov term): G_B2[y][r][z][m] -= sum_{q,p,x} Wbar * A2[q][p][x][m]; z = (tau, y)
+__global__ void __launch_bounds__(256) k_b1d_fp64(GemmLaunch L) {
+    __shared__ GemmSmem sm;
+    const int b = blockIdx.z;
+    const int t = find_tau(L, b);
+    const PermBlock &pb = L.ch.pb[t];
+    const Dims &d = L.d;
+    const int o = d.o, v = d.v;
+    const int y = b - L.cum[t];
+    const long long oTz = (long long)o * pb.Tz;
+    const long long sq = (long long)pb.Ty * pb.Tx * oTz;
+    GemmArgs g;
+    g.M = o * pb.Tz;
+    g.N = o;
+    g.K = o * o * pb.Tx;
+    g.K2 = 0;
+    g.A = GOp{L.S + pb.soff + (long long)y * pb.Tx * oTz, map1(1),
+              map3(pb.Tx, o, oTz, (long long)o * sq, sq), 0};
+    g.B = GOp{L.A2 + (long long)pb.X0 * o, map1(1),
+              map3(pb.Tx, o, o, (long long)v * o, (long long)o * v * o), 0};
+    g.C = L.G + (((long long)pb.Y0 + y) * o * v + pb.Z0) * o;
+    g.cm = map2(pb.Tz, o, (long long)v * o);
+    g.cn = map1(1);
+    g.alpha = -1.0;
+    g.alpha2 = 0.0;
+    g.accumulate = 1;
+    const int m0 = blockIdx.x * kGBM, n0 = blockIdx.y * kGBN;
+    if (m0 >= g.M || n0 >= g.N) return;
+    gemm_fp64_tile(g, m0, n0, sm);
+}
+
+// ---------------------------------------------------------------------------
+// chunk epilogue: energy, adjoint of the raw amplitudes, mo_energy gradient
+// ---------------------------------------------------------------------------
+template <typename StageT>
+struct F2Params {
+    Dims d;
+    ChunkDesc ch;
+    const int *ijk;
+    const double *mo_e, *t1, *t2, *ovov, *fvo;
+    StageT *S;    // raw W in, Wbar out (in place)
+    StageT *SV;   // Vbar out
+    double ybar;
+    int want_grad;
+    double *e_part, *e_acc;
+    unsigned *counter;
+    double *mo_bar;
+};
+
+template <typename StageT>
+__device__ __forceinline__ long long stage_pos(const F2Params<StageT> &P, int p, int q, int r,
+                                               int x, int y, int z) {
+    const int Tv = P.d.Tv, o = P.d.o;
+    const int bx = x / Tv, by = y / Tv, bz = z / Tv;
+    int t = 0;
+#pragma unroll 1
+    for (; t < P.ch.nperm - 1; t++)
+        if (P.ch.pb[t].bx == bx && P.ch.pb[t].by == by && P.ch.pb[t].bz == bz) break;
+    const PermBlock &pb = P.ch.pb[t];
+    return pb.soff +
+           ((((long long)(p * o + q) * pb.Ty + (y - pb.Y0)) * pb.Tx + (x - pb.X0)) * o + r) * pb.Tz +
+           (z - pb.Z0);
+}
+
+template <typename StageT>
+__global__ void __launch_bounds__(kF2Threads) k_f2(F2Params<StageT> P) {
+    const Dims &d = P.d;
+    const int o = d.o, v = d.v;
+    __shared__ double s_evir[3 * kMaxTv];
+    __shared__ double s_red[2][kF2Threads / 32];
+    for (int e = threadIdx.x; e < 3 * kMaxTv; e += blockDim.x) s_evir[e] = 0.0;
+    __syncthreads();
+
+    const int rep = blockIdx.x;
+    const int ijk[3] = {P.ijk[3 * rep], P.ijk[3 * rep + 1], P.ijk[3 * rep + 2]};
+    const int nA = P.ch.nabc[0], nB = P.ch.nabc[1], nC = P.ch.nabc[2];
+    const int it = blockIdx.y * blockDim.x + threadIdx.x;
+    double e_loc = 0.0, dd_loc = 0.0;
+
+    int la = 0, lb = 0, lc = 0;
+    bool valid = it < nA * nB * nC;
+    if (valid) {
+        la = it / (nB * nC);
+        lb = (it / nC) % nB;
+        lc = it % nC;
+    }
+    const int abc[3] = {P.ch.base[0] + la, P.ch.base[1] + lb, P.ch.base[2] + lc};
+    if (valid && P.ch.blk[0] == P.ch.blk[1] && abc[0] < abc[1]) valid = false;
+    if (valid && P.ch.blk[1] == P.ch.blk[2] && abc[1] < abc[2]) valid = false;
+
+    if (valid) {
+        double WW[6], VV[6], X[6];
+#pragma unroll
+        for (int s = 0; s < 6; s++) {
+            int ps[3];
+            perm_of(s, ps);
+            const int dd[3] = {abc[ps[0]], abc[ps[1]], abc[ps[2]]};
+            double sw = 0.0, sv = 0.0;
+#pragma unroll
+            for (int tau = 0; tau < 6; tau++) {
+                int pt[3];
+                perm_of(tau, pt);
+                const int p = ijk[pt[0]], q = ijk[pt[1]], r = ijk[pt[2]];
+                const int x = dd[pt[0]], y = dd[pt[1]], z = dd[pt[2]];
+                sw += (double)P.S[stage_pos(P, p, q, r, x, y, z)];
+                sv += P.ovov[(((long long)p * v + x) * o + q) * v + y] * P.t1[(long long)r * v + z] +
+                      P.t2[(((long long)q * o + p) * v + y) * v + x] * P.fvo[(long long)z * o + r];
+            }
+            WW[s] = sw;
+            VV[s] = sv;
+            X[s] = sw + 0.5 * sv;
+        }
+        double Z[6], RW[6];
+#pragma unroll
+        for (int s = 0; s < 6; s++) {
+            Z[s] = 4.0 * X[s] + X[perm_compose(s, 4)] + X[perm_compose(s, 3)] -
+                   2.0 * (X[perm_compose(s, 5)] + X[perm_compose(s, 1)] + X[perm_compose(s, 2)]);
+            RW[s] = 4.0 * WW[s] + WW[perm_compose(s, 4)] + WW[perm_compose(s, 3)] -
+                    2.0 * (WW[perm_compose(s, 5)] + WW[perm_compose(s, 1)] + WW[perm_compose(s, 2)]);
+        }
+        const int i = ijk[0], j = ijk[1], k = ijk[2];
+        const int a = abc[0], b = abc[1], c = abc[2];
+        const int n_ijk = (i == k) ? 1 : ((i == j || j == k) ? 3 : 6);
+        const int n_abc = (a == c) ? 1 : ((a == b || b == c) ? 3 : 6);
+        const double cfac = (double)(n_ijk * n_abc) / 18.0;
+        const double Dn = P.mo_e[i] + P.mo_e[j] + P.mo_e[k] - P.mo_e[o + a] - P.mo_e[o + b] -
+                          P.mo_e[o + c];
+        const double rD = 1.0 / Dn;
+        double esum = 0.0;
+#pragma unroll
+        for (int s = 0; s < 6; s++) esum += WW[s] * Z[s];
+        e_loc = cfac * esum * rD;
+        if (P.want_grad) {
+            const double g0 = P.ybar * cfac * rD;
+            double gW[6], gV[6];
+#pragma unroll
+            for (int s = 0; s < 6; s++) {
+                gW[s] = g0 * (Z[s] + RW[s]);
+                gV[s] = g0 * 0.5 * RW[s];
+            }
+            const double dD = -P.ybar * cfac * esum * rD * rD;
+            dd_loc = dD;
+            // zero all raw positions of this orbit, then accumulate (duplicates
+            // occur when indices coincide)
+#pragma unroll 1
+            for (int pass = 0; pass < 2; pass++) {
+#pragma unroll
+                for (int s = 0; s < 6; s++) {
+                    int ps[3];
+                    perm_of(s, ps);
+                    const int dd[3] = {abc[ps[0]], abc[ps[1]], abc[ps[2]]};
+#pragma unroll
+                    for (int tau = 0; tau < 6; tau++) {
+                        int pt[3];
+                        perm_of(tau, pt);
+                        long long pos = stage_pos(P, ijk[pt[0]], ijk[pt[1]], ijk[pt[2]], dd[pt[0]],
+                                                  dd[pt[1]], dd[pt[2]]);
+                        if (pass == 0) {
+                            P.S[pos] = (StageT)0;
+                            P.SV[pos] = (StageT)0;
+                        } else {
+                            P.S[pos] = (StageT)((double)P.S[pos] + gW[s]);
+                            P.SV[pos] = (StageT)((double)P.SV[pos] + gV[s]);
+                        }
+                    }
+                }
+            }
+            // virtual part of the mo_energy gradient
+            for (int t = 0; t < 3; t++) {
+                int slot = (P.ch.blk[t] == P.ch.blk[0]) ? 0 : ((P.ch.blk[t] == P.ch.blk[1]) ? 1 : 2);
+                atomicAdd(&s_evir[slot * kMaxTv + (abc[t] - P.ch.base[slot])], -dD);
+            }
+        }
+    }
+
+    // block reductions
+    for (int off = 16; off > 0; off >>= 1) {
+        e_loc += __shfl_down_sync(0xffffffffu, e_loc, off);
+        dd_loc += __shfl_down_sync(0xffffffffu, dd_loc, off);
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        s_red[0][warp] = e_loc;
+        s_red[1][warp] = dd_loc;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double es = 0.0, ds = 0.0;
+        for (int w = 0; w < kF2Threads / 32; w++) {
+            es += s_red[0][w];
+            ds += s_red[1][w];
+        }
+        P.e_part[blockIdx.y * gridDim.x + blockIdx.x] = es;
+        if (P.want_grad && ds != 0.0) {
+            atomicAdd(&P.mo_bar[ijk[0]], ds);
+            atomicAdd(&P.mo_bar[ijk[1]], ds);
+            atomicAdd(&P.mo_bar[ijk[2]], ds);
+        }
+    }
+    if (P.want_grad) {
+        for (int e = threadIdx.x; e < 3 * kMaxTv; e += blockDim.x) {
+            int slot = e / kMaxTv, l = e % kMaxTv;
+            if (l < P.ch.nabc[slot] && s_evir[e] != 0.0) {
+                bool dup = (slot == 1 && P.ch.blk[1] == P.ch.blk[0]) ||
+                           (slot == 2 && (P.ch.blk[2] == P.ch.blk[0] || P.ch.blk[2] == P.ch.blk[1]));
+                if (!dup) atomicAdd(&P.mo_bar[o + P.ch.base[slot] + l], s_evir[e]);
+            }
+        }
+    }
+    // deterministic chunk energy: the last block sums the block partials in order
+    __shared__ bool s_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned prev = atomicAdd(P.counter, 1u);
+        s_last = (prev == gridDim.x * gridDim.y - 1);
+    }
+    __syncthreads();
+    if (s_last && threadIdx.x == 0) {
+        __threadfence();
+        double tot = 0.0;
+        const int nblk = gridDim.x * gridDim.y;
+        for (int bidx = 0; bidx < nblk; bidx++) tot += ((volatile double *)P.e_part)[bidx];
+        P.e_acc[0] += tot;
+        *P.counter = 0u;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// V-term gradients from Vbar: ovov, t2 (row dots), t1, fvo (column sums)
+// ---------------------------------------------------------------------------
+template <typename StageT>
+struct VGParams {
+    Dims d;
+    ChunkDesc ch;
+    const StageT *SV;
+    const double *t1, *fvo, *ovov, *t2;
+    double *ovov_bar, *t2_bar, *t1_bar, *fvo_bar;
+};
+
+template <typename StageT>
+__global__ void __launch_bounds__(256) k_vgrad(VGParams<StageT> P) {
+    const Dims &d = P.d;
+    const int o = d.o, v = d.v;
+    const PermBlock &pb = P.ch.pb[blockIdx.y];
+    const int ncol = o * pb.Tz;
+    const long long nrow = (long long)o * o * pb.Ty * pb.Tx;
+    const long long row0 = (long long)blockIdx.x * kVgRows;
+    if (row0 >= nrow) return;
+    __shared__ double s_c1[kMaxCols], s_c2[kMaxCols];
+    for (int c = threadIdx.x; c < ncol; c += blockDim.x) {
+        s_c1[c] = 0.0;
+        s_c2[c] = 0.0;
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double c1[kMaxCols / 32], c2[kMaxCols / 32];
+#pragma unroll
+    for (int c = 0; c < kMaxCols / 32; c++) {
+        c1[c] = 0.0;
+        c2[c] = 0.0;
+    }
+    long long row_end = row0 + kVgRows;
+    if (row_end > nrow) row_end = nrow;
+    for (long long row = row0 + warp; row < row_end; row += 8) {
+        const int x = row % pb.Tx;
+        const int y = (row / pb.Tx) % pb.Ty;
+        const long long pq = row / ((long long)pb.Tx * pb.Ty);
+        const int q = pq % o, p = pq / o;
+        const int xg = pb.X0 + x, yg = pb.Y0 + y;
+        const double wv1 = P.ovov[(((long long)p * v + xg) * o + q) * v + yg];
+        const double wv2 = P.t2[(((long long)q * o + p) * v + yg) * v + xg];
+        const StageT *src = P.SV + pb.soff + row * ncol;
+        double dot1 = 0.0, dot2 = 0.0;
+#pragma unroll
+        for (int c = 0; c < kMaxCols / 32; c++) {
+            const int col = lane + 32 * c;
+            if (col < ncol) {
+                const int r = col / pb.Tz, z = col % pb.Tz;
+                const double val = (double)src[col];
+                dot1 += val * P.t1[(long long)r * v + pb.Z0 + z];
+                dot2 += val * P.fvo[(long long)(pb.Z0 + z) * o + r];
+                c1[c] += val * wv1;
+                c2[c] += val * wv2;
+            }
+        }
+        for (int off = 16; off > 0; off >>= 1) {
+            dot1 += __shfl_down_sync(0xffffffffu, dot1, off);
+            dot2 += __shfl_down_sync(0xffffffffu, dot2, off);
+        }
+        if (lane == 0) {
+            P.ovov_bar[(((long long)p * v + xg) * o + q) * v + yg] += dot1;
+            P.t2_bar[(((long long)q * o + p) * v + yg) * v + xg] += dot2;
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < kMaxCols / 32; c++) {
+        const int col = lane + 32 * c;
+        if (col < ncol) {
+            atomicAdd(&s_c1[col], c1[c]);
+            atomicAdd(&s_c2[col], c2[c]);
+        }
+    }
+    __syncthreads();
+    for (int col = threadIdx.x; col < ncol; col += blockDim.x) {
+        const int r = col / pb.Tz, z = col % pb.Tz;
+        atomicAdd(&P.t1_bar[(long long)r * v + pb.Z0 + z], s_c1[col]);
+        atomicAdd(&P.fvo_bar[(long long)(pb.Z0 + z) * o + r], s_c2[col]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// gradient fold back to the reference layouts
+// ---------------------------------------------------------------------------
+// full ovvv_bar[p,x,f,y] = G_A1[y][p][x][f]
+__global__ void k_fold_ovvv_full(const double *__restrict__ GA1, Dims d, double *__restrict__ out) {
+    __shared__ double tile[32][33];
+    const long long px = blockIdx.z;
+    const int y0 = blockIdx.x * 32, f0 = blockIdx.y * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        int y = y0 + r, f = f0 + threadIdx.x;
+        tile[r][threadIdx.x] = (y < d.v && f < d.v) ? GA1[((long long)y * d.o * d.v + px) * d.Kp + f] : 0.0;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        int f = f0 + r, y = y0 + threadIdx.x;
+        if (f < d.v && y < d.v) out[(px * d.v + f) * d.v + y] = tile[threadIdx.x][r];
+    }
+}
+
+// packed ovvv_bar[p,x,tri(f,y)] = G[f,y] + G[y,f] (f != y), G[f,f]; G[f,y] = G_A1[y][p][x][f]
+// (pyscfad/cc/ccsd_t.py:184-191)
+__global__ void k_fold_ovvv_packed(const double *__restrict__ GA1, Dims d, double *__restrict__ out) {
+    const long long npair = (long long)d.v * (d.v + 1) / 2;
+    const long long total = (long long)d.o * d.v * npair;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long px = e / npair;
+        const long long ij = e % npair;
+        int f = (int)((sqrt(8.0 * (double)ij + 1.0) - 1.0) * 0.5);
+        while ((long long)f * (f + 1) / 2 > ij) f--;
+        while ((long long)(f + 1) * (f + 2) / 2 <= ij) f++;
+        const int y = (int)(ij - (long long)f * (f + 1) / 2);
+        const long long sy = (long long)d.o * d.v * d.Kp;
+        double val = GA1[y * sy + px * d.Kp + f];
+        if (f != y) val += GA1[(long long)f * sy + px * d.Kp + y];
+        out[e] = val;
+    }
+}
+
+// t2_bar[r,q,z,f] += G_B1[q][r][z][f] + G_B2[f][r][z][q]
+__global__ void k_fold_t2(const double *__restrict__ GB1, const double *__restrict__ GB2, Dims d,
+                          double *__restrict__ t2_bar) {
+    const long long total = (long long)d.o * d.o * d.v * d.v;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int f = e % d.v;
+        long long t = e / d.v;
+        const int z = t % d.v;
+        t /= d.v;
+        const int q = t % d.o;
+        const int r = t / d.o;
+        t2_bar[e] += GB1[(((long long)q * d.o + r) * d.v + z) * d.Kp + f] +
+                     GB2[(((long long)f * d.o + r) * d.v + z) * d.o + q];
+    }
+}
+
+// ovoo_bar[p,x,m,q] = G_A2[q][p][x][m]
+__global__ void k_fold_ovoo(const double *__restrict__ GA2, Dims d, double *__restrict__ out) {
+    const long long total = (long long)d.o * d.v * d.o * d.o;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int q = e % d.o;
+        long long t = e / d.o;
+        const int m = t % d.o;
+        t /= d.o;
+        const int x = t % d.v;
+        const int p = t / d.v;
+        out[e] = GA2[(((long long)q * d.o + p) * d.v + x) * d.o + m];
+    }
+}
+
+__global__ void k_copy_scalar(const double *src, double *dst) { dst[0] = src[0]; }
+
+// ---------------------------------------------------------------------------
+// driver
+// ---------------------------------------------------------------------------
+static inline unsigned grid1d(long long n, int threads) {
+    long long b = (n + threads - 1) / threads;
+    if (b > 148 * 64) b = 148 * 64;
+    if (b < 1) b = 1;
+    return (unsigned)b;
+}
+
+int run_triples(const Plan &P, cudaStream_t st, const TriplesIO &io) {
+    const Dims d = P.d;
+    char *ws = (char *)io.workspace;
+    double *A1 = (double *)(ws + P.off_A1);
+    double *B1 = (double *)(ws + P.off_B1);
+    double *A2 = (double *)(ws + P.off_A2);
+    double *B2 = (double *)(ws + P.off_B2);
+    double *S = (double *)(ws + P.off_S);
+    double *SV = P.want_grad ? (double *)(ws + P.off_SV) : nullptr;
+    double *GA1 = P.want_grad ? (double *)(ws + P.off_GA1) : nullptr;
+    double *GB1 = P.want_grad ? (double *)(ws + P.off_GB1) : nullptr;
+    double *GA2 = P.want_grad ? (double *)(ws + P.off_GA2) : nullptr;
+    double *GB2 = P.want_grad ? (double *)(ws + P.off_GB2) : nullptr;
+    int *ijk = (int *)(ws + P.off_ijk);
+    double *e_part = (double *)(ws + P.off_epart);
+    double *e_acc = (double *)(ws + P.off_eacc);
+    unsigned *counter = (unsigned *)(ws + P.off_counter);
+    const size_t o = d.o, v = d.v, n = d.n;
+
+    // occupied triplet representatives i >= j >= k
+    {
+        std::vector<int> h;
+        h.reserve((size_t)P.n_ijk * 3);
+        for (int i = 0; i < d.o; i++)
+            for (int j = 0; j <= i; j++)
+                for (int k = 0; k <= j; k++) {
+                    h.push_back(i);
+                    h.push_back(j);
+                    h.push_back(k);
+                }
+        TB_CUDA(cudaMemcpyAsync(ijk, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        TB_CUDA(cudaStreamSynchronize(st));  // host vector goes out of scope
+    }
+    TB_CUDA(cudaMemsetAsync(e_acc, 0, 2 * sizeof(double), st));
+    TB_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned), st));
+    if (P.want_grad) {
+        TB_CUDA(cudaMemsetAsync(GA1, 0, v * o * v * d.Kp * sizeof(double), st));
+        TB_CUDA(cudaMemsetAsync(GB1, 0, o * o * v * d.Kp * sizeof(double), st));
+        TB_CUDA(cudaMemsetAsync(GA2, 0, o * o * v * o * sizeof(double), st));
+        TB_CUDA(cudaMemsetAsync(GB2, 0, v * o * v * o * sizeof(double), st));
+        TB_CUDA(cudaMemsetAsync(io.mo_energy_bar, 0, n * sizeof(double), st));
+        TB_CUDA(cudaMemsetAsync(io.t1_bar, 0, o * v * sizeof(double), st));
+        TB_CUDA(cudaMemsetAsync(io.t2_bar, 0, o * o * v * v * sizeof(double), st));
+        TB_CUDA(cudaMemsetAsync(io.ovov_bar, 0, o * v * o * v * sizeof(double), st));
+        TB_CUDA(cudaMemsetAsync(io.fvo_bar, 0, v * o * sizeof(double), st));
+    }
+
+    // operand layouts
+    k_prep_A1<<<dim3((d.Kp + 31) / 32, (d.v + 31) / 32, (unsigned)(o * v)), dim3(32, 8), 0, st>>>(
+        io.ovvv, P.packed, d, A1);
+    TB_LAUNCH_CHECK();
+    k_prep_B1<<<(unsigned)(o * o * v), 128, 0, st>>>(io.t2, d, B1);
+    TB_LAUNCH_CHECK();
+    k_prep_A2<<<grid1d((long long)o * o * v * o, 256), 256, 0, st>>>(io.ovoo, d, A2);
+    TB_LAUNCH_CHECK();
+    k_prep_B2<<<grid1d((long long)v * o * v * o, 256), 256, 0, st>>>(io.t2, d, B2);
+    TB_LAUNCH_CHECK();
+
+    for (int A = 0; A < P.nb; A++)
+        for (int B = 0; B <= A; B++)
+            for (int C = 0; C <= B; C++) {
+                ChunkDesc ch;
+                make_chunk(d, A, B, C, ch);
+                int maxTx = 0, maxTz = 0;
+                for (int t = 0; t < ch.nperm; t++) {
+                    if (ch.pb[t].Tx > maxTx) maxTx = ch.pb[t].Tx;
+                    if (ch.pb[t].Tz > maxTz) maxTz = ch.pb[t].Tz;
+                }
+                GemmLaunch L;
+                L.d = d;
+                L.ch = ch;
+                L.tau_only = -1;
+                L.A1 = A1; L.B1 = B1; L.A2 = A2; L.B2 = B2;
+                L.S = S; L.G = nullptr;
+                // F1: raw amplitudes
+                L.cum[0] = 0;
+                for (int t = 0; t < ch.nperm; t++) L.cum[t + 1] = L.cum[t] + ch.pb[t].Ty * d.o;
+                k_f1_fp64<<<dim3((d.o * maxTx + kGBM - 1) / kGBM, (d.o * maxTz + kGBN - 1) / kGBN,
+                                 L.cum[ch.nperm]),
+                            256, 0, st>>>(L);
+                TB_LAUNCH_CHECK();
+                // F2: energy (+ adjoint of the raw amplitudes)
+                F2Params<double> F;
+                F.d = d;
+                F.ch = ch;
+                F.ijk = ijk;
+                F.mo_e = io.mo_energy; F.t1 = io.t1; F.t2 = io.t2; F.ovov = io.ovov; F.fvo = io.fvo;
+                F.S = S; F.SV = SV;
+                F.ybar = io.ybar;
+                F.want_grad = P.want_grad;
+                F.e_part = e_part; F.e_acc = e_acc; F.counter = counter;
+                F.mo_bar = io.mo_energy_bar;
+                const int items = ch.nabc[0] * ch.nabc[1] * ch.nabc[2];
+                k_f2<double><<<dim3(P.n_ijk, (items + kF2Threads - 1) / kF2Threads), kF2Threads, 0, st>>>(F);
+                TB_LAUNCH_CHECK();
+                if (!P.want_grad) continue;
+                // V-term gradients
+                VGParams<double> VG;
+                VG.d = d;
+                VG.ch = ch;
+                VG.SV = SV;
+                VG.t1 = io.t1; VG.fvo = io.fvo; VG.ovov = io.ovov; VG.t2 = io.t2;
+                VG.ovov_bar = io.ovov_bar; VG.t2_bar = io.t2_bar; VG.t1_bar = io.t1_bar;
+                VG.fvo_bar = io.fvo_bar;
+                long long maxrows = 0;
+                for (int t = 0; t < ch.nperm; t++) {
+                    long long r = (long long)d.o * d.o * ch.pb[t].Ty * ch.pb[t].Tx;
+                    if (r > maxrows) maxrows = r;
+                }
+                k_vgrad<double><<<dim3((unsigned)((maxrows + kVgRows - 1) / kVgRows), ch.nperm), 256, 0, st>>>(VG);
+                TB_LAUNCH_CHECK();
+                // W-term gradients
+                L.cum[0] = 0;
+                for (int t = 0; t < ch.nperm; t++) L.cum[t + 1] = L.cum[t] + ch.pb[t].Ty;
+                L.G = GA1;
+                k_b1a_fp64<<<dim3((d.o * maxTx + kGBM - 1) / kGBM, (d.v + kGBN - 1) / kGBN, L.cum[ch.nperm]),
+                             256, 0, st>>>(L);
+                TB_LAUNCH_CHECK();
+                L.G = GB2;
+                k_b1d_fp64<<<dim3((d.o * maxTz + kGBM - 1) / kGBM, (d.o + kGBN - 1) / kGBN, L.cum[ch.nperm]),
+                             256, 0, st>>>(L);
+                TB_LAUNCH_CHECK();
+                for (int t = 0; t < ch.nperm; t++) {
+                    L.tau_only = t;
+                    L.G = GB1;
+                    k_b1b_fp64<<<dim3((d.o * ch.pb[t].Tz + kGBM - 1) / kGBM, (d.v + kGBN - 1) / kGBN, d.o),
+                                 256, 0, st>>>(L);
+                    TB_LAUNCH_CHECK();
+                    L.G = GA2;
+                    k_b1c_fp64<<<dim3((d.o * ch.pb[t].Tx + kGBM - 1) / kGBM, (d.o + kGBN - 1) / kGBN, d.o),
+                                 256, 0, st>>>(L);
+                    TB_LAUNCH_CHECK();
+                }
+            }
+
+    if (P.want_grad) {
+        if (P.packed) {
+            k_fold_ovvv_packed<<<grid1d((long long)o * v * (v * (v + 1) / 2), 256), 256, 0, st>>>(
+                GA1, d, io.ovvv_bar);
+        } else {
+            k_fold_ovvv_full<<<dim3((d.v + 31) / 32, (d.v + 31) / 32, (unsigned)(o * v)), dim3(32, 8), 0, st>>>(
+                GA1, d, io.ovvv_bar);
+        }
+        TB_LAUNCH_CHECK();
+        k_fold_t2<<<grid1d((long long)o * o * v * v, 256), 256, 0, st>>>(GB1, GB2, d, io.t2_bar);
+        TB_LAUNCH_CHECK();
+        k_fold_ovoo<<<grid1d((long long)o * v * o * o, 256), 256, 0, st>>>(GA2, d, io.ovoo_bar);
+        TB_LAUNCH_CHECK();
+    }
+    k_copy_scalar<<<1, 1, 0, st>>>(e_acc, io.e_out);
+    TB_LAUNCH_CHECK();
+    return TRIPLES_OK;
+}
+
+void set_block_size(int tv) { g_tv_override = tv; }
+int last_cuda_error() { return g_last_cuda_error; }
+
+}  // namespace tb
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+size_t triples_workspace_size(int precision, int nocc, int nvir, int ovvv_packed, int want_grad) {
+    tb::Plan P;
+    if (tb::make_plan(precision, nocc, nvir, ovvv_packed, want_grad, P) != TRIPLES_OK) return 0;
+    return P.total;
+}
+
+static int triples_call(void *stream, int precision, int nocc, int nvir, int ovvv_packed, int want_grad,
+                        const tb::TriplesIO &io, size_t workspace_bytes) {
+    tb::Plan P;
+    int rc = tb::make_plan(precision, nocc, nvir, ovvv_packed, want_grad, P);
+    if (rc != TRIPLES_OK) return rc;
+    if (precision != TRIPLES_PRECISION_FP64) return TRIPLES_ERR_UNSUPPORTED;
+    if (!io.workspace || workspace_bytes < P.total) return TRIPLES_ERR_WORKSPACE;
+    if (!io.mo_energy || !io.t1 || !io.t2 || !io.ovoo || !io.ovov || !io.ovvv || !io.fvo || !io.e_out)
+        return TRIPLES_ERR_INVALID_ARGUMENT;
+    if (want_grad && (!io.mo_energy_bar || !io.t1_bar || !io.t2_bar || !io.ovoo_bar || !io.ovov_bar ||
+                      !io.ovvv_bar || !io.fvo_bar))
+        return TRIPLES_ERR_INVALID_ARGUMENT;
+    return tb::run_triples(P, (cudaStream_t)stream, io);
+}
+
+int triples_energy(void *stream, int precision, int nocc, int nvir, int ovvv_packed,
+                   const double *mo_energy, const double *t1, const double *t2, const double *ovoo,
+                   const double *ovov, const double *ovvv, const double *fvo, void *workspace,
+                   size_t workspace_bytes, double *e_out) {
+    tb::TriplesIO io{};
+    io.mo_energy = mo_energy; io.t1 = t1; io.t2 = t2; io.ovoo = ovoo; io.ovov = ovov;
+    io.ovvv = ovvv; io.fvo = fvo; io.ybar = 1.0; io.workspace = workspace; io.e_out = e_out;
+    return triples_call(stream, precision, nocc, nvir, ovvv_packed, 0, io, workspace_bytes);
+}
+
+int triples_energy_vjp(void *stream, int precision, int nocc, int nvir, int ovvv_packed,
+                       const double *mo_energy, const double *t1, const double *t2, const double *ovoo,
+                       const double *ovov, const double *ovvv, const double *fvo, double ybar,
+                       void *workspace, size_t workspace_bytes, double *e_out, double *mo_energy_bar,
+                       double *t1_bar, double *t2_bar, double *ovoo_bar, double *ovov_bar,
+                       double *ovvv_bar, double *fvo_bar) {
+    tb::TriplesIO io{};
+    io.mo_energy = mo_energy; io.t1 = t1; io.t2 = t2; io.ovoo = ovoo; io.ovov = ovov;
+    io.ovvv = ovvv; io.fvo = fvo; io.ybar = ybar; io.workspace = workspace; io.e_out = e_out;
+    io.mo_energy_bar = mo_energy_bar; io.t1_bar = t1_bar; io.t2_bar = t2_bar; io.ovoo_bar = ovoo_bar;
+    io.ovov_bar = ovov_bar; io.ovvv_bar = ovvv_bar; io.fvo_bar = fvo_bar;
+    return triples_call(stream, precision, nocc, nvir, ovvv_packed, 1, io, workspace_bytes);
+}
+
+const char *triples_status_string(int status) {
+    switch (status) {
+    case TRIPLES_OK: return "ok";
+    case TRIPLES_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case TRIPLES_ERR_WORKSPACE: return "workspace too small";
+    case TRIPLES_ERR_CUDA: return "CUDA error";
+    case TRIPLES_ERR_UNSUPPORTED: return "unsupported precision or device";
+    case TRIPLES_ERR_DEVICE_TIMEOUT: return "device-side wait timed out";
+    default: return "unknown status";
+    }
+}
+
+int triples_last_cuda_error(void) { return tb::last_cuda_error(); }
+
+const char *triples_version(void) { return "0.1.0"; }
+
+void triples_set_block_size(int tv) { tb::set_block_size(tv); }
+
+}  // extern "C"

@@ -1,0 +1,39 @@
+// Internal planning structures shared by the (T) drivers.
+#pragma once
+#include <cstddef>
+
+#include "common.cuh"
+
+namespace tb {
+
+constexpr int kF2Threads = 256;   // chunk-epilogue block size
+constexpr int kMaxTv = 16;        // largest virtual block
+constexpr int kMaxCols = 1024;    // largest nocc * Tv handled by the V-gradient kernel
+constexpr int kVgRows = 2048;     // staged rows per V-gradient block
+
+struct Plan {
+    Dims d;
+    int prec, want_grad, packed;
+    int nb;          // number of virtual blocks
+    int n_ijk;       // occupied triplet representatives i >= j >= k
+    int max_items;   // largest |A||B||C| over chunks
+    int f2_gy;       // epilogue grid.y upper bound
+    size_t stage_elems;
+    size_t off_A1, off_B1, off_A2, off_B2, off_S, off_SV;
+    size_t off_GA1, off_GB1, off_GA2, off_GB2;
+    size_t off_ijk, off_epart, off_eacc, off_counter;
+    size_t total;
+};
+
+struct TriplesIO {
+    const double *mo_energy, *t1, *t2, *ovoo, *ovov, *ovvv, *fvo;
+    double ybar;
+    void *workspace;
+    double *e_out;
+    double *mo_energy_bar, *t1_bar, *t2_bar, *ovoo_bar, *ovov_bar, *ovvv_bar, *fvo_bar;
+};
+
+int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan &P);
+int run_triples(const Plan &P, cudaStream_t st, const TriplesIO &io);
+
+}  // namespace tb

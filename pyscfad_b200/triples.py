@@ -1,0 +1,108 @@
+"""Device-level calls of the (T) energy and VJP on torch CUDA tensors.
+
+Inputs use the reference's canonical layouts (FP64, C order):
+mo_energy[n], t1[o,v], t2[o,o,v,v], ovoo[o,v,o,o], ovov[o,v,o,v],
+ovvv[o,v,v(v+1)/2] (packed, DF ERIs) or ovvv[o,v,v,v], fvo[v,o].
+"""
+from __future__ import annotations
+
+import torch
+
+from . import _lib
+
+KEYS = ("mo_energy", "t1", "t2", "ovoo", "ovov", "ovvv", "fvo")
+
+_workspaces: dict = {}
+
+
+def _workspace(nbytes: int, device: torch.device) -> torch.Tensor:
+    key = (device.type, device.index)
+    buf = _workspaces.get(key)
+    if buf is None or buf.numel() < nbytes:
+        _workspaces.pop(key, None)
+        buf = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=device)
+        _workspaces[key] = buf
+    return buf
+
+
+def release_workspace():
+    _workspaces.clear()
+
+
+def _as_dev(x, device) -> torch.Tensor:
+    t = torch.as_tensor(x)
+    if t.dtype != torch.float64:
+        raise TypeError(f"(T) inputs must be float64, got {t.dtype}")
+    return t.to(device=device).contiguous()
+
+
+def _shapes(t1, t2, ovoo, ovov, ovvv, fvo, mo_energy):
+    if t1.dim() != 2:
+        raise ValueError("t1 must be [nocc, nvir]")
+    o, v = t1.shape
+    packed = ovvv.dim() == 3
+    exp = {
+        "mo_energy": (o + v,), "t1": (o, v), "t2": (o, o, v, v), "ovoo": (o, v, o, o),
+        "ovov": (o, v, o, v), "fvo": (v, o),
+        "ovvv": (o, v, v * (v + 1) // 2) if packed else (o, v, v, v),
+    }
+    got = dict(mo_energy=mo_energy, t1=t1, t2=t2, ovoo=ovoo, ovov=ovov, ovvv=ovvv, fvo=fvo)
+    for k, shp in exp.items():
+        if tuple(got[k].shape) != shp:
+            raise ValueError(f"{k} has shape {tuple(got[k].shape)}, expected {shp}")
+    return o, v, packed
+
+
+def set_block_size(tv: int):
+    _lib.load().triples_set_block_size(int(tv))
+
+
+def workspace_size(nocc, nvir, packed=True, want_grad=True, precision="fp64") -> int:
+    return int(_lib.load().triples_workspace_size(_lib.PRECISION[precision], nocc, nvir,
+                                                  int(packed), int(want_grad)))
+
+
+def energy(mo_energy, t1, t2, ovoo, ovov, ovvv, fvo, precision="fp64", device=None,
+           stream=None) -> torch.Tensor:
+    """E(T) as a 0-dim FP64 tensor on the device (no host synchronisation)."""
+    lib = _lib.load()
+    device = torch.device(device or (t1.device if isinstance(t1, torch.Tensor) and t1.is_cuda else "cuda"))
+    args = [_as_dev(a, device) for a in (mo_energy, t1, t2, ovoo, ovov, ovvv, fvo)]
+    mo_energy, t1, t2, ovoo, ovov, ovvv, fvo = args
+    o, v, packed = _shapes(t1, t2, ovoo, ovov, ovvv, fvo, mo_energy)
+    prec = _lib.PRECISION[precision]
+    nbytes = lib.triples_workspace_size(prec, o, v, int(packed), 0)
+    if nbytes == 0:
+        raise _lib.TriplesError(1, "triples_workspace_size")
+    ws = _workspace(nbytes, device)
+    e = torch.zeros((), dtype=torch.float64, device=device)
+    st = stream if stream is not None else torch.cuda.current_stream(device)
+    rc = lib.triples_energy(st.cuda_stream, prec, o, v, int(packed),
+                            *[a.data_ptr() for a in args], ws.data_ptr(), ws.numel(), e.data_ptr())
+    _lib.check(rc, "triples_energy")
+    return e
+
+
+def energy_vjp(mo_energy, t1, t2, ovoo, ovov, ovvv, fvo, ybar=1.0, precision="fp64",
+               device=None, stream=None):
+    """E(T) and dE/d(inputs) * ybar.  Gradients have the input layouts; for a
+    packed ovvv the gradient is the reference's packed-tril fold
+    (pyscfad/cc/ccsd_t.py:184-191).  Returns (e, dict)."""
+    lib = _lib.load()
+    device = torch.device(device or (t1.device if isinstance(t1, torch.Tensor) and t1.is_cuda else "cuda"))
+    args = [_as_dev(a, device) for a in (mo_energy, t1, t2, ovoo, ovov, ovvv, fvo)]
+    mo_energy, t1, t2, ovoo, ovov, ovvv, fvo = args
+    o, v, packed = _shapes(t1, t2, ovoo, ovov, ovvv, fvo, mo_energy)
+    prec = _lib.PRECISION[precision]
+    nbytes = lib.triples_workspace_size(prec, o, v, int(packed), 1)
+    if nbytes == 0:
+        raise _lib.TriplesError(1, "triples_workspace_size")
+    ws = _workspace(nbytes, device)
+    e = torch.zeros((), dtype=torch.float64, device=device)
+    grads = {k: torch.empty_like(a) for k, a in zip(KEYS, args)}
+    st = stream if stream is not None else torch.cuda.current_stream(device)
+    rc = lib.triples_energy_vjp(st.cuda_stream, prec, o, v, int(packed),
+                                *[a.data_ptr() for a in args], float(ybar), ws.data_ptr(), ws.numel(),
+                                e.data_ptr(), *[grads[k].data_ptr() for k in KEYS])
+    _lib.check(rc, "triples_energy_vjp")
+    return e, grads

@@ -1,0 +1,61 @@
+"""C-ABI library: loads, exports every declared entry point, validates
+arguments on the host (no GPU needed for any of this)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from pyscfad_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared_functions():
+    names = []
+    for fn in os.listdir(os.path.join(ROOT, "include")):
+        if not fn.endswith(".h"):
+            continue
+        src = open(os.path.join(ROOT, "include", fn)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        names += re.findall(r"^[A-Za-z_][\w\s\*]*?\b(\w+)\s*\(", src, flags=re.M)
+    return sorted(set(n for n in names if n not in ("if", "defined")))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    decl = _declared_functions()
+    assert "triples_energy_vjp" in decl and "triples_energy" in decl
+    for name in decl:
+        assert hasattr(lib, name), name
+
+
+def test_workspace_size_is_host_only_and_monotone():
+    lib = _lib.load()
+    a = lib.triples_workspace_size(0, 5, 19, 1, 0)
+    b = lib.triples_workspace_size(0, 5, 19, 1, 1)
+    c = lib.triples_workspace_size(0, 40, 360, 1, 1)
+    assert 0 < a < b < c
+    assert lib.triples_workspace_size(0, 0, 19, 1, 1) == 0       # nocc < 1
+    assert lib.triples_workspace_size(7, 5, 19, 1, 1) == 0       # bad precision
+
+
+def test_invalid_arguments_rejected_before_any_cuda_call():
+    lib = _lib.load()
+    null = None
+    rc = lib.triples_energy(null, 0, 0, 19, 1, *([null] * 7), null, 0, null)
+    assert rc == 1
+    rc = lib.triples_energy(null, 9, 5, 19, 1, *([null] * 7), null, 0, null)
+    assert rc == 1
+    # workspace too small is reported as such
+    rc = lib.triples_energy(null, 0, 5, 19, 1, *([ctypes.c_void_p(16)] * 7), ctypes.c_void_p(16), 8,
+                            ctypes.c_void_p(16))
+    assert rc == 2
+
+
+def test_status_strings():
+    lib = _lib.load()
+    assert lib.triples_status_string(0) == b"ok"
+    assert b"workspace" in lib.triples_status_string(2)
+    with pytest.raises(_lib.TriplesError):
+        _lib.check(1, "probe")

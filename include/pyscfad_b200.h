@@ -46,9 +46,12 @@ enum triples_status {
 };
 
 enum triples_precision {
-    TRIPLES_PRECISION_FP64 = 0,   /* all contractions in FP64 */
-    TRIPLES_PRECISION_MIXED = 1   /* tcgen05 split-operand contractions, FP32 accumulate;
-                                     FP64 denominators and energy sums */
+    TRIPLES_PRECISION_FP64 = 0,       /* all contractions in FP64 */
+    TRIPLES_PRECISION_MIXED = 1,      /* tcgen05 contractions on fp16 hi/lo splits with
+                                         power-of-two scaling (3 products, ~22-bit
+                                         operands), FP32 accumulate; FP64 denominators
+                                         and energy sums */
+    TRIPLES_PRECISION_MIXED_BF16 = 2  /* same with unscaled bf16 hi/lo splits (~16-bit) */
 };
 
 /* Bytes of device workspace the calls below need for this problem.
@@ -83,6 +86,11 @@ int triples_energy_vjp(void *stream, int precision, int nocc, int nvir, int ovvv
                        double *mo_energy_bar, double *t1_bar, double *t2_bar,
                        double *ovoo_bar, double *ovov_bar, double *ovvv_bar,
                        double *fvo_bar);
+
+/* Synchronises `stream` and reports device-side failures of the last call
+ * that used `workspace` (bounded waits that gave up): TRIPLES_OK or
+ * TRIPLES_ERR_DEVICE_TIMEOUT. */
+int triples_check_device_status(void *stream, const void *workspace);
 
 /* Human-readable text for a triples_status value. */
 const char *triples_status_string(int status);

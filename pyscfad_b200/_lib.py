@@ -11,7 +11,7 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libpyscfad_b200.so")
 
-PRECISION = {"fp64": 0, "mixed": 1}
+PRECISION = {"fp64": 0, "mixed": 1, "mixed_bf16": 2}
 STATUS_OK = 0
 
 _lib = None
@@ -51,6 +51,8 @@ def load():
     lib.triples_status_string.argtypes = [_c_int]
     lib.triples_last_cuda_error.restype = _c_int
     lib.triples_version.restype = ctypes.c_char_p
+    lib.triples_check_device_status.restype = _c_int
+    lib.triples_check_device_status.argtypes = [_vp, _vp]
     lib.triples_set_block_size.restype = None
     lib.triples_set_block_size.argtypes = [_c_int]
     _lib = lib

@@ -13,21 +13,27 @@
 
 namespace tb {
 
-struct GOp {
-    const double *p;
+template <typename T>
+struct GOpT {
+    const T *p;
     Map4 mn;
     Map4 k;
     int kfast;  // 1: operand contiguous along k -> load along k
 };
+using GOp = GOpT<double>;
 
-struct GemmArgs {
+// TA: element type of the A operand (FP32 staging in the mixed-precision path)
+template <typename TA>
+struct GemmArgsT {
     int M, N, K, K2;
-    GOp A, B, A2, B2;
+    GOpT<TA> A;
+    GOp B, A2, B2;
     double *C;
     Map4 cm, cn;
     double alpha, alpha2;
     int accumulate;
 };
+using GemmArgs = GemmArgsT<double>;
 
 constexpr int kGBM = 128, kGBN = 128, kGBK = 8;
 
@@ -37,7 +43,8 @@ struct GemmSmem {
     long long rowA[kGBM], rowB[kGBN], rowA2[kGBM], rowB2[kGBN];
 };
 
-__device__ __forceinline__ void gemm_load_tile(const GOp &op, const long long *rows, int K, int k0,
+template <typename T>
+__device__ __forceinline__ void gemm_load_tile(const GOpT<T> &op, const long long *rows, int K, int k0,
                                                int tid, double scale, double (&r)[4]) {
 #pragma unroll
     for (int i = 0; i < 4; i++) {
@@ -53,7 +60,7 @@ __device__ __forceinline__ void gemm_load_tile(const GOp &op, const long long *r
         int k = k0 + kl;
         long long ro = rows[ml];
         double val = 0.0;
-        if (ro >= 0 && k < K) val = op.p[ro + apply(op.k, k)] * scale;
+        if (ro >= 0 && k < K) val = (double)op.p[ro + apply(op.k, k)] * scale;
         r[i] = val;
     }
 }
@@ -75,7 +82,8 @@ __device__ __forceinline__ void gemm_store_tile(double (*S)[kGBM + 1], int kfast
     }
 }
 
-__device__ void gemm_fp64_tile(const GemmArgs &g, int m0, int n0, GemmSmem &sm) {
+template <typename TA>
+__device__ void gemm_fp64_tile(const GemmArgsT<TA> &g, int m0, int n0, GemmSmem &sm) {
     const int tid = threadIdx.x;
     const int tx = tid & 15, ty = tid >> 4;
     if (tid < 128) {

@@ -1,0 +1,285 @@
+// Tensor-core (tcgen05) form of the raw-amplitude contraction F1:
+//   S_tau[p][q][y][x][r][z] = sum_f A1[y][p][x][f] B1[q][r][z][f]
+//                           + sum_m A2n[q][p][x][m] B2[y][r][z][m]
+// (A2n holds -ovoo, so the ooov term is a plain second K segment).
+//
+// Operands are 16-bit hi/lo splits of the FP64 inputs, scaled by powers of two
+// (fp16) or unscaled (bf16), stored as [h][...] so one 5-D tensor map covers
+// both halves.  Each K step issues hi*hi + hi*lo + lo*hi into one FP32 TMEM
+// accumulator.
+//
+// Tile: 128 rows = 8 p x 16 x, BN columns = BN/16 r x 16 z, K blocks of 64.
+// Persistent CTAs (one per SM), warp roles: 0 TMA producer, 1 MMA issuer and
+// TMEM owner, 2-5 epilogue (TMEM -> registers -> staging, FP32).
+#pragma once
+#include "common.cuh"
+#include "tc_ptx.cuh"
+
+namespace tb {
+
+constexpr int kTcBM = 128;
+constexpr int kTcBK = 64;
+
+template <int BN>
+struct TcCfg {
+    static constexpr int A_BYTES = kTcBM * kTcBK * 2;
+    static constexpr int B_BYTES = BN * kTcBK * 2;
+    static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+    static constexpr int STAGES = (BN >= 256) ? 2 : 3;
+    static constexpr int BAR_BYTES = 256;
+    static constexpr int SMEM = STAGES * STAGE_BYTES + BAR_BYTES + 1024;
+    static constexpr int RT = BN / 16;
+    static constexpr int TMEM_COLS = 2 * BN;
+};
+
+struct TcF1Params {
+    Dims d;
+    ChunkDesc ch;
+    int cum[7];        // prefix over orderings of tile counts
+    int mt_count;      // p tiles of 8
+    int nt_count;      // r tiles of BN/16
+    int nkb1, nkb2;    // K blocks of the ovvv and ooov terms
+    float *S;
+    const float *out_scale;   // device scalar: 1 / (scale_A * scale_B)
+    int *err;
+    int bf16;
+};
+
+struct F1Tile {
+    int tau, y, q, mt, nt;
+};
+
+__device__ __forceinline__ F1Tile f1_decode(const TcF1Params &P, int t) {
+    F1Tile T;
+    int tau = 0;
+    while (tau + 1 < P.ch.nperm && t >= P.cum[tau + 1]) tau++;
+    int rem = t - P.cum[tau];
+    T.tau = tau;
+    T.nt = rem % P.nt_count;
+    rem /= P.nt_count;
+    T.mt = rem % P.mt_count;
+    rem /= P.mt_count;
+    T.q = rem % P.d.o;
+    T.y = rem / P.d.o;
+    return T;
+}
+
+template <int BN>
+__global__ void __launch_bounds__(192, 1)
+    k_f1_tc(const __grid_constant__ CUtensorMap tmA1, const __grid_constant__ CUtensorMap tmB1,
+            const __grid_constant__ CUtensorMap tmA2, const __grid_constant__ CUtensorMap tmB2, TcF1Params P) {
+    using C = TcCfg<BN>;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t *full = (uint64_t *)(smem + C::STAGES * C::STAGE_BYTES);
+    uint64_t *empty = full + C::STAGES;
+    uint64_t *tfull = empty + C::STAGES;
+    uint64_t *tempty = tfull + 2;
+    uint64_t *drain = tempty + 2;
+    uint32_t *tmem_slot = (uint32_t *)(drain + 1);
+    __shared__ int s_abort;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        s_abort = 0;
+        for (int s = 0; s < C::STAGES; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int a = 0; a < 2; a++) {
+            mbar_init(&tfull[a], 1);
+            mbar_init(&tempty[a], 4);
+        }
+        mbar_init(drain, 1);
+        fence_mbar_init();
+    }
+    if (warp == 0 && lane == 0) {
+        tma_prefetch_desc(&tmA1);
+        tma_prefetch_desc(&tmB1);
+        tma_prefetch_desc(&tmA2);
+        tma_prefetch_desc(&tmB2);
+    }
+    if (warp == 1) {
+        tmem_alloc(tmem_slot, C::TMEM_COLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    volatile int *abortp = &s_abort;
+    const int total = P.cum[P.ch.nperm];
+    const int nkb = P.nkb1 + P.nkb2;
+
+    if (warp == 0 && lane == 0) {
+        // ---------------- TMA producer ----------------
+        int stage = 0;
+        uint32_t phase = 0;
+        uint32_t pend_phase[C::STAGES];
+        bool pending[C::STAGES];
+        for (int s = 0; s < C::STAGES; s++) pending[s] = false;
+        bool ok = true;
+        for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+            const F1Tile T = f1_decode(P, t);
+            const PermBlock &pb = P.ch.pb[T.tau];
+            const int yg = pb.Y0 + T.y;
+            for (int kb = 0; kb < nkb; kb++) {
+                if (!mbar_wait(&empty[stage], phase ^ 1u, abortp)) {
+                    ok = false;
+                    break;
+                }
+                pending[stage] = false;
+                mbar_expect_tx(&full[stage], C::STAGE_BYTES);
+                uint8_t *sA = smem + stage * C::STAGE_BYTES;
+                uint8_t *sAl = sA + C::A_BYTES;
+                uint8_t *sB = sAl + C::A_BYTES;
+                uint8_t *sBl = sB + C::B_BYTES;
+                if (kb < P.nkb1) {
+                    const int f0 = kb * kTcBK;
+                    tma_load_5d(sA, &tmA1, &full[stage], f0, pb.X0, T.mt * 8, yg, 0);
+                    tma_load_5d(sAl, &tmA1, &full[stage], f0, pb.X0, T.mt * 8, yg, 1);
+                    tma_load_5d(sB, &tmB1, &full[stage], f0, pb.Z0, T.nt * C::RT, T.q, 0);
+                    tma_load_5d(sBl, &tmB1, &full[stage], f0, pb.Z0, T.nt * C::RT, T.q, 1);
+                } else {
+                    const int m0 = (kb - P.nkb1) * kTcBK;
+                    tma_load_5d(sA, &tmA2, &full[stage], m0, pb.X0, T.mt * 8, T.q, 0);
+                    tma_load_5d(sAl, &tmA2, &full[stage], m0, pb.X0, T.mt * 8, T.q, 1);
+                    tma_load_5d(sB, &tmB2, &full[stage], m0, pb.Z0, T.nt * C::RT, yg, 0);
+                    tma_load_5d(sBl, &tmB2, &full[stage], m0, pb.Z0, T.nt * C::RT, yg, 1);
+                }
+                pending[stage] = true;
+                pend_phase[stage] = phase;
+                if (++stage == C::STAGES) {
+                    stage = 0;
+                    phase ^= 1u;
+                }
+            }
+        }
+        if (!ok) {
+            *abortp = 1;
+            atomicOr(P.err, 1);
+            // let copies already in flight land before the CTA can exit
+            for (int s = 0; s < C::STAGES; s++)
+                if (pending[s]) {
+                    for (uint32_t i = 0; i < kSpinLimit && !mbar_try_wait(&full[s], pend_phase[s]); i++) {
+                    }
+                }
+        }
+    } else if (warp == 1 && lane == 0) {
+        // ---------------- MMA issuer ----------------
+        const uint32_t idesc = make_idesc_f16(kTcBM, BN, P.bf16 != 0, false, false);
+        int stage = 0;
+        uint32_t phase = 0;
+        int local = 0;
+        bool ok = true;
+        for (int t = blockIdx.x; t < total && ok; t += gridDim.x, local++) {
+            const int acc = local & 1;
+            const uint32_t accph = (local >> 1) & 1;
+            if (!mbar_wait(&tempty[acc], accph ^ 1u, abortp)) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
+            for (int kb = 0; kb < nkb; kb++) {
+                if (!mbar_wait(&full[stage], phase, abortp)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t a_h = smem_u32(smem + stage * C::STAGE_BYTES);
+                const uint32_t a_l = a_h + C::A_BYTES;
+                const uint32_t b_h = a_l + C::A_BYTES;
+                const uint32_t b_l = b_h + C::B_BYTES;
+#pragma unroll
+                for (int ks = 0; ks < kTcBK / 16; ks++) {
+                    const uint64_t dah = make_sdesc_sw128(a_h + 32 * ks, 16, 1024);
+                    const uint64_t dal = make_sdesc_sw128(a_l + 32 * ks, 16, 1024);
+                    const uint64_t dbh = make_sdesc_sw128(b_h + 32 * ks, 16, 1024);
+                    const uint64_t dbl = make_sdesc_sw128(b_l + 32 * ks, 16, 1024);
+                    umma_f16(d_tmem, dah, dbh, idesc, (kb > 0 || ks > 0) ? 1u : 0u);
+                    umma_f16(d_tmem, dah, dbl, idesc, 1u);
+                    umma_f16(d_tmem, dal, dbh, idesc, 1u);
+                }
+                umma_commit(&empty[stage]);
+                if (++stage == C::STAGES) {
+                    stage = 0;
+                    phase ^= 1u;
+                }
+            }
+            if (!ok) break;
+            umma_commit(&tfull[acc]);
+        }
+        if (!ok) {
+            *abortp = 1;
+            atomicOr(P.err, 2);
+        }
+        // all MMAs of this thread complete before TMEM can be released
+        umma_commit(drain);
+        for (uint32_t i = 0; i < kSpinLimit && !mbar_try_wait(drain, 0); i++) {
+        }
+    } else if (warp >= 2) {
+        // ---------------- epilogue ----------------
+        const int quarter = warp & 3;
+        const int row = quarter * 32 + lane;
+        const int o = P.d.o;
+        const float sc = *P.out_scale;
+        int local = 0;
+        for (int t = blockIdx.x; t < total; t += gridDim.x, local++) {
+            const int acc = local & 1;
+            const uint32_t accph = (local >> 1) & 1;
+            if (!mbar_wait(&tfull[acc], accph, abortp)) {
+                *abortp = 1;
+                atomicOr(P.err, 4);
+                break;
+            }
+            tc_fence_after();
+            const F1Tile T = f1_decode(P, t);
+            const PermBlock &pb = P.ch.pb[T.tau];
+            const int p = T.mt * 8 + row / 16;
+            const int x = row % 16;
+            const bool vrow = (p < o) && (x < pb.Tx);
+            float *dst = P.S + pb.soff +
+                         ((((long long)(p * o + T.q) * pb.Ty + T.y) * pb.Tx + x) * o) * pb.Tz;
+#pragma unroll 1
+            for (int c = 0; c < BN / 32; c++) {
+                uint32_t v[32];
+                tmem_ld32(tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * BN + c * 32), v);
+                tmem_ld_wait();
+                if (vrow) {
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        const int r = T.nt * C::RT + c * 2 + h;
+                        if (r >= o) continue;
+                        float *d = dst + (long long)r * pb.Tz;
+                        if (pb.Tz == 16) {
+                            float4 *d4 = reinterpret_cast<float4 *>(d);
+#pragma unroll
+                            for (int z4 = 0; z4 < 4; z4++) {
+                                float4 w;
+                                w.x = __uint_as_float(v[h * 16 + z4 * 4 + 0]) * sc;
+                                w.y = __uint_as_float(v[h * 16 + z4 * 4 + 1]) * sc;
+                                w.z = __uint_as_float(v[h * 16 + z4 * 4 + 2]) * sc;
+                                w.w = __uint_as_float(v[h * 16 + z4 * 4 + 3]) * sc;
+                                d4[z4] = w;
+                            }
+                        } else {
+                            for (int z = 0; z < pb.Tz; z++) d[z] = __uint_as_float(v[h * 16 + z]) * sc;
+                        }
+                    }
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty[acc]);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem_base, C::TMEM_COLS);
+    }
+}
+
+}  // namespace tb

@@ -9,7 +9,11 @@
 #include <vector>
 
 #include "common.cuh"
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include "gemm_fp64.cuh"
+#include "tc_f1.cuh"
 #include "pyscfad_b200.h"
 #include "triples_internal.h"
 
@@ -66,19 +70,19 @@ static void make_chunk(const Dims &d, int A, int B, int C, ChunkDesc &ch) {
         pb.Y0 = by * d.Tv; pb.Ty = bsize(by);
         pb.Z0 = bz * d.Tv; pb.Tz = bsize(bz);
         pb.soff = off;
-        off += o3 * pb.Tx * pb.Ty * pb.Tz;
+        off += (o3 * pb.Tx * pb.Ty * pb.Tz + 15) / 16 * 16;   // 64 B aligned sub-buffers
     }
 }
 
 static long long chunk_stage_elems(const ChunkDesc &ch, const Dims &d) {
     long long o3 = (long long)d.o * d.o * d.o, s = 0;
-    for (int t = 0; t < ch.nperm; t++) s += o3 * ch.pb[t].Tx * ch.pb[t].Ty * ch.pb[t].Tz;
+    for (int t = 0; t < ch.nperm; t++) s += (o3 * ch.pb[t].Tx * ch.pb[t].Ty * ch.pb[t].Tz + 15) / 16 * 16;
     return s;
 }
 
 int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan &P) {
     if (nocc < 1 || nvir < 1 || nocc > kMaxCols || nvir > 32767) return TRIPLES_ERR_INVALID_ARGUMENT;
-    if (precision != TRIPLES_PRECISION_FP64 && precision != TRIPLES_PRECISION_MIXED)
+    if (precision < TRIPLES_PRECISION_FP64 || precision > TRIPLES_PRECISION_MIXED_BF16)
         return TRIPLES_ERR_INVALID_ARGUMENT;
     P = Plan{};
     P.prec = precision;
@@ -90,6 +94,8 @@ int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan
     d.n = nocc + nvir;
     d.Tv = choose_tv(nocc, nvir);
     d.Kp = nvir;
+    P.Kp8 = (nvir + 7) / 8 * 8;
+    P.Op8 = (nocc + 7) / 8 * 8;
     P.nb = (nvir + d.Tv - 1) / d.Tv;
     P.n_ijk = nocc * (nocc + 1) * (nocc + 2) / 6;
     long long maxst = 0;
@@ -107,18 +113,27 @@ int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan
     P.stage_elems = (size_t)maxst;
     P.max_items = maxitems;
     P.f2_gy = (maxitems + kF2Threads - 1) / kF2Threads;
+    const bool mixed = precision != TRIPLES_PRECISION_FP64;
+    P.stage_bytes = mixed ? sizeof(float) : sizeof(double);
 
     const size_t o = nocc, v = nvir, Kp = d.Kp;
     const size_t el = sizeof(double);
     size_t off = 0;
     auto take = [&](size_t bytes) { size_t at = off; off = align256(off + bytes); return at; };
+    P.off_ctrl = take(kCtrlBytes);
     P.off_A1 = take(v * o * v * Kp * el);
     P.off_B1 = take(o * o * v * Kp * el);
     P.off_A2 = take(o * o * v * o * el);
     P.off_B2 = take(v * o * v * o * el);
-    P.off_S = take(P.stage_elems * el);
+    if (mixed) {
+        P.off_A1h = take(2 * v * o * v * P.Kp8 * 2);
+        P.off_B1h = take(2 * o * o * v * P.Kp8 * 2);
+        P.off_A2h = take(2 * o * o * v * P.Op8 * 2);
+        P.off_B2h = take(2 * v * o * v * P.Op8 * 2);
+    }
+    P.off_S = take(P.stage_elems * P.stage_bytes);
     if (want_grad) {
-        P.off_SV = take(P.stage_elems * el);
+        P.off_SV = take(P.stage_elems * P.stage_bytes);
         P.off_GA1 = take(v * o * v * Kp * el);
         P.off_GB1 = take(o * o * v * Kp * el);
         P.off_GA2 = take(o * o * v * o * el);
@@ -126,8 +141,6 @@ int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan
     }
     P.off_ijk = take((size_t)P.n_ijk * 3 * sizeof(int));
     P.off_epart = take((size_t)P.n_ijk * P.f2_gy * el);
-    P.off_eacc = take(2 * el);
-    P.off_counter = take(sizeof(unsigned));
     P.total = off;
     return TRIPLES_OK;
 }
@@ -203,25 +216,181 @@ __global__ void k_prep_B2(const double *__restrict__ t2, Dims d, double *__restr
 }
 
 // ---------------------------------------------------------------------------
+// 16-bit split operands for the tensor-core path
+// ---------------------------------------------------------------------------
+__global__ void k_ijk_table(int o, int *ijk) {
+    // representatives i >= j >= k, enumerated i-major
+    const int n = o * (o + 1) * (o + 2) / 6;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        int i = 0;
+        while ((i + 1) * (i + 2) * (i + 3) / 6 <= r) i++;
+        int rem = r - i * (i + 1) * (i + 2) / 6;
+        int j = 0;
+        while ((j + 1) * (j + 2) / 2 <= rem) j++;
+        int k = rem - j * (j + 1) / 2;
+        ijk[3 * r] = i;
+        ijk[3 * r + 1] = j;
+        ijk[3 * r + 2] = k;
+    }
+}
+
+__global__ void k_absmax(const double *__restrict__ x, long long n, unsigned long long *out) {
+    double m = 0.0;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+         e += (long long)gridDim.x * blockDim.x)
+        m = fmax(m, fabs(x[e]));
+    for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, off));
+    if ((threadIdx.x & 31) == 0 && m > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+__device__ __forceinline__ double pow2_scale(double m) {
+    // largest power of two s with m * s < 2^14 (fp16 keeps headroom below 65504)
+    if (!(m > 0.0) || !isfinite(m)) return 1.0;
+    int e;
+    frexp(m, &e);   // m < 2^e
+    return ldexp(1.0, 14 - e);
+}
+
+__global__ void k_make_scales(Ctrl *ctrl, int scaled) {
+    const double a = fmax(__longlong_as_double((long long)ctrl->absmax[0]),
+                          __longlong_as_double((long long)ctrl->absmax[1]));
+    const double b = __longlong_as_double((long long)ctrl->absmax[2]);
+    const double sA = scaled ? pow2_scale(a) : 1.0;
+    const double sB = scaled ? pow2_scale(b) : 1.0;
+    ctrl->scale[0] = sA;
+    ctrl->scale[1] = sB;
+    ctrl->out_scale = (float)(1.0 / (sA * sB));
+}
+
+template <typename H>
+__device__ __forceinline__ void split16(double xs, H &hi, H &lo);
+template <>
+__device__ __forceinline__ void split16<__half>(double xs, __half &hi, __half &lo) {
+    hi = __double2half(xs);
+    lo = __double2half(xs - (double)__half2float(hi));
+}
+template <>
+__device__ __forceinline__ void split16<__nv_bfloat16>(double xs, __nv_bfloat16 &hi, __nv_bfloat16 &lo) {
+    hi = __double2bfloat16(xs);
+    lo = __double2bfloat16(xs - (double)__bfloat162float(hi));
+}
+
+// A1h[h][y][p][x][f] = split(ovvv[p,x,f,y] * sA), f < Kp8 (zero beyond v)
+template <typename H>
+__global__ void k_prep_A1h(const double *__restrict__ ovvv, int packed, Dims d, int Kp8,
+                           const Ctrl *ctrl, H *__restrict__ out) {
+    __shared__ double tile[32][33];
+    const long long px = blockIdx.z;
+    const int f0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+    const long long npair = (long long)d.v * (d.v + 1) / 2;
+    const double sA = ctrl->scale[0];
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        int f = f0 + r, y = y0 + threadIdx.x;
+        double val = 0.0;
+        if (f < d.v && y < d.v)
+            val = packed ? ovvv[px * npair + tri_index(f, y)] : ovvv[(px * d.v + f) * d.v + y];
+        tile[r][threadIdx.x] = val;
+    }
+    __syncthreads();
+    const long long half = (long long)d.v * d.o * d.v * Kp8;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        int y = y0 + r, f = f0 + threadIdx.x;
+        if (y < d.v && f < Kp8) {
+            H hi, lo;
+            split16<H>(tile[threadIdx.x][r] * sA, hi, lo);
+            const long long e = ((long long)y * d.o * d.v + px) * Kp8 + f;
+            out[e] = hi;
+            out[half + e] = lo;
+        }
+    }
+}
+
+// B1h[h][q][r][z][f] = split(t2[r,q,z,f] * sB)
+template <typename H>
+__global__ void k_prep_B1h(const double *__restrict__ t2, Dims d, int Kp8, const Ctrl *ctrl,
+                           H *__restrict__ out) {
+    const long long row = blockIdx.x;  // (q*o + r)*v + z
+    const int z = row % d.v;
+    const int qr = row / d.v;
+    const int r = qr % d.o, q = qr / d.o;
+    const double *src = t2 + (((long long)r * d.o + q) * d.v + z) * d.v;
+    const double sB = ctrl->scale[1];
+    const long long half = (long long)d.o * d.o * d.v * Kp8;
+    for (int f = threadIdx.x; f < Kp8; f += blockDim.x) {
+        H hi, lo;
+        split16<H>(f < d.v ? src[f] * sB : 0.0, hi, lo);
+        out[row * Kp8 + f] = hi;
+        out[half + row * Kp8 + f] = lo;
+    }
+}
+
+// A2h[h][q][p][x][m] = split(-ovoo[p,x,m,q] * sA), m < Op8
+template <typename H>
+__global__ void k_prep_A2h(const double *__restrict__ ovoo, Dims d, int Op8, const Ctrl *ctrl,
+                           H *__restrict__ out) {
+    const long long total = (long long)d.o * d.o * d.v * Op8;
+    const double sA = ctrl->scale[0];
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        int m = e % Op8;
+        long long t = e / Op8;
+        int x = t % d.v;
+        t /= d.v;
+        int p = t % d.o;
+        int q = t / d.o;
+        double val = m < d.o ? -ovoo[(((long long)p * d.v + x) * d.o + m) * d.o + q] * sA : 0.0;
+        H hi, lo;
+        split16<H>(val, hi, lo);
+        out[e] = hi;
+        out[total + e] = lo;
+    }
+}
+
+// B2h[h][y][r][z][m] = split(t2[r,m,z,y] * sB), m < Op8
+template <typename H>
+__global__ void k_prep_B2h(const double *__restrict__ t2, Dims d, int Op8, const Ctrl *ctrl,
+                           H *__restrict__ out) {
+    const long long total = (long long)d.v * d.o * d.v * Op8;
+    const double sB = ctrl->scale[1];
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        int m = e % Op8;
+        long long t = e / Op8;
+        int z = t % d.v;
+        t /= d.v;
+        int r = t % d.o;
+        int y = t / d.o;
+        double val = m < d.o ? t2[(((long long)r * d.o + m) * d.v + z) * d.v + y] * sB : 0.0;
+        H hi, lo;
+        split16<H>(val, hi, lo);
+        out[e] = hi;
+        out[total + e] = lo;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // FP64 contraction kernels (one GEMM problem per blockIdx.z)
 // ---------------------------------------------------------------------------
+template <typename StageT>
 struct GemmLaunch {
     Dims d;
     ChunkDesc ch;
     int cum[7];      // prefix sums used to decode blockIdx.z
     int tau_only;    // >= 0: restrict to this ordering
     const double *A1, *B1, *A2, *B2;
-    double *S, *G;   // staging, gradient target
+    StageT *S;       // staging
+    double *G;       // gradient target
 };
 
-__device__ __forceinline__ int find_tau(const GemmLaunch &L, int b) {
+template <typename StageT>
+__device__ __forceinline__ int find_tau(const GemmLaunch<StageT> &L, int b) {
     int t = 0;
     while (t + 1 < L.ch.nperm && b >= L.cum[t + 1]) t++;
     return t;
 }
 
 // F1: S_tau[p][q][y][x][r][z] = W for all (tau, y, q)
-__global__ void __launch_bounds__(256) k_f1_fp64(GemmLaunch L) {
+__global__ void __launch_bounds__(256) k_f1_fp64(GemmLaunch<double> L) {
     __shared__ GemmSmem sm;
     const int b = blockIdx.z;
     const int t = find_tau(L, b);
@@ -253,7 +422,8 @@ __global__ void __launch_bounds__(256) k_f1_fp64(GemmLaunch L) {
 }
 
 // ovvv gradient: G_A1[y][p][x][f] += sum_{q,r,z} Wbar * B1[q][r][z][f]; z = (tau, y)
-__global__ void __launch_bounds__(256) k_b1a_fp64(GemmLaunch L) {
+template <typename StageT>
+__global__ void __launch_bounds__(256) k_b1a_fp64(GemmLaunch<StageT> L) {
     __shared__ GemmSmem sm;
     const int b = blockIdx.z;
     const int t = find_tau(L, b);
@@ -263,12 +433,12 @@ __global__ void __launch_bounds__(256) k_b1a_fp64(GemmLaunch L) {
     const int y = b - L.cum[t];
     const long long oTz = (long long)o * pb.Tz;
     const long long sq = (long long)pb.Ty * pb.Tx * oTz;   // stride of q in S
-    GemmArgs g;
+    GemmArgsT<StageT> g;
     g.M = o * pb.Tx;
     g.N = v;
     g.K = o * o * pb.Tz;
     g.K2 = 0;
-    g.A = GOp{L.S + pb.soff + (long long)y * pb.Tx * oTz, map2(pb.Tx, oTz, (long long)o * sq),
+    g.A = GOpT<StageT>{L.S + pb.soff + (long long)y * pb.Tx * oTz, map2(pb.Tx, oTz, (long long)o * sq),
               map2((int)oTz, 1, sq), 1};
     g.B = GOp{L.B1 + (long long)pb.Z0 * Kp, map1(1),
               map3(pb.Tz, o, Kp, (long long)v * Kp, (long long)o * v * Kp), 0};
@@ -284,7 +454,8 @@ __global__ void __launch_bounds__(256) k_b1a_fp64(GemmLaunch L) {
 }
 
 // t2 gradient (ovvv term): G_B1[q][r][z][f] += sum_{y,p,x} Wbar * A1[y][p][x][f]; z = q
-__global__ void __launch_bounds__(256) k_b1b_fp64(GemmLaunch L) {
+template <typename StageT>
+__global__ void __launch_bounds__(256) k_b1b_fp64(GemmLaunch<StageT> L) {
     __shared__ GemmSmem sm;
     const int q = blockIdx.z;
     const PermBlock &pb = L.ch.pb[L.tau_only];
@@ -292,12 +463,12 @@ __global__ void __launch_bounds__(256) k_b1b_fp64(GemmLaunch L) {
     const int o = d.o, v = d.v, Kp = d.Kp;
     const long long oTz = (long long)o * pb.Tz;
     const long long sq = (long long)pb.Ty * pb.Tx * oTz;
-    GemmArgs g;
+    GemmArgsT<StageT> g;
     g.M = o * pb.Tz;
     g.N = v;
     g.K = pb.Ty * o * pb.Tx;
     g.K2 = 0;
-    g.A = GOp{L.S + pb.soff + (long long)q * sq, map1(1),
+    g.A = GOpT<StageT>{L.S + pb.soff + (long long)q * sq, map1(1),
               map3(pb.Tx, o, oTz, (long long)o * sq, (long long)pb.Tx * oTz), 0};
     g.B = GOp{L.A1 + ((long long)pb.Y0 * o * v + pb.X0) * Kp, map1(1),
               map3(pb.Tx, o, Kp, (long long)v * Kp, (long long)o * v * Kp), 0};
@@ -313,7 +484,8 @@ __global__ void __launch_bounds__(256) k_b1b_fp64(GemmLaunch L) {
 }
 
 // ovoo gradient: G_A2[q][p][x][m] -= sum_{y,r,z} Wbar * B2[y][r][z][m]; z = q
-__global__ void __launch_bounds__(256) k_b1c_fp64(GemmLaunch L) {
+template <typename StageT>
+__global__ void __launch_bounds__(256) k_b1c_fp64(GemmLaunch<StageT> L) {
     __shared__ GemmSmem sm;
     const int q = blockIdx.z;
     const PermBlock &pb = L.ch.pb[L.tau_only];
@@ -321,12 +493,12 @@ __global__ void __launch_bounds__(256) k_b1c_fp64(GemmLaunch L) {
     const int o = d.o, v = d.v;
     const long long oTz = (long long)o * pb.Tz;
     const long long sq = (long long)pb.Ty * pb.Tx * oTz;
-    GemmArgs g;
+    GemmArgsT<StageT> g;
     g.M = o * pb.Tx;
     g.N = o;
     g.K = pb.Ty * o * pb.Tz;
     g.K2 = 0;
-    g.A = GOp{L.S + pb.soff + (long long)q * sq, map2(pb.Tx, oTz, (long long)o * sq),
+    g.A = GOpT<StageT>{L.S + pb.soff + (long long)q * sq, map2(pb.Tx, oTz, (long long)o * sq),
               map2((int)oTz, 1, (long long)pb.Tx * oTz), 1};
     g.B = GOp{L.B2 + ((long long)pb.Y0 * o * v + pb.Z0) * o, map1(1),
               map3(pb.Tz, o, o, (long long)v * o, (long long)o * v * o), 0};
@@ -342,7 +514,8 @@ __global__ void __launch_bounds__(256) k_b1c_fp64(GemmLaunch L) {
 }
 
 // t2 gradient (ooov term): G_B2[y][r][z][m] -= sum_{q,p,x} Wbar * A2[q][p][x][m]; z = (tau, y)
-__global__ void __launch_bounds__(256) k_b1d_fp64(GemmLaunch L) {
+template <typename StageT>
+__global__ void __launch_bounds__(256) k_b1d_fp64(GemmLaunch<StageT> L) {
     __shared__ GemmSmem sm;
     const int b = blockIdx.z;
     const int t = find_tau(L, b);
@@ -352,12 +525,12 @@ __global__ void __launch_bounds__(256) k_b1d_fp64(GemmLaunch L) {
     const int y = b - L.cum[t];
     const long long oTz = (long long)o * pb.Tz;
     const long long sq = (long long)pb.Ty * pb.Tx * oTz;
-    GemmArgs g;
+    GemmArgsT<StageT> g;
     g.M = o * pb.Tz;
     g.N = o;
     g.K = o * o * pb.Tx;
     g.K2 = 0;
-    g.A = GOp{L.S + pb.soff + (long long)y * pb.Tx * oTz, map1(1),
+    g.A = GOpT<StageT>{L.S + pb.soff + (long long)y * pb.Tx * oTz, map1(1),
               map3(pb.Tx, o, oTz, (long long)o * sq, sq), 0};
     g.B = GOp{L.A2 + (long long)pb.X0 * o, map1(1),
               map3(pb.Tx, o, o, (long long)v * o, (long long)o * v * o), 0};
@@ -735,41 +908,80 @@ static inline unsigned grid1d(long long n, int threads) {
     return (unsigned)b;
 }
 
-int run_triples(const Plan &P, cudaStream_t st, const TriplesIO &io) {
+// ---- tensor maps (driver entry point fetched through the runtime) ----
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *,
+                                  CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                  CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn get_encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void *ptr = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)ptr;
+    }
+    return fn;
+}
+
+// 5-D map over a [2][d3][d2][d1][d0] 16-bit array (d0 innermost), 128B swizzle.
+static int make_tmap5(CUtensorMap *tm, void *base, bool bf16, const uint64_t dims[5], const uint32_t box[5]) {
+    EncodeTiledFn enc = get_encode_fn();
+    if (!enc) return TRIPLES_ERR_UNSUPPORTED;
+    cuuint64_t gdim[5], gstr[4];
+    uint64_t stride = 2;
+    for (int i = 0; i < 5; i++) {
+        gdim[i] = dims[i];
+        if (i < 4) {
+            stride *= dims[i];
+            gstr[i] = stride;
+        }
+    }
+    cuuint32_t bx[5], es[5] = {1, 1, 1, 1, 1};
+    for (int i = 0; i < 5; i++) bx[i] = box[i];
+    CUresult r = enc(tm, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 5, base, gdim,
+                     gstr, bx, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? TRIPLES_OK : TRIPLES_ERR_CUDA;
+}
+
+static int num_sms() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+template <typename StageT>
+static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
     const Dims d = P.d;
+    const bool mixed = P.prec != TRIPLES_PRECISION_FP64;
+    const bool bf16 = P.prec == TRIPLES_PRECISION_MIXED_BF16;
     char *ws = (char *)io.workspace;
+    Ctrl *ctrl = (Ctrl *)(ws + P.off_ctrl);
     double *A1 = (double *)(ws + P.off_A1);
     double *B1 = (double *)(ws + P.off_B1);
     double *A2 = (double *)(ws + P.off_A2);
     double *B2 = (double *)(ws + P.off_B2);
-    double *S = (double *)(ws + P.off_S);
-    double *SV = P.want_grad ? (double *)(ws + P.off_SV) : nullptr;
+    StageT *S = (StageT *)(ws + P.off_S);
+    StageT *SV = P.want_grad ? (StageT *)(ws + P.off_SV) : nullptr;
     double *GA1 = P.want_grad ? (double *)(ws + P.off_GA1) : nullptr;
     double *GB1 = P.want_grad ? (double *)(ws + P.off_GB1) : nullptr;
     double *GA2 = P.want_grad ? (double *)(ws + P.off_GA2) : nullptr;
     double *GB2 = P.want_grad ? (double *)(ws + P.off_GB2) : nullptr;
     int *ijk = (int *)(ws + P.off_ijk);
     double *e_part = (double *)(ws + P.off_epart);
-    double *e_acc = (double *)(ws + P.off_eacc);
-    unsigned *counter = (unsigned *)(ws + P.off_counter);
     const size_t o = d.o, v = d.v, n = d.n;
 
-    // occupied triplet representatives i >= j >= k
-    {
-        std::vector<int> h;
-        h.reserve((size_t)P.n_ijk * 3);
-        for (int i = 0; i < d.o; i++)
-            for (int j = 0; j <= i; j++)
-                for (int k = 0; k <= j; k++) {
-                    h.push_back(i);
-                    h.push_back(j);
-                    h.push_back(k);
-                }
-        TB_CUDA(cudaMemcpyAsync(ijk, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice, st));
-        TB_CUDA(cudaStreamSynchronize(st));  // host vector goes out of scope
-    }
-    TB_CUDA(cudaMemsetAsync(e_acc, 0, 2 * sizeof(double), st));
-    TB_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned), st));
+    TB_CUDA(cudaMemsetAsync(ctrl, 0, kCtrlBytes, st));
+    k_ijk_table<<<grid1d(P.n_ijk, 128), 128, 0, st>>>(d.o, ijk);
+    TB_LAUNCH_CHECK();
     if (P.want_grad) {
         TB_CUDA(cudaMemsetAsync(GA1, 0, v * o * v * d.Kp * sizeof(double), st));
         TB_CUDA(cudaMemsetAsync(GB1, 0, o * o * v * d.Kp * sizeof(double), st));
@@ -782,7 +994,7 @@ int run_triples(const Plan &P, cudaStream_t st, const TriplesIO &io) {
         TB_CUDA(cudaMemsetAsync(io.fvo_bar, 0, v * o * sizeof(double), st));
     }
 
-    // operand layouts
+    // FP64 operand layouts (used by the FP64 contractions)
     k_prep_A1<<<dim3((d.Kp + 31) / 32, (d.v + 31) / 32, (unsigned)(o * v)), dim3(32, 8), 0, st>>>(
         io.ovvv, P.packed, d, A1);
     TB_LAUNCH_CHECK();
@@ -792,6 +1004,59 @@ int run_triples(const Plan &P, cudaStream_t st, const TriplesIO &io) {
     TB_LAUNCH_CHECK();
     k_prep_B2<<<grid1d((long long)v * o * v * o, 256), 256, 0, st>>>(io.t2, d, B2);
     TB_LAUNCH_CHECK();
+
+    // 16-bit split operands and tensor maps (tensor-core path)
+    constexpr int BN = 256;
+    CUtensorMap tmA1, tmB1, tmA2, tmB2;
+    if (mixed) {
+        const long long npair = (long long)v * (v + 1) / 2;
+        k_absmax<<<grid1d((long long)o * v * (P.packed ? npair : (long long)v * v), 256), 256, 0, st>>>(
+            io.ovvv, (long long)o * v * (P.packed ? npair : (long long)v * v), &ctrl->absmax[0]);
+        k_absmax<<<grid1d((long long)o * v * o * o, 256), 256, 0, st>>>(io.ovoo, (long long)o * v * o * o,
+                                                                         &ctrl->absmax[1]);
+        k_absmax<<<grid1d((long long)o * o * v * v, 256), 256, 0, st>>>(io.t2, (long long)o * o * v * v,
+                                                                         &ctrl->absmax[2]);
+        k_make_scales<<<1, 1, 0, st>>>(ctrl, bf16 ? 0 : 1);
+        TB_LAUNCH_CHECK();
+        if (bf16) {
+            k_prep_A1h<__nv_bfloat16><<<dim3((P.Kp8 + 31) / 32, (d.v + 31) / 32, (unsigned)(o * v)), dim3(32, 8), 0, st>>>(
+                io.ovvv, P.packed, d, P.Kp8, ctrl, (__nv_bfloat16 *)(ws + P.off_A1h));
+            k_prep_B1h<__nv_bfloat16><<<(unsigned)(o * o * v), 128, 0, st>>>(io.t2, d, P.Kp8, ctrl,
+                                                                            (__nv_bfloat16 *)(ws + P.off_B1h));
+            k_prep_A2h<__nv_bfloat16><<<grid1d((long long)o * o * v * P.Op8, 256), 256, 0, st>>>(
+                io.ovoo, d, P.Op8, ctrl, (__nv_bfloat16 *)(ws + P.off_A2h));
+            k_prep_B2h<__nv_bfloat16><<<grid1d((long long)v * o * v * P.Op8, 256), 256, 0, st>>>(
+                io.t2, d, P.Op8, ctrl, (__nv_bfloat16 *)(ws + P.off_B2h));
+        } else {
+            k_prep_A1h<__half><<<dim3((P.Kp8 + 31) / 32, (d.v + 31) / 32, (unsigned)(o * v)), dim3(32, 8), 0, st>>>(
+                io.ovvv, P.packed, d, P.Kp8, ctrl, (__half *)(ws + P.off_A1h));
+            k_prep_B1h<__half><<<(unsigned)(o * o * v), 128, 0, st>>>(io.t2, d, P.Kp8, ctrl,
+                                                                     (__half *)(ws + P.off_B1h));
+            k_prep_A2h<__half><<<grid1d((long long)o * o * v * P.Op8, 256), 256, 0, st>>>(
+                io.ovoo, d, P.Op8, ctrl, (__half *)(ws + P.off_A2h));
+            k_prep_B2h<__half><<<grid1d((long long)v * o * v * P.Op8, 256), 256, 0, st>>>(
+                io.t2, d, P.Op8, ctrl, (__half *)(ws + P.off_B2h));
+        }
+        TB_LAUNCH_CHECK();
+        {
+            const uint64_t dA1[5] = {(uint64_t)P.Kp8, v, o, v, 2};
+            const uint32_t bA[5] = {64, 16, 8, 1, 1};
+            const uint64_t dB1[5] = {(uint64_t)P.Kp8, v, o, o, 2};
+            const uint32_t bB[5] = {64, 16, (uint32_t)TcCfg<BN>::RT, 1, 1};
+            const uint64_t dA2[5] = {(uint64_t)P.Op8, v, o, o, 2};
+            const uint64_t dB2[5] = {(uint64_t)P.Op8, v, o, v, 2};
+            int rc;
+            if ((rc = make_tmap5(&tmA1, ws + P.off_A1h, bf16, dA1, bA)) != TRIPLES_OK) return rc;
+            if ((rc = make_tmap5(&tmB1, ws + P.off_B1h, bf16, dB1, bB)) != TRIPLES_OK) return rc;
+            if ((rc = make_tmap5(&tmA2, ws + P.off_A2h, bf16, dA2, bA)) != TRIPLES_OK) return rc;
+            if ((rc = make_tmap5(&tmB2, ws + P.off_B2h, bf16, dB2, bB)) != TRIPLES_OK) return rc;
+        }
+        static bool attr_set = false;
+        if (!attr_set) {
+            TB_CUDA(cudaFuncSetAttribute(k_f1_tc<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcCfg<BN>::SMEM));
+            attr_set = true;
+        }
+    }
 
     for (int A = 0; A < P.nb; A++)
         for (int B = 0; B <= A; B++)
@@ -803,21 +1068,43 @@ int run_triples(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                     if (ch.pb[t].Tx > maxTx) maxTx = ch.pb[t].Tx;
                     if (ch.pb[t].Tz > maxTz) maxTz = ch.pb[t].Tz;
                 }
-                GemmLaunch L;
-                L.d = d;
-                L.ch = ch;
-                L.tau_only = -1;
-                L.A1 = A1; L.B1 = B1; L.A2 = A2; L.B2 = B2;
-                L.S = S; L.G = nullptr;
                 // F1: raw amplitudes
-                L.cum[0] = 0;
-                for (int t = 0; t < ch.nperm; t++) L.cum[t + 1] = L.cum[t] + ch.pb[t].Ty * d.o;
-                k_f1_fp64<<<dim3((d.o * maxTx + kGBM - 1) / kGBM, (d.o * maxTz + kGBN - 1) / kGBN,
-                                 L.cum[ch.nperm]),
-                            256, 0, st>>>(L);
-                TB_LAUNCH_CHECK();
+                if (mixed) {
+                    TcF1Params T;
+                    T.d = d;
+                    T.ch = ch;
+                    T.mt_count = (d.o + 7) / 8;
+                    T.nt_count = (d.o + TcCfg<BN>::RT - 1) / TcCfg<BN>::RT;
+                    T.cum[0] = 0;
+                    for (int t = 0; t < ch.nperm; t++)
+                        T.cum[t + 1] = T.cum[t] + ch.pb[t].Ty * d.o * T.mt_count * T.nt_count;
+                    T.nkb1 = (P.Kp8 + kTcBK - 1) / kTcBK;
+                    T.nkb2 = (P.Op8 + kTcBK - 1) / kTcBK;
+                    T.S = (float *)S;
+                    T.out_scale = &ctrl->out_scale;
+                    T.err = &ctrl->err;
+                    T.bf16 = bf16 ? 1 : 0;
+                    const int tiles = T.cum[ch.nperm];
+                    const int grid = tiles < num_sms() ? tiles : num_sms();
+                    k_f1_tc<BN><<<grid, 192, TcCfg<BN>::SMEM, st>>>(tmA1, tmB1, tmA2, tmB2, T);
+                    TB_LAUNCH_CHECK();
+                } else {
+                    GemmLaunch<double> L;
+                    L.d = d;
+                    L.ch = ch;
+                    L.tau_only = -1;
+                    L.A1 = A1; L.B1 = B1; L.A2 = A2; L.B2 = B2;
+                    L.S = (double *)S;
+                    L.G = nullptr;
+                    L.cum[0] = 0;
+                    for (int t = 0; t < ch.nperm; t++) L.cum[t + 1] = L.cum[t] + ch.pb[t].Ty * d.o;
+                    k_f1_fp64<<<dim3((d.o * maxTx + kGBM - 1) / kGBM, (d.o * maxTz + kGBN - 1) / kGBN,
+                                     L.cum[ch.nperm]),
+                                256, 0, st>>>(L);
+                    TB_LAUNCH_CHECK();
+                }
                 // F2: energy (+ adjoint of the raw amplitudes)
-                F2Params<double> F;
+                F2Params<StageT> F;
                 F.d = d;
                 F.ch = ch;
                 F.ijk = ijk;
@@ -825,14 +1112,14 @@ int run_triples(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                 F.S = S; F.SV = SV;
                 F.ybar = io.ybar;
                 F.want_grad = P.want_grad;
-                F.e_part = e_part; F.e_acc = e_acc; F.counter = counter;
+                F.e_part = e_part; F.e_acc = &ctrl->e_acc; F.counter = &ctrl->counter;
                 F.mo_bar = io.mo_energy_bar;
                 const int items = ch.nabc[0] * ch.nabc[1] * ch.nabc[2];
-                k_f2<double><<<dim3(P.n_ijk, (items + kF2Threads - 1) / kF2Threads), kF2Threads, 0, st>>>(F);
+                k_f2<StageT><<<dim3(P.n_ijk, (items + kF2Threads - 1) / kF2Threads), kF2Threads, 0, st>>>(F);
                 TB_LAUNCH_CHECK();
                 if (!P.want_grad) continue;
                 // V-term gradients
-                VGParams<double> VG;
+                VGParams<StageT> VG;
                 VG.d = d;
                 VG.ch = ch;
                 VG.SV = SV;
@@ -844,28 +1131,34 @@ int run_triples(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                     long long r = (long long)d.o * d.o * ch.pb[t].Ty * ch.pb[t].Tx;
                     if (r > maxrows) maxrows = r;
                 }
-                k_vgrad<double><<<dim3((unsigned)((maxrows + kVgRows - 1) / kVgRows), ch.nperm), 256, 0, st>>>(VG);
+                k_vgrad<StageT><<<dim3((unsigned)((maxrows + kVgRows - 1) / kVgRows), ch.nperm), 256, 0, st>>>(VG);
                 TB_LAUNCH_CHECK();
                 // W-term gradients
+                GemmLaunch<StageT> L;
+                L.d = d;
+                L.ch = ch;
+                L.tau_only = -1;
+                L.A1 = A1; L.B1 = B1; L.A2 = A2; L.B2 = B2;
+                L.S = S;
                 L.cum[0] = 0;
                 for (int t = 0; t < ch.nperm; t++) L.cum[t + 1] = L.cum[t] + ch.pb[t].Ty;
                 L.G = GA1;
-                k_b1a_fp64<<<dim3((d.o * maxTx + kGBM - 1) / kGBM, (d.v + kGBN - 1) / kGBN, L.cum[ch.nperm]),
-                             256, 0, st>>>(L);
+                k_b1a_fp64<StageT><<<dim3((d.o * maxTx + kGBM - 1) / kGBM, (d.v + kGBN - 1) / kGBN, L.cum[ch.nperm]),
+                                     256, 0, st>>>(L);
                 TB_LAUNCH_CHECK();
                 L.G = GB2;
-                k_b1d_fp64<<<dim3((d.o * maxTz + kGBM - 1) / kGBM, (d.o + kGBN - 1) / kGBN, L.cum[ch.nperm]),
-                             256, 0, st>>>(L);
+                k_b1d_fp64<StageT><<<dim3((d.o * maxTz + kGBM - 1) / kGBM, (d.o + kGBN - 1) / kGBN, L.cum[ch.nperm]),
+                                     256, 0, st>>>(L);
                 TB_LAUNCH_CHECK();
                 for (int t = 0; t < ch.nperm; t++) {
                     L.tau_only = t;
                     L.G = GB1;
-                    k_b1b_fp64<<<dim3((d.o * ch.pb[t].Tz + kGBM - 1) / kGBM, (d.v + kGBN - 1) / kGBN, d.o),
-                                 256, 0, st>>>(L);
+                    k_b1b_fp64<StageT><<<dim3((d.o * ch.pb[t].Tz + kGBM - 1) / kGBM, (d.v + kGBN - 1) / kGBN, d.o),
+                                         256, 0, st>>>(L);
                     TB_LAUNCH_CHECK();
                     L.G = GA2;
-                    k_b1c_fp64<<<dim3((d.o * ch.pb[t].Tx + kGBM - 1) / kGBM, (d.o + kGBN - 1) / kGBN, d.o),
-                                 256, 0, st>>>(L);
+                    k_b1c_fp64<StageT><<<dim3((d.o * ch.pb[t].Tx + kGBM - 1) / kGBM, (d.o + kGBN - 1) / kGBN, d.o),
+                                         256, 0, st>>>(L);
                     TB_LAUNCH_CHECK();
                 }
             }
@@ -884,9 +1177,14 @@ int run_triples(const Plan &P, cudaStream_t st, const TriplesIO &io) {
         k_fold_ovoo<<<grid1d((long long)o * v * o * o, 256), 256, 0, st>>>(GA2, d, io.ovoo_bar);
         TB_LAUNCH_CHECK();
     }
-    k_copy_scalar<<<1, 1, 0, st>>>(e_acc, io.e_out);
+    k_copy_scalar<<<1, 1, 0, st>>>(&ctrl->e_acc, io.e_out);
     TB_LAUNCH_CHECK();
     return TRIPLES_OK;
+}
+
+int run_triples(const Plan &P, cudaStream_t st, const TriplesIO &io) {
+    if (P.prec == TRIPLES_PRECISION_FP64) return run_impl<double>(P, st, io);
+    return run_impl<float>(P, st, io);
 }
 
 void set_block_size(int tv) { g_tv_override = tv; }
@@ -910,7 +1208,6 @@ static int triples_call(void *stream, int precision, int nocc, int nvir, int ovv
     tb::Plan P;
     int rc = tb::make_plan(precision, nocc, nvir, ovvv_packed, want_grad, P);
     if (rc != TRIPLES_OK) return rc;
-    if (precision != TRIPLES_PRECISION_FP64) return TRIPLES_ERR_UNSUPPORTED;
     if (!io.workspace || workspace_bytes < P.total) return TRIPLES_ERR_WORKSPACE;
     if (!io.mo_energy || !io.t1 || !io.t2 || !io.ovoo || !io.ovov || !io.ovvv || !io.fvo || !io.e_out)
         return TRIPLES_ERR_INVALID_ARGUMENT;
@@ -942,6 +1239,15 @@ int triples_energy_vjp(void *stream, int precision, int nocc, int nvir, int ovvv
     io.mo_energy_bar = mo_energy_bar; io.t1_bar = t1_bar; io.t2_bar = t2_bar; io.ovoo_bar = ovoo_bar;
     io.ovov_bar = ovov_bar; io.ovvv_bar = ovvv_bar; io.fvo_bar = fvo_bar;
     return triples_call(stream, precision, nocc, nvir, ovvv_packed, 1, io, workspace_bytes);
+}
+
+int triples_check_device_status(void *stream, const void *workspace) {
+    if (!workspace) return TRIPLES_ERR_INVALID_ARGUMENT;
+    tb::Ctrl c;
+    cudaError_t e = cudaMemcpyAsync(&c, workspace, sizeof(c), cudaMemcpyDeviceToHost, (cudaStream_t)stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e != cudaSuccess) return TRIPLES_ERR_CUDA;
+    return c.err ? TRIPLES_ERR_DEVICE_TIMEOUT : TRIPLES_OK;
 }
 
 const char *triples_status_string(int status) {

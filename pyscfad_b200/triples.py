@@ -63,8 +63,9 @@ def workspace_size(nocc, nvir, packed=True, want_grad=True, precision="fp64") ->
 
 
 def energy(mo_energy, t1, t2, ovoo, ovov, ovvv, fvo, precision="fp64", device=None,
-           stream=None) -> torch.Tensor:
-    """E(T) as a 0-dim FP64 tensor on the device (no host synchronisation)."""
+           stream=None, check=True) -> torch.Tensor:
+    """E(T) as a 0-dim FP64 tensor on the device.  With check=True the
+    stream is synchronised and device-side failures raise TriplesError."""
     lib = _lib.load()
     device = torch.device(device or (t1.device if isinstance(t1, torch.Tensor) and t1.is_cuda else "cuda"))
     args = [_as_dev(a, device) for a in (mo_energy, t1, t2, ovoo, ovov, ovvv, fvo)]
@@ -80,11 +81,13 @@ def energy(mo_energy, t1, t2, ovoo, ovov, ovvv, fvo, precision="fp64", device=No
     rc = lib.triples_energy(st.cuda_stream, prec, o, v, int(packed),
                             *[a.data_ptr() for a in args], ws.data_ptr(), ws.numel(), e.data_ptr())
     _lib.check(rc, "triples_energy")
+    if check:
+        _lib.check(lib.triples_check_device_status(st.cuda_stream, ws.data_ptr()), "triples_energy (device)")
     return e
 
 
 def energy_vjp(mo_energy, t1, t2, ovoo, ovov, ovvv, fvo, ybar=1.0, precision="fp64",
-               device=None, stream=None):
+               device=None, stream=None, check=True):
     """E(T) and dE/d(inputs) * ybar.  Gradients have the input layouts; for a
     packed ovvv the gradient is the reference's packed-tril fold
     (pyscfad/cc/ccsd_t.py:184-191).  Returns (e, dict)."""
@@ -105,4 +108,17 @@ def energy_vjp(mo_energy, t1, t2, ovoo, ovov, ovvv, fvo, ybar=1.0, precision="fp
                                 *[a.data_ptr() for a in args], float(ybar), ws.data_ptr(), ws.numel(),
                                 e.data_ptr(), *[grads[k].data_ptr() for k in KEYS])
     _lib.check(rc, "triples_energy_vjp")
+    if check:
+        _lib.check(lib.triples_check_device_status(st.cuda_stream, ws.data_ptr()),
+                   "triples_energy_vjp (device)")
     return e, grads
+
+
+def device_status(device=None, stream=None) -> int:
+    """Synchronise and return the device-side status of the last call."""
+    device = torch.device(device or "cuda")
+    buf = _workspaces.get((device.type, device.index))
+    if buf is None:
+        return 0
+    st = stream if stream is not None else torch.cuda.current_stream(device)
+    return int(_lib.load().triples_check_device_status(st.cuda_stream, buf.data_ptr()))

@@ -1,0 +1,68 @@
+"""Mixed-precision (tcgen05) path vs the FP64 oracle.
+
+Tolerances, fixed here and reported per workload in the benchmark:
+  fp16 hi/lo split with power-of-two scaling ("mixed"): E relative error
+      <= 1e-6, gradient relative error (max abs err / max abs value) <= 1e-5;
+  bf16 hi/lo split ("mixed_bf16"): E <= 1e-4, gradients <= 1e-3.
+"""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from pyscfad_b200 import triples
+from pyscfad_b200.synthetic import make_inputs
+from tests import golden_util as G
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"mixed": (1e-6, 1e-5), "mixed_bf16": (1e-4, 1e-3)}
+
+
+def _relerr(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-7))
+
+
+def _run(inp, packed, precision):
+    ovvv = inp.ovvv_tril() if packed else inp.ovvv
+    e, g = triples.energy_vjp(inp.mo_energy, inp.t1, inp.t2, inp.ovoo, inp.ovov, ovvv, inp.fvo,
+                              precision=precision, device="cuda")
+    return float(e), {k: v.cpu().numpy() for k, v in g.items()}
+
+
+@pytest.fixture(autouse=True)
+def _reset_block_size():
+    yield
+    triples.set_block_size(0)
+
+
+@pytest.mark.parametrize("precision", ["mixed", "mixed_bf16"])
+@pytest.mark.parametrize("name", ["o5v19_fvo", "o4v9_fvo", "o6v2", "o7v13_scaled", "o3v4_fvo"])
+def test_mixed_vs_reference_golden(name, precision):
+    inp, e_ref, g_ref, z = G.load(name)
+    e, g = _run(inp, True, precision)
+    te, tg = TOL[precision]
+    assert abs(e - e_ref) <= te * abs(e_ref) + 1e-14, (e, e_ref)
+    for k in G.KEYS:
+        ref = z["cot_ovvv_tril"] if k == "ovvv" else g_ref[k]
+        assert _relerr(g[k], ref) < tg, (k, _relerr(g[k], ref))
+
+
+@pytest.mark.parametrize("tv", [3, 7])
+def test_mixed_block_sizes(tv):
+    triples.set_block_size(tv)
+    inp, e_ref, g_ref, _ = G.load("o4v9_fvo")
+    e, g = _run(inp, False, "mixed")
+    assert abs(e - e_ref) <= 1e-6 * abs(e_ref)
+    for k in G.KEYS:
+        assert _relerr(g[k], g_ref[k]) < 1e-5, k
+
+
+@pytest.mark.parametrize("o,v,naux,seed", [(8, 40, 60, 21), (12, 33, 50, 22)])
+def test_mixed_random_vs_oracle(o, v, naux, seed):
+    inp = make_inputs(o, v, naux, seed=seed, fvo_sigma=1e-3)
+    e_ref, g_ref = O.oracle_energy_vjp(inp)
+    e, g = _run(inp, False, "mixed")
+    assert abs(e - e_ref) <= 1e-6 * abs(e_ref)
+    for k in G.KEYS:
+        assert _relerr(g[k], g_ref[k]) < 1e-5, k

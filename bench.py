@@ -1,0 +1,367 @@
+"""Benchmark: CCSD(T) energy + VJP throughput on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision mixed|mixed_bf16|fp64] [--workload NAME]
+
+One step = E(T) plus its full VJP (ybar = 1) for one (T) problem of the
+workload's shape (default large_o40v360: nocc=40, nvir=360, naux=1200),
+seeded synthetic inputs with the reference benchmark's distributions.
+Metric: TFLOP/s at the algorithmic count 8*o^3*v^4 per step (forward
+2*o^3*v^4 + backward with recompute 6*o^3*v^4).
+
+Multi-GPU: the (T) problem of this workload fits one GPU, so --gpus N runs N
+independent replicas (one process per GPU under torchrun); value = N
+problems / max-over-ranks time ("weak" scaling).  No data-path collective.
+
+--impl reference times the reference's own CPU kernels (compiled from its
+sources into oracle/_ref) on the host cores on a bounded job sample and
+extrapolates to the full workload; rank 0 alone runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "(T) E+VJP TFLOP/s (o=40,v=360): mixed-prec vs FP64 on B200 at |dE|<=1e-7 Eh"
+WORKLOADS = {
+    "water_ccpvdz_o5v19": (5, 19, 80),
+    "medium_o20v180": (20, 180, 600),
+    "large_o40v360": (40, 360, 1200),
+    "huge_o50v450": (50, 450, 1500),
+}
+DATA = ("synthetic: seeded mo_energy occ~U(-1.5,-0.3) vir~U(0.2,3.0) sorted, t1~N(0,1e-2), "
+        "t2~N(0,2e-2) symmetrised, ERIs from Cholesky-like factors L~N(0,0.1) (naux), fvo=0, "
+        "packed ovvv")
+
+
+def _env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def algorithmic_flops(o, v):
+    """Per step and per kernel class (the tensor contractions only)."""
+    main = 2.0 * o ** 3 * v ** 4
+    ooov = 2.0 * o ** 4 * v ** 3
+    return {
+        "step": 8.0 * o ** 3 * v ** 4,
+        "f1_contract": main + ooov,
+        "b1a_ovvv_grad": main,
+        "b1b_t2_grad": main,
+        "b1c_ovoo_grad": ooov,
+        "b1d_t2_ooov_grad": ooov,
+    }
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        loaded = [x for x in sm if x > 0.5 * (smax or max(sm))] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU legs (reference kernels from oracle/_ref)
+# ---------------------------------------------------------------------------
+def cpu_reference_measure(o, v, target_s=8.0):
+    cores = os.cpu_count() or 1
+    env = dict(os.environ, OMP_NUM_THREADS=str(cores), OPENBLAS_NUM_THREADS="1")
+    env.pop("CUDA_VISIBLE_DEVICES", None)
+    try:
+        out = subprocess.run([sys.executable, os.path.join(ROOT, "oracle", "cpu_baseline.py"), str(o), str(v),
+                              "--target", str(target_s)], env=env, capture_output=True, text=True,
+                             timeout=900, check=True)
+        return json.loads(out.stdout.strip().splitlines()[-1])
+    except Exception as exc:  # noqa: BLE001 - reported, not fatal for the GPU line
+        return {"error": f"{type(exc).__name__}: {exc}"[:300]}
+
+
+def run_reference(args, o, v, rank):
+    if rank != 0:
+        return
+    res = None
+    times = []
+    for i in range(args.warmup + args.steps):
+        res = cpu_reference_measure(o, v, args.cpu_target)
+        if "error" in res:
+            print(json.dumps({"impl": "reference", "unavailable": res["error"]}))
+            return
+        if i >= args.warmup:
+            times.append(res["t_full_s"])
+    t = max(times)
+    flops = algorithmic_flops(o, v)["step"]
+    val = flops / t / 1e12
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": "TFLOP/s", "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA,
+        "config": {"workload": args.workload, "nocc": o, "nvir": v, "naux": WORKLOADS[args.workload][2],
+                   "path": "reference CPU C kernels (ccsd_t_energy_vjp + LNO forward with mat=I)"},
+        "cpu_baseline": {"value": val, "unit": "TFLOP/s", "cores": res["cores"], "kind": "reference",
+                         "sample": res["sample"]},
+        "e2e": {"value": val, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# GPU leg
+# ---------------------------------------------------------------------------
+def load_traffic(workload, precision):
+    path = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d.get(f"{workload}:{precision}", {})
+    except (OSError, ValueError):
+        return {}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "mixed_bf16", "fp64"])
+    ap.add_argument("--workload", default="large_o40v360", choices=sorted(WORKLOADS))
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--cpu-target", type=float, default=8.0, help="seconds per CPU backward sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = _env_int("WORLD_SIZE", 1)
+    rank = _env_int("RANK", 0)
+    local_rank = _env_int("LOCAL_RANK", 0)
+    o, v, naux = WORKLOADS[args.workload]
+
+    if args.impl == "reference":
+        run_reference(args, o, v, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+
+    from pyscfad_b200 import _lib, triples
+    from pyscfad_b200.synthetic import make_inputs_torch
+
+    lib = _lib.load()
+    inp = make_inputs_torch(o, v, naux, seed=args.seed + rank, device=dev)
+    il, jl = torch.tril_indices(v, v, device=dev)
+    inp["ovvv"] = inp["ovvv"][:, :, il, jl].contiguous()   # packed DF layout (dfccsd.py:88)
+    keys = triples.KEYS
+    dev_args = [inp[k] for k in keys]
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def step():
+        e, g = triples.energy_vjp(*dev_args, ybar=1.0, precision=args.precision, device=dev, check=False)
+        return e, g
+
+    # warm-up
+    for _ in range(args.warmup):
+        e, g = step()
+    torch.cuda.synchronize()
+    st = _lib.load().triples_check_device_status(torch.cuda.current_stream(dev).cuda_stream,
+                                                 triples._workspaces[(dev.type, dev.index)].data_ptr())
+    _lib.check(st, "warm-up")
+    e_val = float(e)
+    del g
+
+    # timed region: inputs resident in HBM
+    clocks = ClockSampler(local_rank)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    lib.triples_profile_enable(1)
+    s0 = torch.cuda.Event(enable_timing=True)
+    s1 = torch.cuda.Event(enable_timing=True)
+    s0.record()
+    for _ in range(args.steps):
+        e, g = step()
+    s1.record()
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    import ctypes
+    ncat = 16
+    ms = (ctypes.c_double * ncat)()
+    cnt = (ctypes.c_int * ncat)()
+    ncat = lib.triples_profile_read(ncat, ms, cnt)
+    lib.triples_profile_enable(0)
+    prof = {lib.triples_profile_name(i).decode(): (ms[i], cnt[i]) for i in range(ncat)}
+    t_dev = s0.elapsed_time(s1) / 1e3
+    if world > 1:
+        t = torch.tensor([t_dev], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_dev = float(t)
+    _lib.check(triples.device_status(dev), "timed steps")
+    del g
+
+    flops = algorithmic_flops(o, v)
+    value = world * args.steps * flops["step"] / t_dev / 1e12
+
+    # end-to-end through the public API with host buffers
+    host_in = [a.cpu().pin_memory() for a in dev_args]
+    h2d = sum(a.numel() * a.element_size() for a in host_in)
+    grads_host = None
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    d2h = 0
+    for _ in range(args.steps):
+        dev_in = [a.to(dev, non_blocking=True) for a in host_in]
+        ee, gg = triples.energy_vjp(*dev_in, ybar=1.0, precision=args.precision, device=dev, check=False)
+        if grads_host is None:
+            grads_host = {k: torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for k, t in gg.items()}
+            e_host = torch.empty((), dtype=torch.float64, pin_memory=True)
+        e_host.copy_(ee, non_blocking=True)
+        for k in keys:
+            grads_host[k].copy_(gg[k], non_blocking=True)
+        d2h = 8 + sum(t.numel() * t.element_size() for t in gg.values())
+        del dev_in, gg
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    t_e2e = e0.elapsed_time(e1) / 1e3
+    if world > 1:
+        t = torch.tensor([t_e2e], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t)
+    e2e_value = world * args.steps * flops["step"] / t_e2e / 1e12
+
+    # roofline of the dominant kernel class
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except (OSError, ValueError):
+        pass
+    dom = max((k for k in prof if k in flops), key=lambda k: prof[k][0], default=None)
+    roof = None
+    if dom and prof[dom][0] > 0:
+        per_launch_flops = flops[dom] * args.steps / max(prof[dom][1], 1)
+        avg_s = prof[dom][0] / 1e3 / max(prof[dom][1], 1)
+        achieved = per_launch_flops / avg_s / 1e12
+        traffic = load_traffic(args.workload, args.precision).get(dom)
+        if args.precision == "fp64":
+            peak, note = 40.0, "nominal B200 FP64 (no measured FP64 peak on this pool)"
+        elif "bf16_tflops_sustained" in peaks:
+            peak, note = float(peaks["bf16_tflops_sustained"]), "of measured (cuBLAS bf16, sustained)"
+        else:
+            peak, note = 1400.0, "of fallback (sustained)"
+        roof = {"bound": "tensor", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_note": note,
+                "launches": prof[dom][1], "avg_launch_ms": avg_s * 1e3}
+        if args.precision != "fp64":
+            roof["split_products"] = 3
+            roof["peak_emulated"] = peak / 3
+            roof["frac_emulated"] = achieved / (peak / 3)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_dev / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else (
+            "fp16x3-split f32acc, f64 epilogue" if args.precision == "mixed" else "bf16x3-split f32acc, f64 epilogue"),
+        "data": DATA,
+        "config": {"workload": args.workload, "nocc": o, "nvir": v, "naux": naux, "precision": args.precision,
+                   "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (packed ovvv %.1f GB)" % (inp["ovvv"].numel() * 8 / 1e9),
+                   "e_t": e_val},
+        "e2e": {"value": e2e_value, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(sum(c for _, c in prof.values())),
+        "kernel_ms": {k: round(m, 3) for k, (m, _) in prof.items()},
+        "roofline": roof,
+        "clocks": clk,
+    }
+    if rank == 0 and not args.no_cpu_baseline and world == 1:
+        res = cpu_reference_measure(o, v, args.cpu_target)
+        if "error" in res:
+            line["cpu_baseline"] = {"value": None, "unit": "TFLOP/s", "error": res["error"]}
+        else:
+            line["cpu_baseline"] = {"value": res["tflops"], "unit": "TFLOP/s", "cores": res["cores"],
+                                    "kind": "reference", "sample": res["sample"]}
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -103,6 +103,15 @@ int triples_last_cuda_error(void);
  * performance, not results beyond FP64 summation order. */
 void triples_set_block_size(int tv);
 
+/* Measurement: when enabled, every kernel launched by the calls above is
+ * bracketed by CUDA events on the caller's stream (enabling clears earlier
+ * records).  triples_profile_read() synchronises on those events and fills
+ * per-category totals (milliseconds, launch counts) for up to max_categories
+ * categories; it returns the number of categories, or -1 on error. */
+void triples_profile_enable(int on);
+int triples_profile_read(int max_categories, double *ms, int *launches);
+const char *triples_profile_name(int category);
+
 /* Version of this library, e.g. "0.1.0". */
 const char *triples_version(void);
 

@@ -53,6 +53,12 @@ def load():
     lib.triples_version.restype = ctypes.c_char_p
     lib.triples_check_device_status.restype = _c_int
     lib.triples_check_device_status.argtypes = [_vp, _vp]
+    lib.triples_profile_enable.restype = None
+    lib.triples_profile_enable.argtypes = [_c_int]
+    lib.triples_profile_read.restype = _c_int
+    lib.triples_profile_read.argtypes = [_c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_c_int)]
+    lib.triples_profile_name.restype = ctypes.c_char_p
+    lib.triples_profile_name.argtypes = [_c_int]
     lib.triples_set_block_size.restype = None
     lib.triples_set_block_size.argtypes = [_c_int]
     _lib = lib

@@ -72,8 +72,40 @@ struct ChunkDesc {
 };
 
 struct Dims {
-    int o, v, n, Kp, Tv;
+    int o, v, n, Kp, Tv;   // Tv: power-of-two block size
 };
+
+// Virtual blocks: v / Tv full blocks of Tv, then the remainder split into
+// descending powers of two (so every block size divides 64).
+__host__ __device__ inline int num_blocks(const Dims &d) {
+    int nfull = d.v / d.Tv, rem = d.v - nfull * d.Tv, n = nfull;
+    for (int bit = d.Tv >> 1; bit > 0; bit >>= 1)
+        if (rem & bit) n++;
+    return n;
+}
+__host__ __device__ inline int block_size(const Dims &d, int b) {
+    int nfull = d.v / d.Tv;
+    if (b < nfull) return d.Tv;
+    int rem = d.v - nfull * d.Tv, k = b - nfull;
+    for (int bit = d.Tv >> 1; bit > 0; bit >>= 1)
+        if (rem & bit) {
+            if (k == 0) return bit;
+            --k;
+        }
+    return 0;
+}
+__host__ __device__ inline int block_start(const Dims &d, int b) {
+    int nfull = d.v / d.Tv;
+    if (b <= nfull) return b * d.Tv;
+    int s = nfull * d.Tv, rem = d.v - s, k = b - nfull;
+    for (int bit = d.Tv >> 1; bit > 0; bit >>= 1)
+        if (rem & bit) {
+            if (k == 0) return s;
+            s += bit;
+            --k;
+        }
+    return s;
+}
 
 // The six orderings of three slots, lexicographic: index = 2*first + (second is
 // the larger of the two remaining).

@@ -14,6 +14,7 @@
 
 #include "gemm_fp64.cuh"
 #include "tc_f1.cuh"
+#include "f2.cuh"
 #include "pyscfad_b200.h"
 #include "triples_internal.h"
 
@@ -34,24 +35,72 @@ static int g_tv_override = 0;
 #define TB_LAUNCH_CHECK() TB_CUDA(cudaGetLastError())
 
 // ---------------------------------------------------------------------------
+// optional per-kernel-class timing with CUDA events (on the launch stream)
+// ---------------------------------------------------------------------------
+enum ProfCat { P_PREP = 0, P_F1, P_F2, P_VGRAD, P_B1A, P_B1B, P_B1C, P_B1D, P_FOLD, P_NCAT };
+static const char *kProfNames[P_NCAT] = {"prep", "f1_contract", "f2_epilogue", "vgrad",
+                                         "b1a_ovvv_grad", "b1b_t2_grad", "b1c_ovoo_grad",
+                                         "b1d_t2_ooov_grad", "fold"};
+struct ProfRec {
+    int cat;
+    cudaEvent_t a, b;
+};
+static bool g_prof = false;
+static std::vector<ProfRec> g_prof_recs;
+static std::vector<cudaEvent_t> g_event_pool;
+static size_t g_pool_used = 0;
+
+static cudaEvent_t prof_event() {
+    if (g_pool_used == g_event_pool.size()) {
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        g_event_pool.push_back(e);
+    }
+    return g_event_pool[g_pool_used++];
+}
+
+template <typename F>
+static void prof_wrap(int cat, cudaStream_t st, F &&launch) {
+    cudaEvent_t a = nullptr;
+    if (g_prof) {
+        a = prof_event();
+        cudaEventRecord(a, st);
+    }
+    launch();
+    if (g_prof) {
+        cudaEvent_t b = prof_event();
+        cudaEventRecord(b, st);
+        g_prof_recs.push_back({cat, a, b});
+    }
+}
+
+#define TB_KLAUNCH(cat, ...)                              \
+    do {                                                  \
+        prof_wrap((cat), st, [&]() { __VA_ARGS__; });     \
+        TB_LAUNCH_CHECK();                                \
+    } while (0)
+
+// ---------------------------------------------------------------------------
 // planning
 // ---------------------------------------------------------------------------
 static int choose_tv(int o, int v) {
     int tv = g_tv_override > 0 ? g_tv_override : 16;
     if (tv > kMaxTv) tv = kMaxTv;
-    if (tv * o > kMaxCols) tv = kMaxCols / o;
-    return tv < v ? tv : v;
+    while (tv > 1 && tv * o > kMaxCols) tv >>= 1;
+    int p2 = 1;   // largest power of two <= tv
+    while (p2 * 2 <= tv) p2 *= 2;
+    return p2;
 }
 
 static inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 static void make_chunk(const Dims &d, int A, int B, int C, ChunkDesc &ch) {
     const int blks[3] = {A, B, C};
-    auto bsize = [&](int b) { int lo = b * d.Tv; int hi = lo + d.Tv; if (hi > d.v) hi = d.v; return hi - lo; };
+    auto bsize = [&](int b) { return block_size(d, b); };
     for (int t = 0; t < 3; t++) {
         ch.blk[t] = blks[t];
         ch.nabc[t] = bsize(blks[t]);
-        ch.base[t] = blks[t] * d.Tv;
+        ch.base[t] = block_start(d, blks[t]);
     }
     ch.nperm = 0;
     long long off = 0;
@@ -66,9 +115,9 @@ static void make_chunk(const Dims &d, int A, int B, int C, ChunkDesc &ch) {
         if (dup) continue;
         PermBlock &pb = ch.pb[ch.nperm++];
         pb.bx = bx; pb.by = by; pb.bz = bz;
-        pb.X0 = bx * d.Tv; pb.Tx = bsize(bx);
-        pb.Y0 = by * d.Tv; pb.Ty = bsize(by);
-        pb.Z0 = bz * d.Tv; pb.Tz = bsize(bz);
+        pb.X0 = block_start(d, bx); pb.Tx = bsize(bx);
+        pb.Y0 = block_start(d, by); pb.Ty = bsize(by);
+        pb.Z0 = block_start(d, bz); pb.Tz = bsize(bz);
         pb.soff = off;
         off += (o3 * pb.Tx * pb.Ty * pb.Tz + 15) / 16 * 16;   // 64 B aligned sub-buffers
     }
@@ -96,7 +145,7 @@ int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan
     d.Kp = nvir;
     P.Kp8 = (nvir + 7) / 8 * 8;
     P.Op8 = (nocc + 7) / 8 * 8;
-    P.nb = (nvir + d.Tv - 1) / d.Tv;
+    P.nb = num_blocks(d);
     P.n_ijk = nocc * (nocc + 1) * (nocc + 2) / 6;
     long long maxst = 0;
     int maxitems = 0;
@@ -112,7 +161,7 @@ int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan
             }
     P.stage_elems = (size_t)maxst;
     P.max_items = maxitems;
-    P.f2_gy = (maxitems + kF2Threads - 1) / kF2Threads;
+    P.f2_gy = kMaxSub;
     const bool mixed = precision != TRIPLES_PRECISION_FP64;
     P.stage_bytes = mixed ? sizeof(float) : sizeof(double);
 
@@ -133,7 +182,7 @@ int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan
     }
     P.off_S = take(P.stage_elems * P.stage_bytes);
     if (want_grad) {
-        P.off_SV = take(P.stage_elems * P.stage_bytes);
+        P.off_SW = take(P.stage_elems * P.stage_bytes);
         P.off_GA1 = take(v * o * v * Kp * el);
         P.off_GB1 = take(o * o * v * Kp * el);
         P.off_GA2 = take(o * o * v * o * el);
@@ -438,8 +487,10 @@ __global__ void __launch_bounds__(256) k_b1a_fp64(GemmLaunch<StageT> L) {
     g.N = v;
     g.K = o * o * pb.Tz;
     g.K2 = 0;
-    g.A = GOpT<StageT>{L.S + pb.soff + (long long)y * pb.Tx * oTz, map2(pb.Tx, oTz, (long long)o * sq),
-              map2((int)oTz, 1, sq), 1};
+    const long long s_r = pb.Tz, s_q = (long long)o * pb.Tz, s_x = (long long)o * o * pb.Tz;
+    const long long s_p = (long long)pb.Tx * s_x, s_y = (long long)o * s_p;
+    (void)s_r;
+    g.A = GOpT<StageT>{L.S + pb.soff + (long long)y * s_y, map2(pb.Tx, s_x, s_p), map1(1), 1};
     g.B = GOp{L.B1 + (long long)pb.Z0 * Kp, map1(1),
               map3(pb.Tz, o, Kp, (long long)v * Kp, (long long)o * v * Kp), 0};
     g.C = L.G + (((long long)pb.Y0 + y) * o * v + pb.X0) * Kp;
@@ -468,8 +519,10 @@ __global__ void __launch_bounds__(256) k_b1b_fp64(GemmLaunch<StageT> L) {
     g.N = v;
     g.K = pb.Ty * o * pb.Tx;
     g.K2 = 0;
-    g.A = GOpT<StageT>{L.S + pb.soff + (long long)q * sq, map1(1),
-              map3(pb.Tx, o, oTz, (long long)o * sq, (long long)pb.Tx * oTz), 0};
+    const long long s_r = pb.Tz, s_q = (long long)o * pb.Tz, s_x = (long long)o * o * pb.Tz;
+    const long long s_p = (long long)pb.Tx * s_x, s_y = (long long)o * s_p;
+    (void)s_r;
+    g.A = GOpT<StageT>{L.S + pb.soff + (long long)q * s_q, map1(1), map3(pb.Tx, o, s_x, s_p, s_y), 0};
     g.B = GOp{L.A1 + ((long long)pb.Y0 * o * v + pb.X0) * Kp, map1(1),
               map3(pb.Tx, o, Kp, (long long)v * Kp, (long long)o * v * Kp), 0};
     g.C = L.G + ((long long)q * o * v + pb.Z0) * Kp;
@@ -498,8 +551,10 @@ __global__ void __launch_bounds__(256) k_b1c_fp64(GemmLaunch<StageT> L) {
     g.N = o;
     g.K = pb.Ty * o * pb.Tz;
     g.K2 = 0;
-    g.A = GOpT<StageT>{L.S + pb.soff + (long long)q * sq, map2(pb.Tx, oTz, (long long)o * sq),
-              map2((int)oTz, 1, (long long)pb.Tx * oTz), 1};
+    const long long s_r = pb.Tz, s_q = (long long)o * pb.Tz, s_x = (long long)o * o * pb.Tz;
+    const long long s_p = (long long)pb.Tx * s_x, s_y = (long long)o * s_p;
+    (void)s_r;
+    g.A = GOpT<StageT>{L.S + pb.soff + (long long)q * s_q, map2(pb.Tx, s_x, s_p), map2((int)oTz, 1, s_y), 1};
     g.B = GOp{L.B2 + ((long long)pb.Y0 * o * v + pb.Z0) * o, map1(1),
               map3(pb.Tz, o, o, (long long)v * o, (long long)o * v * o), 0};
     g.C = L.G + ((long long)q * o * v + pb.X0) * o;
@@ -530,8 +585,10 @@ __global__ void __launch_bounds__(256) k_b1d_fp64(GemmLaunch<StageT> L) {
     g.N = o;
     g.K = o * o * pb.Tx;
     g.K2 = 0;
-    g.A = GOpT<StageT>{L.S + pb.soff + (long long)y * pb.Tx * oTz, map1(1),
-              map3(pb.Tx, o, oTz, (long long)o * sq, sq), 0};
+    const long long s_r = pb.Tz, s_q = (long long)o * pb.Tz, s_x = (long long)o * o * pb.Tz;
+    const long long s_p = (long long)pb.Tx * s_x, s_y = (long long)o * s_p;
+    (void)s_r;
+    g.A = GOpT<StageT>{L.S + pb.soff + (long long)y * s_y, map1(1), map3(pb.Tx, o, s_x, s_p, s_q), 0};
     g.B = GOp{L.A2 + (long long)pb.X0 * o, map1(1),
               map3(pb.Tx, o, o, (long long)v * o, (long long)o * v * o), 0};
     g.C = L.G + (((long long)pb.Y0 + y) * o * v + pb.Z0) * o;
@@ -543,203 +600,6 @@ __global__ void __launch_bounds__(256) k_b1d_fp64(GemmLaunch<StageT> L) {
     const int m0 = blockIdx.x * kGBM, n0 = blockIdx.y * kGBN;
     if (m0 >= g.M || n0 >= g.N) return;
     gemm_fp64_tile(g, m0, n0, sm);
-}
-
-// ---------------------------------------------------------------------------
-// chunk epilogue: energy, adjoint of the raw amplitudes, mo_energy gradient
-// ---------------------------------------------------------------------------
-template <typename StageT>
-struct F2Params {
-    Dims d;
-    ChunkDesc ch;
-    const int *ijk;
-    const double *mo_e, *t1, *t2, *ovov, *fvo;
-    StageT *S;    // raw W in, Wbar out (in place)
-    StageT *SV;   // Vbar out
-    double ybar;
-    int want_grad;
-    double *e_part, *e_acc;
-    unsigned *counter;
-    double *mo_bar;
-};
-
-template <typename StageT>
-__device__ __forceinline__ long long stage_pos(const F2Params<StageT> &P, int p, int q, int r,
-                                               int x, int y, int z) {
-    const int Tv = P.d.Tv, o = P.d.o;
-    const int bx = x / Tv, by = y / Tv, bz = z / Tv;
-    int t = 0;
-#pragma unroll 1
-    for (; t < P.ch.nperm - 1; t++)
-        if (P.ch.pb[t].bx == bx && P.ch.pb[t].by == by && P.ch.pb[t].bz == bz) break;
-    const PermBlock &pb = P.ch.pb[t];
-    return pb.soff +
-           ((((long long)(p * o + q) * pb.Ty + (y - pb.Y0)) * pb.Tx + (x - pb.X0)) * o + r) * pb.Tz +
-           (z - pb.Z0);
-}
-
-template <typename StageT>
-__global__ void __launch_bounds__(kF2Threads) k_f2(F2Params<StageT> P) {
-    const Dims &d = P.d;
-    const int o = d.o, v = d.v;
-    __shared__ double s_evir[3 * kMaxTv];
-    __shared__ double s_red[2][kF2Threads / 32];
-    for (int e = threadIdx.x; e < 3 * kMaxTv; e += blockDim.x) s_evir[e] = 0.0;
-    __syncthreads();
-
-    const int rep = blockIdx.x;
-    const int ijk[3] = {P.ijk[3 * rep], P.ijk[3 * rep + 1], P.ijk[3 * rep + 2]};
-    const int nA = P.ch.nabc[0], nB = P.ch.nabc[1], nC = P.ch.nabc[2];
-    const int it = blockIdx.y * blockDim.x + threadIdx.x;
-    double e_loc = 0.0, dd_loc = 0.0;
-
-    int la = 0, lb = 0, lc = 0;
-    bool valid = it < nA * nB * nC;
-    if (valid) {
-        la = it / (nB * nC);
-        lb = (it / nC) % nB;
-        lc = it % nC;
-    }
-    const int abc[3] = {P.ch.base[0] + la, P.ch.base[1] + lb, P.ch.base[2] + lc};
-    if (valid && P.ch.blk[0] == P.ch.blk[1] && abc[0] < abc[1]) valid = false;
-    if (valid && P.ch.blk[1] == P.ch.blk[2] && abc[1] < abc[2]) valid = false;
-
-    if (valid) {
-        double WW[6], VV[6], X[6];
-#pragma unroll
-        for (int s = 0; s < 6; s++) {
-            int ps[3];
-            perm_of(s, ps);
-            const int dd[3] = {abc[ps[0]], abc[ps[1]], abc[ps[2]]};
-            double sw = 0.0, sv = 0.0;
-#pragma unroll
-            for (int tau = 0; tau < 6; tau++) {
-                int pt[3];
-                perm_of(tau, pt);
-                const int p = ijk[pt[0]], q = ijk[pt[1]], r = ijk[pt[2]];
-                const int x = dd[pt[0]], y = dd[pt[1]], z = dd[pt[2]];
-                sw += (double)P.S[stage_pos(P, p, q, r, x, y, z)];
-                sv += P.ovov[(((long long)p * v + x) * o + q) * v + y] * P.t1[(long long)r * v + z] +
-                      P.t2[(((long long)q * o + p) * v + y) * v + x] * P.fvo[(long long)z * o + r];
-            }
-            WW[s] = sw;
-            VV[s] = sv;
-            X[s] = sw + 0.5 * sv;
-        }
-        double Z[6], RW[6];
-#pragma unroll
-        for (int s = 0; s < 6; s++) {
-            Z[s] = 4.0 * X[s] + X[perm_compose(s, 4)] + X[perm_compose(s, 3)] -
-                   2.0 * (X[perm_compose(s, 5)] + X[perm_compose(s, 1)] + X[perm_compose(s, 2)]);
-            RW[s] = 4.0 * WW[s] + WW[perm_compose(s, 4)] + WW[perm_compose(s, 3)] -
-                    2.0 * (WW[perm_compose(s, 5)] + WW[perm_compose(s, 1)] + WW[perm_compose(s, 2)]);
-        }
-        const int i = ijk[0], j = ijk[1], k = ijk[2];
-        const int a = abc[0], b = abc[1], c = abc[2];
-        const int n_ijk = (i == k) ? 1 : ((i == j || j == k) ? 3 : 6);
-        const int n_abc = (a == c) ? 1 : ((a == b || b == c) ? 3 : 6);
-        const double cfac = (double)(n_ijk * n_abc) / 18.0;
-        const double Dn = P.mo_e[i] + P.mo_e[j] + P.mo_e[k] - P.mo_e[o + a] - P.mo_e[o + b] -
-                          P.mo_e[o + c];
-        const double rD = 1.0 / Dn;
-        double esum = 0.0;
-#pragma unroll
-        for (int s = 0; s < 6; s++) esum += WW[s] * Z[s];
-        e_loc = cfac * esum * rD;
-        if (P.want_grad) {
-            const double g0 = P.ybar * cfac * rD;
-            double gW[6], gV[6];
-#pragma unroll
-            for (int s = 0; s < 6; s++) {
-                gW[s] = g0 * (Z[s] + RW[s]);
-                gV[s] = g0 * 0.5 * RW[s];
-            }
-            const double dD = -P.ybar * cfac * esum * rD * rD;
-            dd_loc = dD;
-            // zero all raw positions of this orbit, then accumulate (duplicates
-            // occur when indices coincide)
-#pragma unroll 1
-            for (int pass = 0; pass < 2; pass++) {
-#pragma unroll
-                for (int s = 0; s < 6; s++) {
-                    int ps[3];
-                    perm_of(s, ps);
-                    const int dd[3] = {abc[ps[0]], abc[ps[1]], abc[ps[2]]};
-#pragma unroll
-                    for (int tau = 0; tau < 6; tau++) {
-                        int pt[3];
-                        perm_of(tau, pt);
-                        long long pos = stage_pos(P, ijk[pt[0]], ijk[pt[1]], ijk[pt[2]], dd[pt[0]],
-                                                  dd[pt[1]], dd[pt[2]]);
-                        if (pass == 0) {
-                            P.S[pos] = (StageT)0;
-                            P.SV[pos] = (StageT)0;
-                        } else {
-                            P.S[pos] = (StageT)((double)P.S[pos] + gW[s]);
-                            P.SV[pos] = (StageT)((double)P.SV[pos] + gV[s]);
-                        }
-                    }
-                }
-            }
-            // virtual part of the mo_energy gradient
-            for (int t = 0; t < 3; t++) {
-                int slot = (P.ch.blk[t] == P.ch.blk[0]) ? 0 : ((P.ch.blk[t] == P.ch.blk[1]) ? 1 : 2);
-                atomicAdd(&s_evir[slot * kMaxTv + (abc[t] - P.ch.base[slot])], -dD);
-            }
-        }
-    }
-
-    // block reductions
-    for (int off = 16; off > 0; off >>= 1) {
-        e_loc += __shfl_down_sync(0xffffffffu, e_loc, off);
-        dd_loc += __shfl_down_sync(0xffffffffu, dd_loc, off);
-    }
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (lane == 0) {
-        s_red[0][warp] = e_loc;
-        s_red[1][warp] = dd_loc;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double es = 0.0, ds = 0.0;
-        for (int w = 0; w < kF2Threads / 32; w++) {
-            es += s_red[0][w];
-            ds += s_red[1][w];
-        }
-        P.e_part[blockIdx.y * gridDim.x + blockIdx.x] = es;
-        if (P.want_grad && ds != 0.0) {
-            atomicAdd(&P.mo_bar[ijk[0]], ds);
-            atomicAdd(&P.mo_bar[ijk[1]], ds);
-            atomicAdd(&P.mo_bar[ijk[2]], ds);
-        }
-    }
-    if (P.want_grad) {
-        for (int e = threadIdx.x; e < 3 * kMaxTv; e += blockDim.x) {
-            int slot = e / kMaxTv, l = e % kMaxTv;
-            if (l < P.ch.nabc[slot] && s_evir[e] != 0.0) {
-                bool dup = (slot == 1 && P.ch.blk[1] == P.ch.blk[0]) ||
-                           (slot == 2 && (P.ch.blk[2] == P.ch.blk[0] || P.ch.blk[2] == P.ch.blk[1]));
-                if (!dup) atomicAdd(&P.mo_bar[o + P.ch.base[slot] + l], s_evir[e]);
-            }
-        }
-    }
-    // deterministic chunk energy: the last block sums the block partials in order
-    __shared__ bool s_last;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned prev = atomicAdd(P.counter, 1u);
-        s_last = (prev == gridDim.x * gridDim.y - 1);
-    }
-    __syncthreads();
-    if (s_last && threadIdx.x == 0) {
-        __threadfence();
-        double tot = 0.0;
-        const int nblk = gridDim.x * gridDim.y;
-        for (int bidx = 0; bidx < nblk; bidx++) tot += ((volatile double *)P.e_part)[bidx];
-        P.e_acc[0] += tot;
-        *P.counter = 0u;
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -960,6 +820,15 @@ static int num_sms() {
 
 template <typename StageT>
 static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
+    constexpr int kSB = sizeof(StageT) == 4 ? 8 : 4;   // epilogue sub-block edge
+    {
+        static bool f2_attr = false;
+        if (!f2_attr) {
+            TB_CUDA(cudaFuncSetAttribute(k_f2t<StageT, kSB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)f2_smem_bytes<StageT, kSB>()));
+            f2_attr = true;
+        }
+    }
     const Dims d = P.d;
     const bool mixed = P.prec != TRIPLES_PRECISION_FP64;
     const bool bf16 = P.prec == TRIPLES_PRECISION_MIXED_BF16;
@@ -970,7 +839,7 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
     double *A2 = (double *)(ws + P.off_A2);
     double *B2 = (double *)(ws + P.off_B2);
     StageT *S = (StageT *)(ws + P.off_S);
-    StageT *SV = P.want_grad ? (StageT *)(ws + P.off_SV) : nullptr;
+    void *SW = P.want_grad ? (void *)(ws + P.off_SW) : nullptr;
     double *GA1 = P.want_grad ? (double *)(ws + P.off_GA1) : nullptr;
     double *GB1 = P.want_grad ? (double *)(ws + P.off_GB1) : nullptr;
     double *GA2 = P.want_grad ? (double *)(ws + P.off_GA2) : nullptr;
@@ -980,8 +849,7 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
     const size_t o = d.o, v = d.v, n = d.n;
 
     TB_CUDA(cudaMemsetAsync(ctrl, 0, kCtrlBytes, st));
-    k_ijk_table<<<grid1d(P.n_ijk, 128), 128, 0, st>>>(d.o, ijk);
-    TB_LAUNCH_CHECK();
+    TB_KLAUNCH(P_PREP, k_ijk_table<<<grid1d(P.n_ijk, 128), 128, 0, st>>>(d.o, ijk));
     if (P.want_grad) {
         TB_CUDA(cudaMemsetAsync(GA1, 0, v * o * v * d.Kp * sizeof(double), st));
         TB_CUDA(cudaMemsetAsync(GB1, 0, o * o * v * d.Kp * sizeof(double), st));
@@ -995,47 +863,42 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
     }
 
     // FP64 operand layouts (used by the FP64 contractions)
-    k_prep_A1<<<dim3((d.Kp + 31) / 32, (d.v + 31) / 32, (unsigned)(o * v)), dim3(32, 8), 0, st>>>(
-        io.ovvv, P.packed, d, A1);
-    TB_LAUNCH_CHECK();
-    k_prep_B1<<<(unsigned)(o * o * v), 128, 0, st>>>(io.t2, d, B1);
-    TB_LAUNCH_CHECK();
-    k_prep_A2<<<grid1d((long long)o * o * v * o, 256), 256, 0, st>>>(io.ovoo, d, A2);
-    TB_LAUNCH_CHECK();
-    k_prep_B2<<<grid1d((long long)v * o * v * o, 256), 256, 0, st>>>(io.t2, d, B2);
-    TB_LAUNCH_CHECK();
+    TB_KLAUNCH(P_PREP, k_prep_A1<<<dim3((d.Kp + 31) / 32, (d.v + 31) / 32, (unsigned)(o * v)), dim3(32, 8), 0, st>>>(
+        io.ovvv, P.packed, d, A1));
+    TB_KLAUNCH(P_PREP, k_prep_B1<<<(unsigned)(o * o * v), 128, 0, st>>>(io.t2, d, B1));
+    TB_KLAUNCH(P_PREP, k_prep_A2<<<grid1d((long long)o * o * v * o, 256), 256, 0, st>>>(io.ovoo, d, A2));
+    TB_KLAUNCH(P_PREP, k_prep_B2<<<grid1d((long long)v * o * v * o, 256), 256, 0, st>>>(io.t2, d, B2));
 
     // 16-bit split operands and tensor maps (tensor-core path)
     constexpr int BN = 256;
     CUtensorMap tmA1, tmB1, tmA2, tmB2;
     if (mixed) {
         const long long npair = (long long)v * (v + 1) / 2;
-        k_absmax<<<grid1d((long long)o * v * (P.packed ? npair : (long long)v * v), 256), 256, 0, st>>>(
-            io.ovvv, (long long)o * v * (P.packed ? npair : (long long)v * v), &ctrl->absmax[0]);
-        k_absmax<<<grid1d((long long)o * v * o * o, 256), 256, 0, st>>>(io.ovoo, (long long)o * v * o * o,
-                                                                         &ctrl->absmax[1]);
-        k_absmax<<<grid1d((long long)o * o * v * v, 256), 256, 0, st>>>(io.t2, (long long)o * o * v * v,
-                                                                         &ctrl->absmax[2]);
-        k_make_scales<<<1, 1, 0, st>>>(ctrl, bf16 ? 0 : 1);
-        TB_LAUNCH_CHECK();
+        TB_KLAUNCH(P_PREP, k_absmax<<<grid1d((long long)o * v * (P.packed ? npair : (long long)v * v), 256), 256, 0, st>>>(
+            io.ovvv, (long long)o * v * (P.packed ? npair : (long long)v * v), &ctrl->absmax[0]));
+        TB_KLAUNCH(P_PREP, k_absmax<<<grid1d((long long)o * v * o * o, 256), 256, 0, st>>>(io.ovoo, (long long)o * v * o * o,
+                                                                         &ctrl->absmax[1]));
+        TB_KLAUNCH(P_PREP, k_absmax<<<grid1d((long long)o * o * v * v, 256), 256, 0, st>>>(io.t2, (long long)o * o * v * v,
+                                                                         &ctrl->absmax[2]));
+        TB_KLAUNCH(P_PREP, k_make_scales<<<1, 1, 0, st>>>(ctrl, bf16 ? 0 : 1));
         if (bf16) {
-            k_prep_A1h<__nv_bfloat16><<<dim3((P.Kp8 + 31) / 32, (d.v + 31) / 32, (unsigned)(o * v)), dim3(32, 8), 0, st>>>(
-                io.ovvv, P.packed, d, P.Kp8, ctrl, (__nv_bfloat16 *)(ws + P.off_A1h));
-            k_prep_B1h<__nv_bfloat16><<<(unsigned)(o * o * v), 128, 0, st>>>(io.t2, d, P.Kp8, ctrl,
-                                                                            (__nv_bfloat16 *)(ws + P.off_B1h));
-            k_prep_A2h<__nv_bfloat16><<<grid1d((long long)o * o * v * P.Op8, 256), 256, 0, st>>>(
-                io.ovoo, d, P.Op8, ctrl, (__nv_bfloat16 *)(ws + P.off_A2h));
-            k_prep_B2h<__nv_bfloat16><<<grid1d((long long)v * o * v * P.Op8, 256), 256, 0, st>>>(
-                io.t2, d, P.Op8, ctrl, (__nv_bfloat16 *)(ws + P.off_B2h));
+            TB_KLAUNCH(P_PREP, k_prep_A1h<__nv_bfloat16><<<dim3((P.Kp8 + 31) / 32, (d.v + 31) / 32, (unsigned)(o * v)), dim3(32, 8), 0, st>>>(
+                io.ovvv, P.packed, d, P.Kp8, ctrl, (__nv_bfloat16 *)(ws + P.off_A1h)));
+            TB_KLAUNCH(P_PREP, k_prep_B1h<__nv_bfloat16><<<(unsigned)(o * o * v), 128, 0, st>>>(io.t2, d, P.Kp8, ctrl,
+                                                                            (__nv_bfloat16 *)(ws + P.off_B1h)));
+            TB_KLAUNCH(P_PREP, k_prep_A2h<__nv_bfloat16><<<grid1d((long long)o * o * v * P.Op8, 256), 256, 0, st>>>(
+                io.ovoo, d, P.Op8, ctrl, (__nv_bfloat16 *)(ws + P.off_A2h)));
+            TB_KLAUNCH(P_PREP, k_prep_B2h<__nv_bfloat16><<<grid1d((long long)v * o * v * P.Op8, 256), 256, 0, st>>>(
+                io.t2, d, P.Op8, ctrl, (__nv_bfloat16 *)(ws + P.off_B2h)));
         } else {
-            k_prep_A1h<__half><<<dim3((P.Kp8 + 31) / 32, (d.v + 31) / 32, (unsigned)(o * v)), dim3(32, 8), 0, st>>>(
-                io.ovvv, P.packed, d, P.Kp8, ctrl, (__half *)(ws + P.off_A1h));
-            k_prep_B1h<__half><<<(unsigned)(o * o * v), 128, 0, st>>>(io.t2, d, P.Kp8, ctrl,
-                                                                     (__half *)(ws + P.off_B1h));
-            k_prep_A2h<__half><<<grid1d((long long)o * o * v * P.Op8, 256), 256, 0, st>>>(
-                io.ovoo, d, P.Op8, ctrl, (__half *)(ws + P.off_A2h));
-            k_prep_B2h<__half><<<grid1d((long long)v * o * v * P.Op8, 256), 256, 0, st>>>(
-                io.t2, d, P.Op8, ctrl, (__half *)(ws + P.off_B2h));
+            TB_KLAUNCH(P_PREP, k_prep_A1h<__half><<<dim3((P.Kp8 + 31) / 32, (d.v + 31) / 32, (unsigned)(o * v)), dim3(32, 8), 0, st>>>(
+                io.ovvv, P.packed, d, P.Kp8, ctrl, (__half *)(ws + P.off_A1h)));
+            TB_KLAUNCH(P_PREP, k_prep_B1h<__half><<<(unsigned)(o * o * v), 128, 0, st>>>(io.t2, d, P.Kp8, ctrl,
+                                                                     (__half *)(ws + P.off_B1h)));
+            TB_KLAUNCH(P_PREP, k_prep_A2h<__half><<<grid1d((long long)o * o * v * P.Op8, 256), 256, 0, st>>>(
+                io.ovoo, d, P.Op8, ctrl, (__half *)(ws + P.off_A2h)));
+            TB_KLAUNCH(P_PREP, k_prep_B2h<__half><<<grid1d((long long)v * o * v * P.Op8, 256), 256, 0, st>>>(
+                io.t2, d, P.Op8, ctrl, (__half *)(ws + P.off_B2h)));
         }
         TB_LAUNCH_CHECK();
         {
@@ -1086,8 +949,7 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                     T.bf16 = bf16 ? 1 : 0;
                     const int tiles = T.cum[ch.nperm];
                     const int grid = tiles < num_sms() ? tiles : num_sms();
-                    k_f1_tc<BN><<<grid, 192, TcCfg<BN>::SMEM, st>>>(tmA1, tmB1, tmA2, tmB2, T);
-                    TB_LAUNCH_CHECK();
+                    TB_KLAUNCH(P_F1, k_f1_tc<BN><<<grid, 192, TcCfg<BN>::SMEM, st>>>(tmA1, tmB1, tmA2, tmB2, T));
                 } else {
                     GemmLaunch<double> L;
                     L.d = d;
@@ -1098,31 +960,51 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                     L.G = nullptr;
                     L.cum[0] = 0;
                     for (int t = 0; t < ch.nperm; t++) L.cum[t + 1] = L.cum[t] + ch.pb[t].Ty * d.o;
-                    k_f1_fp64<<<dim3((d.o * maxTx + kGBM - 1) / kGBM, (d.o * maxTz + kGBN - 1) / kGBN,
+                    TB_KLAUNCH(P_F1, k_f1_fp64<<<dim3((d.o * maxTx + kGBM - 1) / kGBM, (d.o * maxTz + kGBN - 1) / kGBN,
                                      L.cum[ch.nperm]),
-                                256, 0, st>>>(L);
-                    TB_LAUNCH_CHECK();
+                                256, 0, st>>>(L));
                 }
                 // F2: energy (+ adjoint of the raw amplitudes)
-                F2Params<StageT> F;
-                F.d = d;
-                F.ch = ch;
-                F.ijk = ijk;
-                F.mo_e = io.mo_energy; F.t1 = io.t1; F.t2 = io.t2; F.ovov = io.ovov; F.fvo = io.fvo;
-                F.S = S; F.SV = SV;
-                F.ybar = io.ybar;
-                F.want_grad = P.want_grad;
-                F.e_part = e_part; F.e_acc = &ctrl->e_acc; F.counter = &ctrl->counter;
-                F.mo_bar = io.mo_energy_bar;
-                const int items = ch.nabc[0] * ch.nabc[1] * ch.nabc[2];
-                k_f2<StageT><<<dim3(P.n_ijk, (items + kF2Threads - 1) / kF2Threads), kF2Threads, 0, st>>>(F);
-                TB_LAUNCH_CHECK();
+                {
+                    F2P<StageT> F;
+                    F.d = d;
+                    F.ch = ch;
+                    F.nsub = 0;
+                    int nsb[3];
+                    for (int t = 0; t < 3; t++) nsb[t] = (ch.nabc[t] + kSB - 1) / kSB;
+                    for (int sa = 0; sa < nsb[0]; sa++)
+                        for (int sb = 0; sb < nsb[1]; sb++) {
+                            if (ch.blk[0] == ch.blk[1] && sb > sa) continue;
+                            for (int sc = 0; sc < nsb[2]; sc++) {
+                                if (ch.blk[1] == ch.blk[2] && sc > sb) continue;
+                                F2Sub &u = F.sub[F.nsub++];
+                                const int si[3] = {sa, sb, sc};
+                                for (int t = 0; t < 3; t++) {
+                                    u.st[t] = ch.base[t] + si[t] * kSB;
+                                    int len = ch.nabc[t] - si[t] * kSB;
+                                    u.len[t] = len < kSB ? len : kSB;
+                                }
+                            }
+                        }
+                    F.ijk = ijk;
+                    F.mo_e = io.mo_energy; F.t1 = io.t1; F.t2 = io.t2; F.ovov = io.ovov; F.fvo = io.fvo;
+                    F.S = S;
+                    F.SW = SW;
+                    F.split = 0;
+                    F.wscale = &ctrl->wscale;
+                    F.ybar = io.ybar;
+                    F.want_grad = P.want_grad;
+                    F.e_part = e_part; F.e_acc = &ctrl->e_acc; F.counter = &ctrl->counter;
+                    F.mo_bar = io.mo_energy_bar;
+                    TB_KLAUNCH(P_F2, (k_f2t<StageT, kSB><<<dim3(P.n_ijk, F.nsub), kSB * kSB * kSB,
+                                                           f2_smem_bytes<StageT, kSB>(), st>>>(F)));
+                }
                 if (!P.want_grad) continue;
                 // V-term gradients
                 VGParams<StageT> VG;
                 VG.d = d;
                 VG.ch = ch;
-                VG.SV = SV;
+                VG.SV = S;
                 VG.t1 = io.t1; VG.fvo = io.fvo; VG.ovov = io.ovov; VG.t2 = io.t2;
                 VG.ovov_bar = io.ovov_bar; VG.t2_bar = io.t2_bar; VG.t1_bar = io.t1_bar;
                 VG.fvo_bar = io.fvo_bar;
@@ -1131,54 +1013,46 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                     long long r = (long long)d.o * d.o * ch.pb[t].Ty * ch.pb[t].Tx;
                     if (r > maxrows) maxrows = r;
                 }
-                k_vgrad<StageT><<<dim3((unsigned)((maxrows + kVgRows - 1) / kVgRows), ch.nperm), 256, 0, st>>>(VG);
-                TB_LAUNCH_CHECK();
+                TB_KLAUNCH(P_VGRAD, k_vgrad<StageT><<<dim3((unsigned)((maxrows + kVgRows - 1) / kVgRows), ch.nperm), 256, 0, st>>>(VG));
                 // W-term gradients
                 GemmLaunch<StageT> L;
                 L.d = d;
                 L.ch = ch;
                 L.tau_only = -1;
                 L.A1 = A1; L.B1 = B1; L.A2 = A2; L.B2 = B2;
-                L.S = S;
+                L.S = reinterpret_cast<StageT *>(SW);
                 L.cum[0] = 0;
                 for (int t = 0; t < ch.nperm; t++) L.cum[t + 1] = L.cum[t] + ch.pb[t].Ty;
                 L.G = GA1;
-                k_b1a_fp64<StageT><<<dim3((d.o * maxTx + kGBM - 1) / kGBM, (d.v + kGBN - 1) / kGBN, L.cum[ch.nperm]),
-                                     256, 0, st>>>(L);
-                TB_LAUNCH_CHECK();
+                TB_KLAUNCH(P_B1A, k_b1a_fp64<StageT><<<dim3((d.o * maxTx + kGBM - 1) / kGBM, (d.v + kGBN - 1) / kGBN, L.cum[ch.nperm]),
+                                     256, 0, st>>>(L));
                 L.G = GB2;
-                k_b1d_fp64<StageT><<<dim3((d.o * maxTz + kGBM - 1) / kGBM, (d.o + kGBN - 1) / kGBN, L.cum[ch.nperm]),
-                                     256, 0, st>>>(L);
-                TB_LAUNCH_CHECK();
+                TB_KLAUNCH(P_B1D, k_b1d_fp64<StageT><<<dim3((d.o * maxTz + kGBM - 1) / kGBM, (d.o + kGBN - 1) / kGBN, L.cum[ch.nperm]),
+                                     256, 0, st>>>(L));
                 for (int t = 0; t < ch.nperm; t++) {
                     L.tau_only = t;
                     L.G = GB1;
-                    k_b1b_fp64<StageT><<<dim3((d.o * ch.pb[t].Tz + kGBM - 1) / kGBM, (d.v + kGBN - 1) / kGBN, d.o),
-                                         256, 0, st>>>(L);
-                    TB_LAUNCH_CHECK();
+                    TB_KLAUNCH(P_B1B, k_b1b_fp64<StageT><<<dim3((d.o * ch.pb[t].Tz + kGBM - 1) / kGBM, (d.v + kGBN - 1) / kGBN, d.o),
+                                         256, 0, st>>>(L));
                     L.G = GA2;
-                    k_b1c_fp64<StageT><<<dim3((d.o * ch.pb[t].Tx + kGBM - 1) / kGBM, (d.o + kGBN - 1) / kGBN, d.o),
-                                         256, 0, st>>>(L);
-                    TB_LAUNCH_CHECK();
+                    TB_KLAUNCH(P_B1C, k_b1c_fp64<StageT><<<dim3((d.o * ch.pb[t].Tx + kGBM - 1) / kGBM, (d.o + kGBN - 1) / kGBN, d.o),
+                                         256, 0, st>>>(L));
                 }
             }
 
     if (P.want_grad) {
         if (P.packed) {
-            k_fold_ovvv_packed<<<grid1d((long long)o * v * (v * (v + 1) / 2), 256), 256, 0, st>>>(
-                GA1, d, io.ovvv_bar);
+            TB_KLAUNCH(P_FOLD, k_fold_ovvv_packed<<<grid1d((long long)o * v * (v * (v + 1) / 2), 256), 256, 0, st>>>(
+                GA1, d, io.ovvv_bar));
         } else {
-            k_fold_ovvv_full<<<dim3((d.v + 31) / 32, (d.v + 31) / 32, (unsigned)(o * v)), dim3(32, 8), 0, st>>>(
-                GA1, d, io.ovvv_bar);
+            TB_KLAUNCH(P_FOLD, k_fold_ovvv_full<<<dim3((d.v + 31) / 32, (d.v + 31) / 32, (unsigned)(o * v)), dim3(32, 8), 0, st>>>(
+                GA1, d, io.ovvv_bar));
         }
         TB_LAUNCH_CHECK();
-        k_fold_t2<<<grid1d((long long)o * o * v * v, 256), 256, 0, st>>>(GB1, GB2, d, io.t2_bar);
-        TB_LAUNCH_CHECK();
-        k_fold_ovoo<<<grid1d((long long)o * v * o * o, 256), 256, 0, st>>>(GA2, d, io.ovoo_bar);
-        TB_LAUNCH_CHECK();
+        TB_KLAUNCH(P_FOLD, k_fold_t2<<<grid1d((long long)o * o * v * v, 256), 256, 0, st>>>(GB1, GB2, d, io.t2_bar));
+        TB_KLAUNCH(P_FOLD, k_fold_ovoo<<<grid1d((long long)o * v * o * o, 256), 256, 0, st>>>(GA2, d, io.ovoo_bar));
     }
-    k_copy_scalar<<<1, 1, 0, st>>>(&ctrl->e_acc, io.e_out);
-    TB_LAUNCH_CHECK();
+    TB_KLAUNCH(P_FOLD, k_copy_scalar<<<1, 1, 0, st>>>(&ctrl->e_acc, io.e_out));
     return TRIPLES_OK;
 }
 
@@ -1188,6 +1062,31 @@ int run_triples(const Plan &P, cudaStream_t st, const TriplesIO &io) {
 }
 
 void set_block_size(int tv) { g_tv_override = tv; }
+
+void profile_enable(int on) {
+    g_prof = on != 0;
+    g_prof_recs.clear();
+    g_pool_used = 0;
+}
+
+int profile_read(int max_cats, double *ms, int *launches) {
+    for (int c = 0; c < max_cats && c < P_NCAT; c++) {
+        ms[c] = 0.0;
+        launches[c] = 0;
+    }
+    for (const ProfRec &r : g_prof_recs) {
+        float t = 0.f;
+        if (cudaEventSynchronize(r.b) != cudaSuccess) return -1;
+        cudaEventElapsedTime(&t, r.a, r.b);
+        if (r.cat < max_cats) {
+            ms[r.cat] += t;
+            launches[r.cat] += 1;
+        }
+    }
+    return P_NCAT;
+}
+
+const char *profile_name(int cat) { return (cat >= 0 && cat < P_NCAT) ? kProfNames[cat] : ""; }
 int last_cuda_error() { return g_last_cuda_error; }
 
 }  // namespace tb
@@ -1267,5 +1166,14 @@ int triples_last_cuda_error(void) { return tb::last_cuda_error(); }
 const char *triples_version(void) { return "0.1.0"; }
 
 void triples_set_block_size(int tv) { tb::set_block_size(tv); }
+
+void triples_profile_enable(int on) { tb::profile_enable(on); }
+
+int triples_profile_read(int max_categories, double *ms, int *launches) {
+    if (max_categories < 0 || (max_categories > 0 && (!ms || !launches))) return -1;
+    return tb::profile_read(max_categories, ms, launches);
+}
+
+const char *triples_profile_name(int category) { return tb::profile_name(category); }
 
 }  // extern "C"

@@ -3,6 +3,7 @@
 #include <cstddef>
 
 #include "common.cuh"
+#include "f2.cuh"
 
 namespace tb {
 
@@ -20,6 +21,7 @@ struct Ctrl {
     double scale[2];              // operand scales (A: ovvv/ovoo, B: t2), powers of two
     float out_scale;              // 1 / (scale[0] * scale[1])
     float pad_;
+    double wscale;                // per-chunk power-of-two scale of the split Wbar
     unsigned long long absmax[4]; // bit patterns of max |ovvv|, |ovoo|, |t2|
 };
 
@@ -33,7 +35,7 @@ struct Plan {
     int Kp8, Op8;    // 16-byte padded contraction lengths of the 16-bit operands
     size_t stage_elems, stage_bytes;
     size_t off_ctrl;
-    size_t off_A1, off_B1, off_A2, off_B2, off_S, off_SV;
+    size_t off_A1, off_B1, off_A2, off_B2, off_S, off_SW;
     size_t off_A1h, off_B1h, off_A2h, off_B2h;
     size_t off_GA1, off_GB1, off_GA2, off_GB2;
     size_t off_ijk, off_epart;

@@ -48,7 +48,7 @@ def test_mixed_vs_reference_golden(name, precision):
         assert _relerr(g[k], ref) < tg, (k, _relerr(g[k], ref))
 
 
-@pytest.mark.parametrize("tv", [3, 7])
+@pytest.mark.parametrize("tv", [2, 4])
 def test_mixed_block_sizes(tv):
     triples.set_block_size(tv)
     inp, e_ref, g_ref, _ = G.load("o4v9_fvo")

@@ -112,6 +112,12 @@ void triples_profile_enable(int on);
 int triples_profile_read(int max_categories, double *ms, int *launches);
 const char *triples_profile_name(int category);
 
+/* Tuning (mixed precision): number of 64-wide K blocks the tensor cores
+ * accumulate in FP32 before the partial result is added in higher precision (default 1;
+ * 0 restores the default).  Shorter segments trade epilogue work for accuracy
+ * on long contractions. */
+void triples_set_accumulation_segment(int kblocks);
+
 /* Version of this library, e.g. "0.1.0". */
 const char *triples_version(void);
 

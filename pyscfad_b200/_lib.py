@@ -59,6 +59,8 @@ def load():
     lib.triples_profile_read.argtypes = [_c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_c_int)]
     lib.triples_profile_name.restype = ctypes.c_char_p
     lib.triples_profile_name.argtypes = [_c_int]
+    lib.triples_set_accumulation_segment.restype = None
+    lib.triples_set_accumulation_segment.argtypes = [_c_int]
     lib.triples_set_block_size.restype = None
     lib.triples_set_block_size.argtypes = [_c_int]
     _lib = lib

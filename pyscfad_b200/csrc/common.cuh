@@ -61,6 +61,8 @@ struct PermBlock {
     int bx, by, bz;        // block indices
     int X0, Tx, Y0, Ty, Z0, Tz;
     long long soff;        // offset of S_tau in the staging buffer (elements)
+    int rzp;               // o*Tz rounded up to 8 (16-byte rows of 16-bit Wbar)
+    long long swoff;       // offset of Wbar_tau (values) in the Wbar buffer
 };
 
 struct ChunkDesc {

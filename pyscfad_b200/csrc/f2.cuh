@@ -342,21 +342,21 @@ __global__ void __launch_bounds__(SB *SB *SB) k_f2t(F2P<StageT> P) {
             const int si = reg * REG + (yy * lx + xx) * lz + zz;
             const long long g = pb.soff + ((((long long)(p * o + q) * pb.Ty + yl) * pb.Tx + xl) * o + r) * pb.Tz + zl;
             P.S[g] = sW[si];
-            const long long oTz = (long long)o * pb.Tz;
-            const long long wl = ((((long long)yl * o + p) * pb.Tx + xl) * o + q) * oTz + (long long)r * pb.Tz + zl;
+            const long long wl =
+                ((((long long)yl * o + p) * pb.Tx + xl) * o + q) * pb.rzp + (long long)r * pb.Tz + zl;
             const double wb = (double)sWb[si];
             if (P.split == 0) {
-                reinterpret_cast<StageT *>(P.SW)[pb.soff + wl] = sWb[si];
+                reinterpret_cast<StageT *>(P.SW)[pb.swoff + wl] = sWb[si];
             } else {
-                const long long half = (long long)pb.Ty * o * pb.Tx * o * oTz;
+                const long long half = (long long)pb.Ty * o * pb.Tx * o * pb.rzp;
                 const double xs = wb * wsc;
                 if (P.split == 1) {
-                    __half *dst = reinterpret_cast<__half *>(P.SW) + 2 * pb.soff;
+                    __half *dst = reinterpret_cast<__half *>(P.SW) + 2 * pb.swoff;
                     const __half hi = __double2half(xs);
                     dst[wl] = hi;
                     dst[half + wl] = __double2half(xs - (double)__half2float(hi));
                 } else {
-                    __nv_bfloat16 *dst = reinterpret_cast<__nv_bfloat16 *>(P.SW) + 2 * pb.soff;
+                    __nv_bfloat16 *dst = reinterpret_cast<__nv_bfloat16 *>(P.SW) + 2 * pb.swoff;
                     const __nv_bfloat16 hi = __double2bfloat16(xs);
                     dst[wl] = hi;
                     dst[half + wl] = __double2bfloat16(xs - (double)__bfloat162float(hi));

@@ -1,0 +1,306 @@
+// Tensor-core (tcgen05) form of the adjoint contractions, one launch per
+// ordering tau of a chunk.  Wbar_tau is staged by the epilogue as fp16/bf16
+// hi/lo splits in the layout [h][y][p][x][q][r][z] (scaled by a per-chunk
+// power of two), which serves all four products through 5-D TMA boxes:
+//
+//   kind 0  ovvv:  G_A1[y][p][x][f] += sum_{q,rz} Wbar[y][p][x][q][rz] B1[q][rz][f]
+//                  rows (p,x) K-major, batch y, K = (q, rz)
+//   kind 1  t2:    G_B1[q][rz][f]   += sum_{y,p,x} Wbar[y][p][x][q][rz] A1[y][p][x][f]
+//                  rows rz MN-major, batch q, K = (y, p, x)
+//   kind 2  ovoo:  G_A2[q][p][x][m] -= sum_{y,rz} Wbar[y][p][x][q][rz] B2[y][rz][m]
+//                  rows (p,x) K-major, batch q, K = (y, rz)
+//   kind 3  t2:    G_B2[y][rz][m]   += sum_{q,p,x} Wbar[y][p][x][q][rz] A2n[q][p][x][m]
+//                  rows rz MN-major, batch y, K = (q, p, x)   (A2n = -ovoo)
+//
+// (the adjoint GEMMs of get_eris_amps_bar, ccsd_t_vjp.c:139-246, batched over
+// all occupied indices).  The second operand is always MN-major.  Products:
+// hi*hi + hi*lo + lo*hi into FP32 TMEM; the epilogue adds the descaled tile
+// into the FP64 gradient buffer (each output tile has a single owner).
+#pragma once
+#include "common.cuh"
+#include "tc_f1.cuh"
+#include "tc_ptx.cuh"
+
+namespace tb {
+
+struct TcB1Params {
+    Dims d;
+    PermBlock pb;
+    int kind;
+    int nbatch, ntile_m, ntile_n;
+    int nk_outer, nk_inner;
+    double *G;
+    const double *wscale;   // device: per-chunk Wbar scale
+    const double *oscale;   // device: scale of the second operand
+    double sign;
+    int *err;
+    int bf16;
+    int kseg;               // K blocks per accumulation segment (summed in FP64)
+};
+
+constexpr int kB1Threads = 320;   // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
+
+template <bool A_MN, int BN>
+struct TcB1Cfg {
+    static constexpr int A_BYTES = kTcBM * kTcBK * 2;
+    static constexpr int B_BYTES = BN * kTcBK * 2;
+    static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+    static constexpr int STAGES = (200 * 1024) / STAGE_BYTES;
+    static constexpr int SMEM = STAGES * STAGE_BYTES + 256 + 1024;
+    static constexpr int TMEM_COLS = 2 * BN < 32 ? 32 : 2 * BN;
+};
+
+template <bool A_MN, int BN>
+__global__ void __launch_bounds__(kB1Threads, 1)
+    k_b1_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, TcB1Params P) {
+    using C = TcB1Cfg<A_MN, BN>;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t *full = (uint64_t *)(smem + C::STAGES * C::STAGE_BYTES);
+    uint64_t *empty = full + C::STAGES;
+    uint64_t *tfull = empty + C::STAGES;
+    uint64_t *tempty = tfull + 2;
+    uint64_t *drain = tempty + 2;
+    uint32_t *tmem_slot = (uint32_t *)(drain + 1);
+    __shared__ int s_abort;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        s_abort = 0;
+        for (int s = 0; s < C::STAGES; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int a = 0; a < 2; a++) {
+            mbar_init(&tfull[a], 1);
+            mbar_init(&tempty[a], 8);
+        }
+        mbar_init(drain, 1);
+        fence_mbar_init();
+    }
+    if (warp == 0 && lane == 0) {
+        tma_prefetch_desc(&tmA);
+        tma_prefetch_desc(&tmB);
+    }
+    if (warp == 1) {
+        tmem_alloc(tmem_slot, C::TMEM_COLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    volatile int *abortp = &s_abort;
+    const int per_batch = P.ntile_m * P.ntile_n;
+    const int total = P.nbatch * per_batch;
+    const int nk = P.nk_outer * P.nk_inner;
+    const PermBlock &pb = P.pb;
+    const int o = P.d.o;
+    const int Ty = pb.Ty, Tz = pb.Tz;
+
+    if (warp == 0 && lane == 0) {
+        // ---------------- TMA producer ----------------
+        int stage = 0;
+        uint32_t phase = 0;
+        uint32_t pend_phase[C::STAGES];
+        bool pending[C::STAGES];
+        for (int s = 0; s < C::STAGES; s++) pending[s] = false;
+        bool ok = true;
+        for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+            const int b = t / per_batch, rem = t % per_batch;
+            const int mt = rem / P.ntile_n, nt = rem % P.ntile_n;
+            for (int kb = 0; kb < nk; kb++) {
+                if (!mbar_wait(&empty[stage], phase ^ 1u, abortp)) {
+                    ok = false;
+                    break;
+                }
+                pending[stage] = false;
+                mbar_expect_tx(&full[stage], C::STAGE_BYTES);
+                uint8_t *sA = smem + stage * C::STAGE_BYTES;
+                uint8_t *sB = sA + 2 * C::A_BYTES;
+                const int ko = kb / P.nk_inner, ki = kb % P.nk_inner;
+                for (int h = 0; h < 2; h++) {
+                    uint8_t *a = sA + h * C::A_BYTES;
+                    uint8_t *bb = sB + h * C::B_BYTES;
+                    switch (P.kind) {
+                    case 0:   // batch y, K = (q = ko, rz block = ki)
+                        tma_load_5d(a, &tmA, &full[stage], ki * 64, ko, 0, mt * 8, h * Ty + b);
+                        for (int j = 0; j < BN / 64; j++)
+                            tma_load_5d(bb + j * 8192, &tmB, &full[stage], nt * BN + j * 64, pb.Z0, ki * 64 / Tz, ko, h);
+                        break;
+                    case 1:   // batch q, K = (y = ko, p group = ki)
+                        for (int j = 0; j < 2; j++)
+                            tma_load_5d(a + j * 8192, &tmA, &full[stage], mt * 128 + j * 64, b, 0, ki * 4, h * Ty + ko);
+                        for (int j = 0; j < BN / 64; j++)
+                            tma_load_5d(bb + j * 8192, &tmB, &full[stage], nt * BN + j * 64, pb.X0, ki * 4, pb.Y0 + ko, h);
+                        break;
+                    case 2:   // batch q, K = (y = ko, rz block = ki)
+                        tma_load_5d(a, &tmA, &full[stage], ki * 64, b, 0, mt * 8, h * Ty + ko);
+                        for (int j = 0; j < BN / 64; j++)
+                            tma_load_5d(bb + j * 8192, &tmB, &full[stage], nt * BN + j * 64, pb.Z0, ki * 64 / Tz, pb.Y0 + ko, h);
+                        break;
+                    default:  // batch y, K = (q = ko, p group = ki)
+                        for (int j = 0; j < 2; j++)
+                            tma_load_5d(a + j * 8192, &tmA, &full[stage], mt * 128 + j * 64, ko, 0, ki * 4, h * Ty + b);
+                        for (int j = 0; j < BN / 64; j++)
+                            tma_load_5d(bb + j * 8192, &tmB, &full[stage], nt * BN + j * 64, pb.X0, ki * 4, ko, h);
+                        break;
+                    }
+                }
+                pending[stage] = true;
+                pend_phase[stage] = phase;
+                if (++stage == C::STAGES) {
+                    stage = 0;
+                    phase ^= 1u;
+                }
+            }
+        }
+        if (!ok) {
+            *abortp = 1;
+            atomicOr(P.err, 8);
+            for (int s = 0; s < C::STAGES; s++)
+                if (pending[s]) {
+                    for (uint32_t i = 0; i < kSpinLimit && !mbar_try_wait(&full[s], pend_phase[s]); i++) {
+                    }
+                }
+        }
+    } else if (warp == 1 && lane == 0) {
+        // ---------------- MMA issuer: one TMEM buffer per K segment ----------------
+        const uint32_t idesc = make_idesc_f16(kTcBM, BN, P.bf16 != 0, A_MN, true);
+        int stage = 0;
+        uint32_t phase = 0;
+        int seg = 0;   // running segment counter (same sequence as the epilogue)
+        bool ok = true;
+        for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+            for (int k0 = 0; k0 < nk && ok; k0 += P.kseg, seg++) {
+                const int acc = seg & 1;
+                const uint32_t accph = (seg >> 1) & 1;
+                if (!mbar_wait(&tempty[acc], accph ^ 1u, abortp)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
+                const int k1 = (k0 + P.kseg < nk) ? k0 + P.kseg : nk;
+                for (int kb = k0; kb < k1; kb++) {
+                    if (!mbar_wait(&full[stage], phase, abortp)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t a_h = smem_u32(smem + stage * C::STAGE_BYTES);
+                    const uint32_t a_l = a_h + C::A_BYTES;
+                    const uint32_t b_h = a_l + C::A_BYTES;
+                    const uint32_t b_l = b_h + C::B_BYTES;
+#pragma unroll
+                    for (int ks = 0; ks < kTcBK / 16; ks++) {
+                        uint64_t dah, dal;
+                        if (A_MN) {
+                            dah = make_sdesc_sw128(a_h + 2048 * ks, 8192, 1024);
+                            dal = make_sdesc_sw128(a_l + 2048 * ks, 8192, 1024);
+                        } else {
+                            dah = make_sdesc_sw128(a_h + 32 * ks, 16, 1024);
+                            dal = make_sdesc_sw128(a_l + 32 * ks, 16, 1024);
+                        }
+                        const uint64_t dbh = make_sdesc_sw128(b_h + 2048 * ks, 8192, 1024);
+                        const uint64_t dbl = make_sdesc_sw128(b_l + 2048 * ks, 8192, 1024);
+                        umma_f16(d_tmem, dah, dbh, idesc, (kb > k0 || ks > 0) ? 1u : 0u);
+                        umma_f16(d_tmem, dah, dbl, idesc, 1u);
+                        umma_f16(d_tmem, dal, dbh, idesc, 1u);
+                    }
+                    umma_commit(&empty[stage]);
+                    if (++stage == C::STAGES) {
+                        stage = 0;
+                        phase ^= 1u;
+                    }
+                }
+                if (!ok) break;
+                umma_commit(&tfull[acc]);
+            }
+        }
+        if (!ok) {
+            *abortp = 1;
+            atomicOr(P.err, 16);
+        }
+        umma_commit(drain);
+        for (uint32_t i = 0; i < kSpinLimit && !mbar_try_wait(drain, 0); i++) {
+        }
+    } else if (warp >= 2) {
+        // ---------------- epilogue: G += sign * sum_seg D_seg / (wscale * oscale) ----------------
+        constexpr int HC = BN / 2;            // columns per epilogue warp
+        const int quarter = warp & 3;         // TMEM lane quarter this warp may access
+        const int half = (warp - 2) >> 2;     // which half of the columns
+        const int row = quarter * 32 + lane;
+        const int v = P.d.v, Kp = P.d.Kp;
+        const double sc = P.sign / ((*P.wscale) * (*P.oscale));
+        int seg = 0;
+        bool ok = true;
+        for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+            double accd[HC];
+#pragma unroll
+            for (int j = 0; j < HC; j++) accd[j] = 0.0;
+            for (int k0 = 0; k0 < nk; k0 += P.kseg, seg++) {
+                const int acc = seg & 1;
+                const uint32_t accph = (seg >> 1) & 1;
+                if (!mbar_wait(&tfull[acc], accph, abortp)) {
+                    *abortp = 1;
+                    atomicOr(P.err, 32);
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+#pragma unroll
+                for (int c = 0; c < HC / 32; c++) {
+                    uint32_t vv[32];
+                    tmem_ld32(tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * BN + half * HC + c * 32),
+                              vv);
+                    tmem_ld_wait();
+#pragma unroll
+                    for (int j = 0; j < 32; j++) accd[c * 32 + j] += (double)__uint_as_float(vv[j]);
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&tempty[acc]);
+            }
+            if (!ok) break;
+            const int b = t / per_batch, rem = t % per_batch;
+            const int mt = rem / P.ntile_n, nt = rem % P.ntile_n;
+            long long roff = -1;
+            if (P.kind == 0 || P.kind == 2) {
+                const int p = mt * 8 + row / 16, x = row % 16;
+                if (p < o && x < pb.Tx) {
+                    if (P.kind == 0)
+                        roff = ((((long long)pb.Y0 + b) * o + p) * v + pb.X0 + x) * Kp;
+                    else
+                        roff = (((long long)b * o + p) * v + pb.X0 + x) * o;
+                }
+            } else {
+                const int rz = mt * 128 + row;
+                if (rz < o * Tz) {
+                    const int r = rz / Tz, z = rz % Tz;
+                    if (P.kind == 1)
+                        roff = (((long long)b * o + r) * v + pb.Z0 + z) * Kp;
+                    else
+                        roff = ((((long long)pb.Y0 + b) * o + r) * v + pb.Z0 + z) * o;
+                }
+            }
+            const int ncol = (P.kind <= 1) ? v : o;
+            if (roff >= 0) {
+                const int c0 = nt * BN + half * HC;
+#pragma unroll
+                for (int j = 0; j < HC; j++) {
+                    const int col = c0 + j;
+                    if (col < ncol) P.G[roff + col] += sc * accd[j];
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem_base, C::TMEM_COLS);
+    }
+}
+
+}  // namespace tb

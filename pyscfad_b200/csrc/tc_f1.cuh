@@ -41,9 +41,13 @@ struct TcF1Params {
     int nkb1, nkb2;    // K blocks of the ovvv and ooov terms
     float *S;
     const float *out_scale;   // device scalar: 1 / (scale_A * scale_B)
+    unsigned *wmax_bits;      // device: running max |W| of this chunk (float bits)
     int *err;
     int bf16;
+    int kseg;                 // K blocks per TMEM accumulation segment
 };
+
+constexpr int kF1Threads = 320;   // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
 
 struct F1Tile {
     int tau, y, q, mt, nt;
@@ -65,7 +69,7 @@ __device__ __forceinline__ F1Tile f1_decode(const TcF1Params &P, int t) {
 }
 
 template <int BN>
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(kF1Threads, 1)
     k_f1_tc(const __grid_constant__ CUtensorMap tmA1, const __grid_constant__ CUtensorMap tmB1,
             const __grid_constant__ CUtensorMap tmA2, const __grid_constant__ CUtensorMap tmB2, TcF1Params P) {
     using C = TcCfg<BN>;
@@ -88,7 +92,7 @@ __global__ void __launch_bounds__(192, 1)
         }
         for (int a = 0; a < 2; a++) {
             mbar_init(&tfull[a], 1);
-            mbar_init(&tempty[a], 4);
+            mbar_init(&tempty[a], 8);
         }
         mbar_init(drain, 1);
         fence_mbar_init();
@@ -166,49 +170,52 @@ __global__ void __launch_bounds__(192, 1)
                 }
         }
     } else if (warp == 1 && lane == 0) {
-        // ---------------- MMA issuer ----------------
+        // ---------------- MMA issuer: one TMEM buffer per K segment ----------------
         const uint32_t idesc = make_idesc_f16(kTcBM, BN, P.bf16 != 0, false, false);
         int stage = 0;
         uint32_t phase = 0;
-        int local = 0;
+        int seg = 0;
         bool ok = true;
-        for (int t = blockIdx.x; t < total && ok; t += gridDim.x, local++) {
-            const int acc = local & 1;
-            const uint32_t accph = (local >> 1) & 1;
-            if (!mbar_wait(&tempty[acc], accph ^ 1u, abortp)) {
-                ok = false;
-                break;
-            }
-            tc_fence_after();
-            const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
-            for (int kb = 0; kb < nkb; kb++) {
-                if (!mbar_wait(&full[stage], phase, abortp)) {
+        for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+            for (int k0 = 0; k0 < nkb && ok; k0 += P.kseg, seg++) {
+                const int acc = seg & 1;
+                const uint32_t accph = (seg >> 1) & 1;
+                if (!mbar_wait(&tempty[acc], accph ^ 1u, abortp)) {
                     ok = false;
                     break;
                 }
                 tc_fence_after();
-                const uint32_t a_h = smem_u32(smem + stage * C::STAGE_BYTES);
-                const uint32_t a_l = a_h + C::A_BYTES;
-                const uint32_t b_h = a_l + C::A_BYTES;
-                const uint32_t b_l = b_h + C::B_BYTES;
+                const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
+                const int k1 = (k0 + P.kseg < nkb) ? k0 + P.kseg : nkb;
+                for (int kb = k0; kb < k1; kb++) {
+                    if (!mbar_wait(&full[stage], phase, abortp)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t a_h = smem_u32(smem + stage * C::STAGE_BYTES);
+                    const uint32_t a_l = a_h + C::A_BYTES;
+                    const uint32_t b_h = a_l + C::A_BYTES;
+                    const uint32_t b_l = b_h + C::B_BYTES;
 #pragma unroll
-                for (int ks = 0; ks < kTcBK / 16; ks++) {
-                    const uint64_t dah = make_sdesc_sw128(a_h + 32 * ks, 16, 1024);
-                    const uint64_t dal = make_sdesc_sw128(a_l + 32 * ks, 16, 1024);
-                    const uint64_t dbh = make_sdesc_sw128(b_h + 32 * ks, 16, 1024);
-                    const uint64_t dbl = make_sdesc_sw128(b_l + 32 * ks, 16, 1024);
-                    umma_f16(d_tmem, dah, dbh, idesc, (kb > 0 || ks > 0) ? 1u : 0u);
-                    umma_f16(d_tmem, dah, dbl, idesc, 1u);
-                    umma_f16(d_tmem, dal, dbh, idesc, 1u);
+                    for (int ks = 0; ks < kTcBK / 16; ks++) {
+                        const uint64_t dah = make_sdesc_sw128(a_h + 32 * ks, 16, 1024);
+                        const uint64_t dal = make_sdesc_sw128(a_l + 32 * ks, 16, 1024);
+                        const uint64_t dbh = make_sdesc_sw128(b_h + 32 * ks, 16, 1024);
+                        const uint64_t dbl = make_sdesc_sw128(b_l + 32 * ks, 16, 1024);
+                        umma_f16(d_tmem, dah, dbh, idesc, (kb > k0 || ks > 0) ? 1u : 0u);
+                        umma_f16(d_tmem, dah, dbl, idesc, 1u);
+                        umma_f16(d_tmem, dal, dbh, idesc, 1u);
+                    }
+                    umma_commit(&empty[stage]);
+                    if (++stage == C::STAGES) {
+                        stage = 0;
+                        phase ^= 1u;
+                    }
                 }
-                umma_commit(&empty[stage]);
-                if (++stage == C::STAGES) {
-                    stage = 0;
-                    phase ^= 1u;
-                }
+                if (!ok) break;
+                umma_commit(&tfull[acc]);
             }
-            if (!ok) break;
-            umma_commit(&tfull[acc]);
         }
         if (!ok) {
             *abortp = 1;
@@ -219,21 +226,44 @@ __global__ void __launch_bounds__(192, 1)
         for (uint32_t i = 0; i < kSpinLimit && !mbar_try_wait(drain, 0); i++) {
         }
     } else if (warp >= 2) {
-        // ---------------- epilogue ----------------
+        // ---------------- epilogue: sum the segments (FP32, round to nearest) ----------------
+        constexpr int HC = BN / 2;          // columns handled by one epilogue warp
         const int quarter = warp & 3;
+        const int half = (warp - 2) >> 2;
         const int row = quarter * 32 + lane;
         const int o = P.d.o;
         const float sc = *P.out_scale;
-        int local = 0;
-        for (int t = blockIdx.x; t < total; t += gridDim.x, local++) {
-            const int acc = local & 1;
-            const uint32_t accph = (local >> 1) & 1;
-            if (!mbar_wait(&tfull[acc], accph, abortp)) {
-                *abortp = 1;
-                atomicOr(P.err, 4);
-                break;
+        float wmax = 0.f;
+        int seg = 0;
+        bool ok = true;
+        for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+            float accf[HC];
+#pragma unroll
+            for (int j = 0; j < HC; j++) accf[j] = 0.f;
+            for (int k0 = 0; k0 < nkb; k0 += P.kseg, seg++) {
+                const int acc = seg & 1;
+                const uint32_t accph = (seg >> 1) & 1;
+                if (!mbar_wait(&tfull[acc], accph, abortp)) {
+                    *abortp = 1;
+                    atomicOr(P.err, 4);
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+#pragma unroll
+                for (int c = 0; c < HC / 32; c++) {
+                    uint32_t vv[32];
+                    tmem_ld32(tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * BN + half * HC + c * 32),
+                              vv);
+                    tmem_ld_wait();
+#pragma unroll
+                    for (int j = 0; j < 32; j++) accf[c * 32 + j] += __uint_as_float(vv[j]);
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&tempty[acc]);
             }
-            tc_fence_after();
+            if (!ok) break;
             const F1Tile T = f1_decode(P, t);
             const PermBlock &pb = P.ch.pb[T.tau];
             const int p = T.mt * 8 + row / 16;
@@ -241,38 +271,39 @@ __global__ void __launch_bounds__(192, 1)
             const bool vrow = (p < o) && (x < pb.Tx);
             float *dst = P.S + pb.soff +
                          ((((long long)(p * o + T.q) * pb.Ty + T.y) * pb.Tx + x) * o) * pb.Tz;
-#pragma unroll 1
-            for (int c = 0; c < BN / 32; c++) {
-                uint32_t v[32];
-                tmem_ld32(tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * BN + c * 32), v);
-                tmem_ld_wait();
-                if (vrow) {
+            if (vrow) {
 #pragma unroll
-                    for (int h = 0; h < 2; h++) {
-                        const int r = T.nt * C::RT + c * 2 + h;
-                        if (r >= o) continue;
-                        float *d = dst + (long long)r * pb.Tz;
-                        if (pb.Tz == 16) {
-                            float4 *d4 = reinterpret_cast<float4 *>(d);
+                for (int h = 0; h < HC / 16; h++) {
+                    const int r = T.nt * C::RT + half * (HC / 16) + h;
+                    if (r >= o) continue;
+                    float *d = dst + (long long)r * pb.Tz;
+                    if (pb.Tz == 16) {
+                        float4 *d4 = reinterpret_cast<float4 *>(d);
 #pragma unroll
-                            for (int z4 = 0; z4 < 4; z4++) {
-                                float4 w;
-                                w.x = __uint_as_float(v[h * 16 + z4 * 4 + 0]) * sc;
-                                w.y = __uint_as_float(v[h * 16 + z4 * 4 + 1]) * sc;
-                                w.z = __uint_as_float(v[h * 16 + z4 * 4 + 2]) * sc;
-                                w.w = __uint_as_float(v[h * 16 + z4 * 4 + 3]) * sc;
-                                d4[z4] = w;
+                        for (int z4 = 0; z4 < 4; z4++) {
+                            float4 w;
+                            w.x = accf[h * 16 + z4 * 4 + 0] * sc;
+                            w.y = accf[h * 16 + z4 * 4 + 1] * sc;
+                            w.z = accf[h * 16 + z4 * 4 + 2] * sc;
+                            w.w = accf[h * 16 + z4 * 4 + 3] * sc;
+                            wmax = fmaxf(wmax, fmaxf(fmaxf(fabsf(w.x), fabsf(w.y)), fmaxf(fabsf(w.z), fabsf(w.w))));
+                            d4[z4] = w;
+                        }
+                    } else {
+#pragma unroll
+                        for (int z = 0; z < 16; z++) {
+                            if (z < pb.Tz) {
+                                const float w1 = accf[h * 16 + z] * sc;
+                                wmax = fmaxf(wmax, fabsf(w1));
+                                d[z] = w1;
                             }
-                        } else {
-                            for (int z = 0; z < pb.Tz; z++) d[z] = __uint_as_float(v[h * 16 + z]) * sc;
                         }
                     }
                 }
             }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&tempty[acc]);
         }
+        for (int off = 16; off > 0; off >>= 1) wmax = fmaxf(wmax, __shfl_xor_sync(0xffffffffu, wmax, off));
+        if (lane == 0 && wmax > 0.f) atomicMax(P.wmax_bits, __float_as_uint(wmax));
     }
     tc_fence_before();
     __syncthreads();

@@ -15,6 +15,7 @@
 #include "gemm_fp64.cuh"
 #include "tc_f1.cuh"
 #include "f2.cuh"
+#include "tc_b1.cuh"
 #include "pyscfad_b200.h"
 #include "triples_internal.h"
 
@@ -22,6 +23,8 @@ namespace tb {
 
 static thread_local int g_last_cuda_error = 0;
 static int g_tv_override = 0;
+static int g_kseg = 1;     // K blocks per FP32 accumulation segment of the adjoint contractions
+static int g_kseg_f1 = 1;  // same for the W contraction
 
 #define TB_CUDA(call)                                     \
     do {                                                  \
@@ -103,7 +106,7 @@ static void make_chunk(const Dims &d, int A, int B, int C, ChunkDesc &ch) {
         ch.base[t] = block_start(d, blks[t]);
     }
     ch.nperm = 0;
-    long long off = 0;
+    long long off = 0, swoff = 0;
     const long long o3 = (long long)d.o * d.o * d.o;
     for (int s = 0; s < 6; s++) {
         int ps[3];
@@ -120,7 +123,17 @@ static void make_chunk(const Dims &d, int A, int B, int C, ChunkDesc &ch) {
         pb.Z0 = block_start(d, bz); pb.Tz = bsize(bz);
         pb.soff = off;
         off += (o3 * pb.Tx * pb.Ty * pb.Tz + 15) / 16 * 16;   // 64 B aligned sub-buffers
+        pb.rzp = (d.o * pb.Tz + 7) / 8 * 8;
+        pb.swoff = swoff;
+        swoff += ((long long)pb.Ty * d.o * pb.Tx * d.o * pb.rzp + 15) / 16 * 16;
     }
+}
+
+static long long chunk_wbar_elems(const ChunkDesc &ch, const Dims &d) {
+    long long s = 0;
+    for (int t = 0; t < ch.nperm; t++)
+        s += ((long long)ch.pb[t].Ty * d.o * ch.pb[t].Tx * d.o * ch.pb[t].rzp + 15) / 16 * 16;
+    return s;
 }
 
 static long long chunk_stage_elems(const ChunkDesc &ch, const Dims &d) {
@@ -147,7 +160,7 @@ int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan
     P.Op8 = (nocc + 7) / 8 * 8;
     P.nb = num_blocks(d);
     P.n_ijk = nocc * (nocc + 1) * (nocc + 2) / 6;
-    long long maxst = 0;
+    long long maxst = 0, maxwb = 0;
     int maxitems = 0;
     for (int A = 0; A < P.nb; A++)
         for (int B = 0; B <= A; B++)
@@ -156,10 +169,13 @@ int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan
                 make_chunk(d, A, B, C, ch);
                 long long s = chunk_stage_elems(ch, d);
                 if (s > maxst) maxst = s;
+                long long w = chunk_wbar_elems(ch, d);
+                if (w > maxwb) maxwb = w;
                 int it = ch.nabc[0] * ch.nabc[1] * ch.nabc[2];
                 if (it > maxitems) maxitems = it;
             }
     P.stage_elems = (size_t)maxst;
+    P.wbar_elems = (size_t)maxwb;
     P.max_items = maxitems;
     P.f2_gy = kMaxSub;
     const bool mixed = precision != TRIPLES_PRECISION_FP64;
@@ -182,7 +198,7 @@ int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan
     }
     P.off_S = take(P.stage_elems * P.stage_bytes);
     if (want_grad) {
-        P.off_SW = take(P.stage_elems * P.stage_bytes);
+        P.off_SW = take(P.wbar_elems * (mixed ? 4 : 8));
         P.off_GA1 = take(v * o * v * Kp * el);
         P.off_GB1 = take(o * o * v * Kp * el);
         P.off_GA2 = take(o * o * v * o * el);
@@ -309,6 +325,38 @@ __global__ void k_make_scales(Ctrl *ctrl, int scaled) {
     ctrl->scale[0] = sA;
     ctrl->scale[1] = sB;
     ctrl->out_scale = (float)(1.0 / (sA * sB));
+}
+
+// Per-chunk power-of-two scale for the split Wbar, from a bound that needs no
+// pass over Wbar:  |Wbar| <= 2|ybar| (144 max|w| + 36 max|v|) / min|D| over the
+// chunk (|Z| <= 12 max|X|, |X| <= 6 max|w| + 3 max|v|, |R WW| <= 72 max|w|,
+// orbit weight <= 2).  Resets the running max |w| for the next chunk.
+__global__ void k_chunk_scale(Ctrl *ctrl, const double *__restrict__ mo_e, int o, int a0, int na, int b0,
+                              int nb, int c0, int nc, double ybar, int scaled) {
+    __shared__ double s_min[3], s_maxo;
+    const double inf = 1e300;
+    if (threadIdx.x < 4) {
+        double m = (threadIdx.x < 3) ? inf : -inf;
+        const int st = threadIdx.x == 0 ? a0 : (threadIdx.x == 1 ? b0 : c0);
+        const int n = threadIdx.x == 0 ? na : (threadIdx.x == 1 ? nb : nc);
+        if (threadIdx.x < 3) {
+            for (int t = 0; t < n; t++) m = fmin(m, mo_e[o + st + t]);
+            s_min[threadIdx.x] = m;
+        } else {
+            for (int t = 0; t < o; t++) m = fmax(m, mo_e[t]);
+            s_maxo = m;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const double dmin = s_min[0] + s_min[1] + s_min[2] - 3.0 * s_maxo;
+        const double mw = (double)__uint_as_float(ctrl->wmax_bits);
+        const double mv = __longlong_as_double((long long)ctrl->absmax[3]) * __longlong_as_double((long long)ctrl->absmax[4]) +
+                          __longlong_as_double((long long)ctrl->absmax[2]) * __longlong_as_double((long long)ctrl->absmax[5]);
+        double bound = 2.0 * fabs(ybar) * (144.0 * mw + 36.0 * mv) / (dmin > 1e-300 ? dmin : 1e-300);
+        ctrl->wscale = scaled ? pow2_scale(bound) : 1.0;
+        ctrl->wmax_bits = 0u;
+    }
 }
 
 template <typename H>
@@ -487,10 +535,10 @@ __global__ void __launch_bounds__(256) k_b1a_fp64(GemmLaunch<StageT> L) {
     g.N = v;
     g.K = o * o * pb.Tz;
     g.K2 = 0;
-    const long long s_r = pb.Tz, s_q = (long long)o * pb.Tz, s_x = (long long)o * o * pb.Tz;
+    const long long s_r = pb.Tz, s_q = pb.rzp, s_x = (long long)o * pb.rzp;
     const long long s_p = (long long)pb.Tx * s_x, s_y = (long long)o * s_p;
     (void)s_r;
-    g.A = GOpT<StageT>{L.S + pb.soff + (long long)y * s_y, map2(pb.Tx, s_x, s_p), map1(1), 1};
+    g.A = GOpT<StageT>{L.S + pb.swoff + (long long)y * s_y, map2(pb.Tx, s_x, s_p), map2((int)oTz, 1, s_q), 1};
     g.B = GOp{L.B1 + (long long)pb.Z0 * Kp, map1(1),
               map3(pb.Tz, o, Kp, (long long)v * Kp, (long long)o * v * Kp), 0};
     g.C = L.G + (((long long)pb.Y0 + y) * o * v + pb.X0) * Kp;
@@ -519,10 +567,10 @@ __global__ void __launch_bounds__(256) k_b1b_fp64(GemmLaunch<StageT> L) {
     g.N = v;
     g.K = pb.Ty * o * pb.Tx;
     g.K2 = 0;
-    const long long s_r = pb.Tz, s_q = (long long)o * pb.Tz, s_x = (long long)o * o * pb.Tz;
+    const long long s_r = pb.Tz, s_q = pb.rzp, s_x = (long long)o * pb.rzp;
     const long long s_p = (long long)pb.Tx * s_x, s_y = (long long)o * s_p;
     (void)s_r;
-    g.A = GOpT<StageT>{L.S + pb.soff + (long long)q * s_q, map1(1), map3(pb.Tx, o, s_x, s_p, s_y), 0};
+    g.A = GOpT<StageT>{L.S + pb.swoff + (long long)q * s_q, map1(1), map3(pb.Tx, o, s_x, s_p, s_y), 0};
     g.B = GOp{L.A1 + ((long long)pb.Y0 * o * v + pb.X0) * Kp, map1(1),
               map3(pb.Tx, o, Kp, (long long)v * Kp, (long long)o * v * Kp), 0};
     g.C = L.G + ((long long)q * o * v + pb.Z0) * Kp;
@@ -551,10 +599,10 @@ __global__ void __launch_bounds__(256) k_b1c_fp64(GemmLaunch<StageT> L) {
     g.N = o;
     g.K = pb.Ty * o * pb.Tz;
     g.K2 = 0;
-    const long long s_r = pb.Tz, s_q = (long long)o * pb.Tz, s_x = (long long)o * o * pb.Tz;
+    const long long s_r = pb.Tz, s_q = pb.rzp, s_x = (long long)o * pb.rzp;
     const long long s_p = (long long)pb.Tx * s_x, s_y = (long long)o * s_p;
     (void)s_r;
-    g.A = GOpT<StageT>{L.S + pb.soff + (long long)q * s_q, map2(pb.Tx, s_x, s_p), map2((int)oTz, 1, s_y), 1};
+    g.A = GOpT<StageT>{L.S + pb.swoff + (long long)q * s_q, map2(pb.Tx, s_x, s_p), map2((int)oTz, 1, s_y), 1};
     g.B = GOp{L.B2 + ((long long)pb.Y0 * o * v + pb.Z0) * o, map1(1),
               map3(pb.Tz, o, o, (long long)v * o, (long long)o * v * o), 0};
     g.C = L.G + ((long long)q * o * v + pb.X0) * o;
@@ -585,10 +633,10 @@ __global__ void __launch_bounds__(256) k_b1d_fp64(GemmLaunch<StageT> L) {
     g.N = o;
     g.K = o * o * pb.Tx;
     g.K2 = 0;
-    const long long s_r = pb.Tz, s_q = (long long)o * pb.Tz, s_x = (long long)o * o * pb.Tz;
+    const long long s_r = pb.Tz, s_q = pb.rzp, s_x = (long long)o * pb.rzp;
     const long long s_p = (long long)pb.Tx * s_x, s_y = (long long)o * s_p;
     (void)s_r;
-    g.A = GOpT<StageT>{L.S + pb.soff + (long long)y * s_y, map1(1), map3(pb.Tx, o, s_x, s_p, s_q), 0};
+    g.A = GOpT<StageT>{L.S + pb.swoff + (long long)y * s_y, map1(1), map3(pb.Tx, o, s_x, s_p, s_q), 0};
     g.B = GOp{L.A2 + (long long)pb.X0 * o, map1(1),
               map3(pb.Tx, o, o, (long long)v * o, (long long)o * v * o), 0};
     g.C = L.G + (((long long)pb.Y0 + y) * o * v + pb.Z0) * o;
@@ -871,7 +919,11 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
 
     // 16-bit split operands and tensor maps (tensor-core path)
     constexpr int BN = 256;
-    CUtensorMap tmA1, tmB1, tmA2, tmB2;
+    CUtensorMap tmA1, tmB1, tmA2, tmB2, tmA1m, tmA2m, tmB1z[5], tmB2z[5];
+    auto dA1mn = [&]() { static uint64_t dd[5]; dd[0] = P.Kp8; dd[1] = v; dd[2] = o; dd[3] = v; dd[4] = 2; return dd; };
+    auto dA2mn = [&]() { static uint64_t dd[5]; dd[0] = P.Op8; dd[1] = v; dd[2] = o; dd[3] = o; dd[4] = 2; return dd; };
+    auto dB1mn = [&]() { static uint64_t dd[5]; dd[0] = P.Kp8; dd[1] = v; dd[2] = o; dd[3] = o; dd[4] = 2; return dd; };
+    auto dB2mn = [&]() { static uint64_t dd[5]; dd[0] = P.Op8; dd[1] = v; dd[2] = o; dd[3] = v; dd[4] = 2; return dd; };
     if (mixed) {
         const long long npair = (long long)v * (v + 1) / 2;
         TB_KLAUNCH(P_PREP, k_absmax<<<grid1d((long long)o * v * (P.packed ? npair : (long long)v * v), 256), 256, 0, st>>>(
@@ -880,6 +932,9 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                                                                          &ctrl->absmax[1]));
         TB_KLAUNCH(P_PREP, k_absmax<<<grid1d((long long)o * o * v * v, 256), 256, 0, st>>>(io.t2, (long long)o * o * v * v,
                                                                          &ctrl->absmax[2]));
+        TB_KLAUNCH(P_PREP, k_absmax<<<grid1d((long long)o * v * o * v, 256), 256, 0, st>>>(io.ovov, (long long)o * v * o * v, &ctrl->absmax[3]));
+        TB_KLAUNCH(P_PREP, k_absmax<<<grid1d((long long)o * v, 256), 256, 0, st>>>(io.t1, (long long)o * v, &ctrl->absmax[4]));
+        TB_KLAUNCH(P_PREP, k_absmax<<<grid1d((long long)o * v, 256), 256, 0, st>>>(io.fvo, (long long)o * v, &ctrl->absmax[5]));
         TB_KLAUNCH(P_PREP, k_make_scales<<<1, 1, 0, st>>>(ctrl, bf16 ? 0 : 1));
         if (bf16) {
             TB_KLAUNCH(P_PREP, k_prep_A1h<__nv_bfloat16><<<dim3((P.Kp8 + 31) / 32, (d.v + 31) / 32, (unsigned)(o * v)), dim3(32, 8), 0, st>>>(
@@ -914,9 +969,31 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
             if ((rc = make_tmap5(&tmA2, ws + P.off_A2h, bf16, dA2, bA)) != TRIPLES_OK) return rc;
             if ((rc = make_tmap5(&tmB2, ws + P.off_B2h, bf16, dB2, bB)) != TRIPLES_OK) return rc;
         }
+        if (P.want_grad) {
+            // second operands of the adjoint contractions (MN-major boxes)
+            const uint32_t bX[5] = {64, 16, 4, 1, 1};
+            int rc;
+            if ((rc = make_tmap5(&tmA1m, ws + P.off_A1h, bf16, dA1mn(), bX)) != TRIPLES_OK) return rc;
+            if ((rc = make_tmap5(&tmA2m, ws + P.off_A2h, bf16, dA2mn(), bX)) != TRIPLES_OK) return rc;
+            for (int lt = 0; lt < 5; lt++) {
+                const uint32_t tz = 1u << lt;
+                const uint32_t bZ[5] = {64, tz, 64 / tz, 1, 1};
+                if ((rc = make_tmap5(&tmB1z[lt], ws + P.off_B1h, bf16, dB1mn(), bZ)) != TRIPLES_OK) return rc;
+                if ((rc = make_tmap5(&tmB2z[lt], ws + P.off_B2h, bf16, dB2mn(), bZ)) != TRIPLES_OK) return rc;
+            }
+            TB_CUDA(cudaMemsetAsync(SW, 0, P.wbar_elems * 4, st));
+        }
         static bool attr_set = false;
         if (!attr_set) {
             TB_CUDA(cudaFuncSetAttribute(k_f1_tc<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcCfg<BN>::SMEM));
+            TB_CUDA(cudaFuncSetAttribute(k_b1_tc<false, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         TcB1Cfg<false, 128>::SMEM));
+            TB_CUDA(cudaFuncSetAttribute(k_b1_tc<true, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         TcB1Cfg<true, 128>::SMEM));
+            TB_CUDA(cudaFuncSetAttribute(k_b1_tc<false, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         TcB1Cfg<false, 64>::SMEM));
+            TB_CUDA(cudaFuncSetAttribute(k_b1_tc<true, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         TcB1Cfg<true, 64>::SMEM));
             attr_set = true;
         }
     }
@@ -945,11 +1022,13 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                     T.nkb2 = (P.Op8 + kTcBK - 1) / kTcBK;
                     T.S = (float *)S;
                     T.out_scale = &ctrl->out_scale;
+                    T.wmax_bits = &ctrl->wmax_bits;
                     T.err = &ctrl->err;
                     T.bf16 = bf16 ? 1 : 0;
+                    T.kseg = g_kseg_f1;
                     const int tiles = T.cum[ch.nperm];
                     const int grid = tiles < num_sms() ? tiles : num_sms();
-                    TB_KLAUNCH(P_F1, k_f1_tc<BN><<<grid, 192, TcCfg<BN>::SMEM, st>>>(tmA1, tmB1, tmA2, tmB2, T));
+                    TB_KLAUNCH(P_F1, k_f1_tc<BN><<<grid, kF1Threads, TcCfg<BN>::SMEM, st>>>(tmA1, tmB1, tmA2, tmB2, T));
                 } else {
                     GemmLaunch<double> L;
                     L.d = d;
@@ -990,7 +1069,11 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                     F.mo_e = io.mo_energy; F.t1 = io.t1; F.t2 = io.t2; F.ovov = io.ovov; F.fvo = io.fvo;
                     F.S = S;
                     F.SW = SW;
-                    F.split = 0;
+                    F.split = mixed ? (bf16 ? 2 : 1) : 0;
+                    if (mixed && P.want_grad)
+                        TB_KLAUNCH(P_PREP, k_chunk_scale<<<1, 32, 0, st>>>(ctrl, io.mo_energy, d.o, ch.base[0], ch.nabc[0],
+                                                                           ch.base[1], ch.nabc[1], ch.base[2], ch.nabc[2],
+                                                                           io.ybar, bf16 ? 0 : 1));
                     F.wscale = &ctrl->wscale;
                     F.ybar = io.ybar;
                     F.want_grad = P.want_grad;
@@ -1015,6 +1098,53 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                 }
                 TB_KLAUNCH(P_VGRAD, k_vgrad<StageT><<<dim3((unsigned)((maxrows + kVgRows - 1) / kVgRows), ch.nperm), 256, 0, st>>>(VG));
                 // W-term gradients
+                if (mixed) {
+                    for (int t = 0; t < ch.nperm; t++) {
+                        const PermBlock &pb = ch.pb[t];
+                        const uint64_t dW[5] = {(uint64_t)pb.rzp, o, (uint64_t)pb.Tx, o, (uint64_t)(2 * pb.Ty)};
+                        const uint32_t bK[5] = {64, 1, 16, 8, 1};
+                        const uint32_t bM[5] = {64, 1, 16, 4, 1};
+                        CUtensorMap tmWk, tmWm;
+                        void *wbase = (char *)SW + 2 * pb.swoff * 2;
+                        int rc;
+                        if ((rc = make_tmap5(&tmWk, wbase, bf16, dW, bK)) != TRIPLES_OK) return rc;
+                        if ((rc = make_tmap5(&tmWm, wbase, bf16, dW, bM)) != TRIPLES_OK) return rc;
+                        int lz = 0;
+                        while ((1 << lz) < pb.Tz) lz++;
+                        TcB1Params B;
+                        B.d = d;
+                        B.pb = pb;
+                        B.wscale = &ctrl->wscale;
+                        B.err = &ctrl->err;
+                        B.bf16 = bf16 ? 1 : 0;
+                        B.kseg = g_kseg;
+                        const int nsm = num_sms();
+                        auto grid_of = [&](const TcB1Params &q) {
+                            int tiles = q.nbatch * q.ntile_m * q.ntile_n;
+                            return tiles < nsm ? tiles : nsm;
+                        };
+                        // ovvv gradient
+                        B.kind = 0; B.nbatch = pb.Ty; B.ntile_m = (d.o + 7) / 8; B.ntile_n = (d.v + 127) / 128;
+                        B.nk_outer = d.o; B.nk_inner = (d.o * pb.Tz + 63) / 64;
+                        B.G = GA1; B.oscale = &ctrl->scale[1]; B.sign = 1.0;
+                        TB_KLAUNCH(P_B1A, (k_b1_tc<false, 128><<<grid_of(B), kB1Threads, TcB1Cfg<false, 128>::SMEM, st>>>(tmWk, tmB1z[lz], B)));
+                        // t2 gradient, ovvv term
+                        B.kind = 1; B.nbatch = d.o; B.ntile_m = (d.o * pb.Tz + 127) / 128; B.ntile_n = (d.v + 127) / 128;
+                        B.nk_outer = pb.Ty; B.nk_inner = (d.o + 3) / 4;
+                        B.G = GB1; B.oscale = &ctrl->scale[0]; B.sign = 1.0;
+                        TB_KLAUNCH(P_B1B, (k_b1_tc<true, 128><<<grid_of(B), kB1Threads, TcB1Cfg<true, 128>::SMEM, st>>>(tmWm, tmA1m, B)));
+                        // ovoo gradient
+                        B.kind = 2; B.nbatch = d.o; B.ntile_m = (d.o + 7) / 8; B.ntile_n = (d.o + 63) / 64;
+                        B.nk_outer = pb.Ty; B.nk_inner = (d.o * pb.Tz + 63) / 64;
+                        B.G = GA2; B.oscale = &ctrl->scale[1]; B.sign = -1.0;
+                        TB_KLAUNCH(P_B1C, (k_b1_tc<false, 64><<<grid_of(B), kB1Threads, TcB1Cfg<false, 64>::SMEM, st>>>(tmWk, tmB2z[lz], B)));
+                        // t2 gradient, ooov term
+                        B.kind = 3; B.nbatch = pb.Ty; B.ntile_m = (d.o * pb.Tz + 127) / 128; B.ntile_n = (d.o + 63) / 64;
+                        B.nk_outer = d.o; B.nk_inner = (d.o + 3) / 4;
+                        B.G = GB2; B.oscale = &ctrl->scale[0]; B.sign = 1.0;
+                        TB_KLAUNCH(P_B1D, (k_b1_tc<true, 64><<<grid_of(B), kB1Threads, TcB1Cfg<true, 64>::SMEM, st>>>(tmWm, tmA2m, B)));
+                    }
+                } else {
                 GemmLaunch<StageT> L;
                 L.d = d;
                 L.ch = ch;
@@ -1037,6 +1167,7 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                     L.G = GA2;
                     TB_KLAUNCH(P_B1C, k_b1c_fp64<StageT><<<dim3((d.o * ch.pb[t].Tx + kGBM - 1) / kGBM, (d.o + kGBN - 1) / kGBN, d.o),
                                          256, 0, st>>>(L));
+                }
                 }
             }
 
@@ -1062,6 +1193,10 @@ int run_triples(const Plan &P, cudaStream_t st, const TriplesIO &io) {
 }
 
 void set_block_size(int tv) { g_tv_override = tv; }
+void set_kseg(int k) {
+    g_kseg = k > 0 ? k : 1;
+    g_kseg_f1 = g_kseg;
+}
 
 void profile_enable(int on) {
     g_prof = on != 0;
@@ -1166,6 +1301,8 @@ int triples_last_cuda_error(void) { return tb::last_cuda_error(); }
 const char *triples_version(void) { return "0.1.0"; }
 
 void triples_set_block_size(int tv) { tb::set_block_size(tv); }
+
+void triples_set_accumulation_segment(int kblocks) { tb::set_kseg(kblocks); }
 
 void triples_profile_enable(int on) { tb::profile_enable(on); }
 

@@ -22,8 +22,11 @@ struct Ctrl {
     float out_scale;              // 1 / (scale[0] * scale[1])
     float pad_;
     double wscale;                // per-chunk power-of-two scale of the split Wbar
-    unsigned long long absmax[4]; // bit patterns of max |ovvv|, |ovoo|, |t2|
+    unsigned long long absmax[6]; // bit patterns of max |ovvv|, |ovoo|, |t2|, |ovov|, |t1|, |fvo|
+    unsigned wmax_bits;           // bit pattern of max |W| of the current chunk (F1)
 };
+
+static_assert(sizeof(Ctrl) <= kCtrlBytes, "control block too large");
 
 struct Plan {
     Dims d;
@@ -33,7 +36,7 @@ struct Plan {
     int max_items;   // largest |A||B||C| over chunks
     int f2_gy;       // epilogue grid.y upper bound
     int Kp8, Op8;    // 16-byte padded contraction lengths of the 16-bit operands
-    size_t stage_elems, stage_bytes;
+    size_t stage_elems, stage_bytes, wbar_elems;
     size_t off_ctrl;
     size_t off_A1, off_B1, off_A2, off_B2, off_S, off_SW;
     size_t off_A1h, off_B1h, off_A2h, off_B2h;

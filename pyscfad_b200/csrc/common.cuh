@@ -112,10 +112,12 @@ __host__ __device__ inline int block_start(const Dims &d, int b) {
 // The six orderings of three slots, lexicographic: index = 2*first + (second is
 // the larger of the two remaining).
 __host__ __device__ inline void perm_of(int s, int out[3]) {
-    const int P[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
-    out[0] = P[s][0];
-    out[1] = P[s][1];
-    out[2] = P[s][2];
+    const int first = s >> 1;
+    const int lo = (first == 0) ? 1 : 0;
+    const int hi = (first == 2) ? 1 : 2;
+    out[0] = first;
+    out[1] = (s & 1) ? hi : lo;
+    out[2] = (s & 1) ? lo : hi;
 }
 
 __host__ __device__ inline int perm_index(int a, int b) {

@@ -52,11 +52,16 @@ struct F2P {
     double *mo_bar;
 };
 
+// Shared-memory region layout: element (y,x,z) at y*SY + x*SX + z.  The padded
+// strides keep the permuted gathers of a warp within 2-way bank conflicts.
 template <int SB>
 struct F2Smem {
-    static constexpr int REG = SB * SB * SB;
+    static constexpr int SX = SB;
+    static constexpr int SY = (SB == 8) ? 69 : SB * SB + 1;
+    static constexpr int REG = SY * SB;
     static constexpr int NV = 3 * SB;
-    static constexpr int TAB = 6 * NV * NV;
+    static constexpr int NVP = NV + 1;
+    static constexpr int TAB = 6 * NV * NVP;
 };
 
 template <typename StageT, int SB>
@@ -66,11 +71,56 @@ __host__ __device__ constexpr size_t f2_smem_bytes() {
 
 __device__ __forceinline__ int pair_index(int sp, int sq) { return 2 * sp + (sq > sp ? sq - 1 : sq); }
 
+// A z run of N contiguous values moved with the widest aligned vector access:
+// one warp instruction then fills whole 32-byte sectors instead of touching
+// 32 sectors with a 2- or 4-byte write each.  Partial or unaligned runs
+// (remainder blocks) fall back to scalar accesses.
+template <typename T, int N>
+union RunBuf {
+    static constexpr int BYTES = N * (int)sizeof(T);
+    static constexpr int VB = BYTES >= 16 ? 16 : (BYTES >= 8 ? 8 : 4);
+    T e[N];
+    uint4 u4[BYTES / 16 > 0 ? BYTES / 16 : 1];
+    uint2 u2[BYTES / 8 > 0 ? BYTES / 8 : 1];
+};
+
+template <typename T, int N>
+__device__ __forceinline__ void st_run(T *dst, const RunBuf<T, N> &b, int n) {
+    using B = RunBuf<T, N>;
+    const uintptr_t a = reinterpret_cast<uintptr_t>(dst);
+    if (n == N && B::VB == 16 && (a & 15) == 0) {
+#pragma unroll
+        for (int c = 0; c < B::BYTES / 16; c++) reinterpret_cast<uint4 *>(dst)[c] = b.u4[c];
+    } else if (n == N && B::VB == 8 && (a & 7) == 0) {
+#pragma unroll
+        for (int c = 0; c < B::BYTES / 8; c++) reinterpret_cast<uint2 *>(dst)[c] = b.u2[c];
+    } else {
+#pragma unroll
+        for (int z = 0; z < N; z++)
+            if (z < n) dst[z] = b.e[z];
+    }
+}
+
+template <typename T, int N>
+__device__ __forceinline__ void ld_run(RunBuf<T, N> &b, const T *src, int n) {
+    using B = RunBuf<T, N>;
+    const uintptr_t a = reinterpret_cast<uintptr_t>(src);
+    if (n == N && B::VB == 16 && (a & 15) == 0) {
+#pragma unroll
+        for (int c = 0; c < B::BYTES / 16; c++) b.u4[c] = reinterpret_cast<const uint4 *>(src)[c];
+    } else {
+#pragma unroll
+        for (int z = 0; z < N; z++) b.e[z] = (z < n) ? src[z] : (T)0;
+    }
+}
+
 template <typename StageT, int SB>
 __global__ void __launch_bounds__(SB *SB *SB) k_f2t(F2P<StageT> P) {
     constexpr int NT = SB * SB * SB;
     constexpr int REG = F2Smem<SB>::REG;
     constexpr int NV = F2Smem<SB>::NV;
+    constexpr int NVP = F2Smem<SB>::NVP;
+    constexpr int SX = F2Smem<SB>::SX, SY = F2Smem<SB>::SY;
     extern __shared__ __align__(16) uint8_t f2_smem[];
     StageT *sW = reinterpret_cast<StageT *>(f2_smem);
     StageT *sWb = sW + 36 * REG;
@@ -82,6 +132,8 @@ __global__ void __launch_bounds__(SB *SB *SB) k_f2t(F2P<StageT> P) {
     __shared__ double s_red[2][NT / 32 > 0 ? NT / 32 : 1];
     __shared__ int s_reg[6][6];     // [ordering pi][role rho] -> region
     __shared__ int s_rd[36][9];     // per region: pi, rho, tau, lx, ly, lz, p, q, r
+    __shared__ long long s_gb[36], s_wb[36];    // staging / Wbar base offsets of each region
+    __shared__ int s_gs[36][2], s_ws[36][2];    // (y, x) strides in staging / Wbar
     __shared__ int s_ntile[2];
 
     const Dims &d = P.d;
@@ -97,46 +149,58 @@ __global__ void __launch_bounds__(SB *SB *SB) k_f2t(F2P<StageT> P) {
     cs[1] = (R.st[1] == R.st[0]) ? 0 : 1;
     cs[2] = (R.st[2] == R.st[1]) ? cs[1] : ((R.st[2] == R.st[0]) ? 0 : 2);
 
-    if (tid == 0) {
-        // distinct occupied orderings and distinct sub-range orderings
-        int rid[6], pid[6], nrole = 0, npi = 0;
-        for (int rho = 0; rho < 6; rho++) {
-            int pr[3];
-            perm_of(rho, pr);
-            rid[rho] = -1;
-            for (int r2 = 0; r2 < rho; r2++) {
-                int q2[3];
-                perm_of(r2, q2);
-                if (ijk[pr[0]] == ijk[q2[0]] && ijk[pr[1]] == ijk[q2[1]] && ijk[pr[2]] == ijk[q2[2]]) {
-                    rid[rho] = rid[r2];
-                    break;
-                }
+    // distinct occupied orderings (roles) and distinct sub-range orderings;
+    // thread (pi, rho) < 36 fills its table entry
+    if (tid < 36) {
+        const int pi = tid / 6, rho = tid % 6;
+        int pr[3], pp[3];
+        perm_of(rho, pr);
+        perm_of(pi, pp);
+        // dense index of a value = number of distinct values first seen before it
+        auto same_ijk = [&](int ra, int rb) {
+            int qa[3], qb[3];
+            perm_of(ra, qa);
+            perm_of(rb, qb);
+            return ijk[qa[0]] == ijk[qb[0]] && ijk[qa[1]] == ijk[qb[1]] && ijk[qa[2]] == ijk[qb[2]];
+        };
+        auto same_rng = [&](int pa, int pb2) {
+            int qa[3], qb[3];
+            perm_of(pa, qa);
+            perm_of(pb2, qb);
+            return R.st[qa[0]] == R.st[qb[0]] && R.st[qa[1]] == R.st[qb[1]] && R.st[qa[2]] == R.st[qb[2]];
+        };
+        int rfirst_at = rho, pfirst_at = pi;
+        for (int r2 = 5; r2 >= 0; r2--)
+            if (same_ijk(r2, rho)) rfirst_at = r2;
+        for (int p2 = 5; p2 >= 0; p2--)
+            if (same_rng(p2, pi)) pfirst_at = p2;
+        int rid = 0, nrole = 0, pid = 0, npi = 0;
+        for (int r2 = 0; r2 < 6; r2++) {
+            bool first = true;
+            for (int r3 = 0; r3 < r2; r3++)
+                if (same_ijk(r2, r3)) first = false;
+            if (first) {
+                nrole++;
+                if (r2 < rfirst_at) rid++;
             }
-            if (rid[rho] < 0) rid[rho] = nrole++;
         }
-        for (int pi = 0; pi < 6; pi++) {
-            int pp[3];
-            perm_of(pi, pp);
-            pid[pi] = -1;
-            for (int p2 = 0; p2 < pi; p2++) {
-                int q2[3];
-                perm_of(p2, q2);
-                if (R.st[pp[0]] == R.st[q2[0]] && R.st[pp[1]] == R.st[q2[1]] && R.st[pp[2]] == R.st[q2[2]]) {
-                    pid[pi] = pid[p2];
-                    break;
-                }
+        for (int p2 = 0; p2 < 6; p2++) {
+            bool first = true;
+            for (int p3 = 0; p3 < p2; p3++)
+                if (same_rng(p2, p3)) first = false;
+            if (first) {
+                npi++;
+                if (p2 < pfirst_at) pid++;
             }
-            if (pid[pi] < 0) pid[pi] = npi++;
         }
-        for (int pi = 0; pi < 6; pi++)
-            for (int rho = 0; rho < 6; rho++) s_reg[pi][rho] = pid[pi] * nrole + rid[rho];
-        s_ntile[0] = nrole;
-        s_ntile[1] = npi;
-        for (int a = 35; a >= 0; a--) {   // first (pi, rho) of each region wins
-            const int pi = a / 6, rho = a % 6, reg = s_reg[pi][rho];
-            int pp[3], pr[3];
-            perm_of(pi, pp);
-            perm_of(rho, pr);
+        const int rfirst = (rfirst_at == rho), pfirst = (pfirst_at == pi);
+        const int reg = pid * nrole + rid;
+        s_reg[pi][rho] = reg;
+        if (tid == 0) {
+            s_ntile[0] = nrole;
+            s_ntile[1] = npi;
+        }
+        if (rfirst && pfirst) {
             s_rd[reg][0] = pi;
             s_rd[reg][1] = rho;
             s_rd[reg][3] = R.len[pp[0]];
@@ -169,30 +233,46 @@ __global__ void __launch_bounds__(SB *SB *SB) k_f2t(F2P<StageT> P) {
     };
 
     const int nreg = nrole * npi;
-    if (tid < nreg) s_rd[tid][2] = tau_of(s_rd[tid][0]);
-    __syncthreads();
-
-    // ---- load the distinct regions: element (reg, yy, xx, zz) ----
-    for (int e = tid; e < nreg * REG; e += NT) {
-        const int reg = e / REG;
-        const int zz = e % SB, xx = (e / SB) % SB, yy = (e / (SB * SB)) % SB;
-        const int *rd = s_rd[reg];
-        const int lx = rd[3], ly = rd[4], lz = rd[5];
-        if (xx >= lx || yy >= ly || zz >= lz) continue;
+    if (tid < nreg) {
+        const int *rd = s_rd[tid];
+        const int tau = tau_of(rd[0]);
+        s_rd[tid][2] = tau;
         int pp[3];
         perm_of(rd[0], pp);
-        const PermBlock &pb = P.ch.pb[rd[2]];
+        const PermBlock &pb = P.ch.pb[tau];
         const int p = rd[6], q = rd[7], r = rd[8];
-        const int x = R.st[pp[0]] + xx, y = R.st[pp[1]] + yy, z = R.st[pp[2]] + zz;
-        const long long g = pb.soff +
-                            ((((long long)(p * o + q) * pb.Ty + (y - pb.Y0)) * pb.Tx + (x - pb.X0)) * o + r) *
-                                pb.Tz +
-                            (z - pb.Z0);
-        sW[reg * REG + (yy * lx + xx) * lz + zz] = P.S[g];
+        const int xs = R.st[pp[0]] - pb.X0, ys = R.st[pp[1]] - pb.Y0, zs = R.st[pp[2]] - pb.Z0;
+        // staging S_tau[p][q][y][x][r][z]
+        const long long gy = (long long)pb.Tx * o * pb.Tz, gx = (long long)o * pb.Tz;
+        s_gb[tid] = pb.soff + (long long)(p * o + q) * pb.Ty * gy + ys * gy + xs * gx + (long long)r * pb.Tz + zs;
+        s_gs[tid][0] = (int)gy;
+        s_gs[tid][1] = (int)gx;
+        // Wbar_tau[y][p][x][q][rzp]
+        const long long wx = (long long)o * pb.rzp, wy = (long long)o * pb.Tx * wx;
+        s_wb[tid] = (long long)ys * wy + (long long)p * pb.Tx * wx + xs * wx + (long long)q * pb.rzp + (long long)r * pb.Tz + zs;
+        s_ws[tid][0] = (int)wy;
+        s_ws[tid][1] = (int)wx;
+    }
+    __syncthreads();
+
+    // ---- load the distinct regions, one (y, x) run of z values per thread step ----
+    for (int e = tid; e < nreg * SB * SB; e += NT) {
+        const int reg = e / (SB * SB), yy = (e / SB) % SB, xx = e % SB;
+        const int *rd = s_rd[reg];
+        const int lx = rd[3], ly = rd[4], lz = rd[5];
+        if (xx >= lx || yy >= ly) continue;
+        const StageT *src = P.S + s_gb[reg] + (long long)yy * s_gs[reg][0] + (long long)xx * s_gs[reg][1];
+        StageT *dst = sW + reg * REG + yy * SY + xx * SX;
+        RunBuf<StageT, SB> b;
+        ld_run(b, src, lz);
+#pragma unroll
+        for (int zz = 0; zz < SB; zz++)
+            if (zz < lz) dst[zz] = b.e[zz];
     }
     // ---- tables for the V terms ----
     for (int e = tid; e < 6 * NV * NV; e += NT) {
         const int pair = e / (NV * NV), xl = (e / NV) % NV, yl = e % NV;
+        const int te = (pair * NV + xl) * NVP + yl;
         const int sp = pair / 2, rem = pair % 2;
         const int sq = (rem < sp) ? rem : rem + 1;   // inverse of pair_index
         const int sx = xl / SB, sy = yl / SB;
@@ -203,8 +283,8 @@ __global__ void __launch_bounds__(SB *SB *SB) k_f2t(F2P<StageT> P) {
             ov = (StageT)P.ovov[(((long long)p * v + x) * o + q) * v + y];
             tt = (StageT)P.t2[(((long long)q * o + p) * v + y) * v + x];
         }
-        tOV[e] = ov;
-        tT2[e] = tt;
+        tOV[te] = ov;
+        tT2[te] = tt;
     }
     for (int e = tid; e < 3 * NV; e += NT) {
         const int sr = e / NV, zl = e % NV, sz = zl / SB;
@@ -239,14 +319,13 @@ __global__ void __launch_bounds__(SB *SB *SB) k_f2t(F2P<StageT> P) {
                 int pp[3], pt[3];
                 perm_of(pi, pp);
                 perm_of(tau, pt);
-                const int lx = R.len[pp[0]], lz = R.len[pp[2]];
-                const int id = s_reg[pi][tau] * REG + (loc[pp[1]] * lx + loc[pp[0]]) * lz + loc[pp[2]];
+                const int id = s_reg[pi][tau] * REG + loc[pp[1]] * SY + loc[pp[0]] * SX + loc[pp[2]];
                 idx[s][tau] = id;
                 sw += (double)sW[id];
                 const int pair = pair_index(pt[0], pt[1]);
                 const int xl = vl[pp[0]], yl = vl[pp[1]], zl = vl[pp[2]];
-                sv += (double)tOV[(pair * NV + xl) * NV + yl] * (double)tT1[pt[2] * NV + zl] +
-                      (double)tT2[(pair * NV + xl) * NV + yl] * (double)tFV[pt[2] * NV + zl];
+                sv += (double)tOV[(pair * NV + xl) * NVP + yl] * (double)tT1[pt[2] * NV + zl] +
+                      (double)tT2[(pair * NV + xl) * NVP + yl] * (double)tFV[pt[2] * NV + zl];
             }
             WW[s] = sw;
             X[s] = sw + 0.5 * sv;
@@ -274,27 +353,49 @@ __global__ void __launch_bounds__(SB *SB *SB) k_f2t(F2P<StageT> P) {
             const double g0 = P.ybar * cfac * rD;
             const double dD = -P.ybar * cfac * esum * rD * rD;
             dd_loc = dD;
+            if (n_ijk == 6 && n_abc == 6) {
+                // all 36 raw positions of the orbit are distinct
 #pragma unroll
-            for (int s = 0; s < 6; s++)
+                for (int s = 0; s < 6; s++) {
+                    const StageT gw = (StageT)(g0 * (Z[s] + RW[s]));
+                    const StageT gv = (StageT)(g0 * 0.5 * RW[s]);
 #pragma unroll
-                for (int tau = 0; tau < 6; tau++) {
-                    sW[idx[s][tau]] = (StageT)0;
-                    sWb[idx[s][tau]] = (StageT)0;
+                    for (int tau = 0; tau < 6; tau++) {
+                        sWb[idx[s][tau]] = gw;
+                        sW[idx[s][tau]] = gv;
+                    }
                 }
+            } else {
+                // repeated indices: several (s, tau) land on one raw position
 #pragma unroll
-            for (int s = 0; s < 6; s++) {
-                const StageT gw = (StageT)(g0 * (Z[s] + RW[s]));
-                const StageT gv = (StageT)(g0 * 0.5 * RW[s]);
+                for (int s = 0; s < 6; s++)
 #pragma unroll
-                for (int tau = 0; tau < 6; tau++) {
-                    sWb[idx[s][tau]] += gw;
-                    sW[idx[s][tau]] += gv;
+                    for (int tau = 0; tau < 6; tau++) {
+                        sW[idx[s][tau]] = (StageT)0;
+                        sWb[idx[s][tau]] = (StageT)0;
+                    }
+#pragma unroll
+                for (int s = 0; s < 6; s++) {
+                    const StageT gw = (StageT)(g0 * (Z[s] + RW[s]));
+                    const StageT gv = (StageT)(g0 * 0.5 * RW[s]);
+#pragma unroll
+                    for (int tau = 0; tau < 6; tau++) {
+                        sWb[idx[s][tau]] += gw;
+                        sW[idx[s][tau]] += gv;
+                    }
                 }
             }
-            atomicAdd(&s_ev[vl[0]], -dD);
+            if (SB * SB < 32) atomicAdd(&s_ev[vl[0]], -dD);
             atomicAdd(&s_ev[vl[1]], -dD);
             atomicAdd(&s_ev[vl[2]], -dD);
         }
+    }
+    // with SB^2 >= 32 the a-slot index (tid / SB^2) is uniform across a warp: reduce first
+    if (SB * SB >= 32 && P.want_grad) {
+        double dsum = valid ? -dd_loc : 0.0;
+        for (int off = 16; off > 0; off >>= 1) dsum += __shfl_down_sync(0xffffffffu, dsum, off);
+        const int la = tid / (SB * SB);
+        if ((tid & 31) == 0 && la < R.len[0] && dsum != 0.0) atomicAdd(&s_ev[cs[0] * SB + la], dsum);
     }
 
     // ---- block reductions ----
@@ -326,41 +427,49 @@ __global__ void __launch_bounds__(SB *SB *SB) k_f2t(F2P<StageT> P) {
             const int sl = e / SB, l = e % SB;
             if (l < R.len[sl] && s_ev[e] != 0.0) atomicAdd(&P.mo_bar[o + R.st[sl] + l], s_ev[e]);
         }
-        // ---- write back: Vbar in place, Wbar to its buffer ----
-        const double wsc = (P.split != 0) ? *P.wscale : 1.0;
-        for (int e = tid; e < nreg * REG; e += NT) {
-            const int reg = e / REG;
-            const int zz = e % SB, xx = (e / SB) % SB, yy = (e / (SB * SB)) % SB;
+        // ---- write back: Vbar in place, Wbar to its buffer, one z run per step ----
+        const float wscf = (P.split != 0) ? (float)*P.wscale : 1.0f;
+        for (int e = tid; e < nreg * SB * SB; e += NT) {
+            const int reg = e / (SB * SB), yy = (e / SB) % SB, xx = e % SB;
             const int *rd = s_rd[reg];
             const int lx = rd[3], ly = rd[4], lz = rd[5];
-            if (xx >= lx || yy >= ly || zz >= lz) continue;
-            int pp[3];
-            perm_of(rd[0], pp);
+            if (xx >= lx || yy >= ly) continue;
             const PermBlock &pb = P.ch.pb[rd[2]];
-            const int p = rd[6], q = rd[7], r = rd[8];
-            const int xl = R.st[pp[0]] + xx - pb.X0, yl = R.st[pp[1]] + yy - pb.Y0, zl = R.st[pp[2]] + zz - pb.Z0;
-            const int si = reg * REG + (yy * lx + xx) * lz + zz;
-            const long long g = pb.soff + ((((long long)(p * o + q) * pb.Ty + yl) * pb.Tx + xl) * o + r) * pb.Tz + zl;
-            P.S[g] = sW[si];
-            const long long wl =
-                ((((long long)yl * o + p) * pb.Tx + xl) * o + q) * pb.rzp + (long long)r * pb.Tz + zl;
-            const double wb = (double)sWb[si];
+            StageT *vdst = P.S + s_gb[reg] + (long long)yy * s_gs[reg][0] + (long long)xx * s_gs[reg][1];
+            const int si = reg * REG + yy * SY + xx * SX;
+            const long long wl = s_wb[reg] + (long long)yy * s_ws[reg][0] + (long long)xx * s_ws[reg][1];
+            const long long half = (long long)pb.Ty * o * pb.Tx * o * pb.rzp;
+            RunBuf<StageT, SB> bv;
+#pragma unroll
+            for (int zz = 0; zz < SB; zz++) bv.e[zz] = sW[si + zz];
+            st_run(vdst, bv, lz);
             if (P.split == 0) {
-                reinterpret_cast<StageT *>(P.SW)[pb.swoff + wl] = sWb[si];
-            } else {
-                const long long half = (long long)pb.Ty * o * pb.Tx * o * pb.rzp;
-                const double xs = wb * wsc;
-                if (P.split == 1) {
-                    __half *dst = reinterpret_cast<__half *>(P.SW) + 2 * pb.swoff;
-                    const __half hi = __double2half(xs);
-                    dst[wl] = hi;
-                    dst[half + wl] = __double2half(xs - (double)__half2float(hi));
-                } else {
-                    __nv_bfloat16 *dst = reinterpret_cast<__nv_bfloat16 *>(P.SW) + 2 * pb.swoff;
-                    const __nv_bfloat16 hi = __double2bfloat16(xs);
-                    dst[wl] = hi;
-                    dst[half + wl] = __double2bfloat16(xs - (double)__bfloat162float(hi));
+#pragma unroll
+                for (int zz = 0; zz < SB; zz++) bv.e[zz] = sWb[si + zz];
+                st_run(reinterpret_cast<StageT *>(P.SW) + pb.swoff + wl, bv, lz);
+            } else if (P.split == 1) {
+                // exact power-of-two scaling, then a two-term 16-bit split in FP32
+                RunBuf<__half, SB> bh, bl;
+#pragma unroll
+                for (int zz = 0; zz < SB; zz++) {
+                    const float xs = (float)sWb[si + zz] * wscf;
+                    bh.e[zz] = __float2half_rn(xs);
+                    bl.e[zz] = __float2half_rn(xs - __half2float(bh.e[zz]));
                 }
+                __half *dst = reinterpret_cast<__half *>(P.SW) + 2 * pb.swoff + wl;
+                st_run(dst, bh, lz);
+                st_run(dst + half, bl, lz);
+            } else {
+                RunBuf<__nv_bfloat16, SB> bh, bl;
+#pragma unroll
+                for (int zz = 0; zz < SB; zz++) {
+                    const float xs = (float)sWb[si + zz] * wscf;
+                    bh.e[zz] = __float2bfloat16_rn(xs);
+                    bl.e[zz] = __float2bfloat16_rn(xs - __bfloat162float(bh.e[zz]));
+                }
+                __nv_bfloat16 *dst = reinterpret_cast<__nv_bfloat16 *>(P.SW) + 2 * pb.swoff + wl;
+                st_run(dst, bh, lz);
+                st_run(dst + half, bl, lz);
             }
         }
     }

@@ -17,8 +17,18 @@
 // over occupied-triplet orbits), and the adjoint
 //   Wbar(d) = c (Z + R WW)/D, Vbar(d) = c (R WW)/(2D), dE/dD = -c sum WW Z / D^2
 // (ccsd_t_vjp.c:64-117) scattered back to every raw position of the orbit.
-// Vbar overwrites W in place; Wbar goes to its own buffer in the layout the
-// gradient contractions read: [h][y][p][x][q][r][z].
+// Wbar goes to its own buffer in the layout the gradient contractions read:
+// [h][y][p][x][q][r][z].  Vbar never leaves the CTA: since
+//   v^{pqr}_{xyz} = ovov[p,x,q,y] t1[r,z] + t2[q,p,y,x] fvo[z,r]
+// and the CTA already holds those factors in its V-term tables, its
+// contributions to ovov_bar / t2_bar (row sums over the z run of a thread)
+// and to t1_bar / fvo_bar (column sums, reduced across the warp) are added
+// to the global gradients directly (FP64 reductions).
+//
+// Item results (Wbar, Vbar per ordering s) are written once per item into
+// shared memory over the dead W tile; the write-back maps every raw position
+// to its item(s) through the (sub-range ordering, occupied ordering) pairs of
+// its region, which in degenerate cases (repeated indices) are several.
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -41,15 +51,14 @@ struct F2P {
     F2Sub sub[kMaxSub];
     const int *ijk;
     const double *mo_e, *t1, *t2, *ovov, *fvo;
-    StageT *S;          // W in, Vbar out; per ordering tau: [p][q][y][x][r][z] at ch.pb[tau].soff
+    const StageT *S;    // W per ordering tau: [p][q][y][x][r][z] at ch.pb[tau].soff
     void *SW;           // Wbar out; per tau at 2*soff: [h][y][p][x][q][r][z] (split) or at soff: [y][p][x][q][r][z]
     int split;          // 0: StageT, 1: fp16 hi/lo, 2: bf16 hi/lo
     const double *wscale;
     double ybar;
     int want_grad;
-    double *e_part, *e_acc;
-    unsigned *counter;
-    double *mo_bar;
+    double *e_part;     // energy partial of each CTA
+    double *mo_bar, *t1_bar, *fvo_bar, *ovov_bar, *t2_bar;
 };
 
 // Shared-memory region layout: element (y,x,z) at y*SY + x*SX + z.  The padded
@@ -62,11 +71,15 @@ struct F2Smem {
     static constexpr int NV = 3 * SB;
     static constexpr int NVP = NV + 1;
     static constexpr int TAB = 6 * NV * NVP;
+    static constexpr int ITEMS = SB * SB * SB;
+    static constexpr int NT = (SB == 8) ? 256 : ITEMS;     // threads per CTA
+    static constexpr int IPT = ITEMS / NT;                  // items per thread
+    static_assert(12 * ITEMS <= 36 * REG, "item results overlay the W tile");
 };
 
 template <typename StageT, int SB>
 __host__ __device__ constexpr size_t f2_smem_bytes() {
-    return sizeof(StageT) * (2 * 36 * F2Smem<SB>::REG + 2 * F2Smem<SB>::TAB + 2 * 3 * F2Smem<SB>::NV);
+    return sizeof(StageT) * (36 * F2Smem<SB>::REG + 2 * F2Smem<SB>::TAB + 2 * 3 * F2Smem<SB>::NV);
 }
 
 __device__ __forceinline__ int pair_index(int sp, int sq) { return 2 * sp + (sq > sp ? sq - 1 : sq); }
@@ -114,31 +127,55 @@ __device__ __forceinline__ void ld_run(RunBuf<T, N> &b, const T *src, int n) {
     }
 }
 
+// Sum NV (power of two) per-lane values over aligned groups of G lanes
+// (NV <= G <= 32, G a power of two); afterwards lane l holds the group total
+// of value (l % NV).
+template <int NV, int G>
+__device__ __forceinline__ double group_reduce_scatter(double (&v)[NV], int lane) {
+#pragma unroll
+    for (int h = NV / 2; h >= 1; h /= 2) {
+        const bool up = (lane & h) != 0;
+#pragma unroll
+        for (int i = 0; i < h; i++) {
+            const double send = up ? v[i] : v[i + h];
+            const double keep = up ? v[i + h] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, h);
+        }
+    }
+    double r = v[0];
+#pragma unroll
+    for (int h = NV; h < G; h *= 2) r += __shfl_xor_sync(0xffffffffu, r, h);
+    return r;
+}
+
 template <typename StageT, int SB>
-__global__ void __launch_bounds__(SB *SB *SB) k_f2t(F2P<StageT> P) {
-    constexpr int NT = SB * SB * SB;
-    constexpr int REG = F2Smem<SB>::REG;
-    constexpr int NV = F2Smem<SB>::NV;
-    constexpr int NVP = F2Smem<SB>::NVP;
-    constexpr int SX = F2Smem<SB>::SX, SY = F2Smem<SB>::SY;
+__global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4) k_f2t(F2P<StageT> P) {
+    using C = F2Smem<SB>;
+    constexpr int NT = C::NT, IPT = C::IPT, ITEMS = C::ITEMS;
+    constexpr int REG = C::REG, NV = C::NV, NVP = C::NVP;
+    constexpr int SX = C::SX, SY = C::SY;
+    constexpr int NW = NT / 32;
     extern __shared__ __align__(16) uint8_t f2_smem[];
     StageT *sW = reinterpret_cast<StageT *>(f2_smem);
-    StageT *sWb = sW + 36 * REG;
-    StageT *tOV = sWb + 36 * REG;
-    StageT *tT2 = tOV + F2Smem<SB>::TAB;
-    StageT *tT1 = tT2 + F2Smem<SB>::TAB;
+    StageT *sG = sW;                      // item results [12][ITEMS] once W is consumed
+    StageT *tOV = sW + 36 * REG;
+    StageT *tT2 = tOV + C::TAB;
+    StageT *tT1 = tT2 + C::TAB;
     StageT *tFV = tT1 + 3 * NV;
     __shared__ double s_ev[NV];
-    __shared__ double s_red[2][NT / 32 > 0 ? NT / 32 : 1];
-    __shared__ int s_reg[6][6];     // [ordering pi][role rho] -> region
-    __shared__ int s_rd[36][9];     // per region: pi, rho, tau, lx, ly, lz, p, q, r
-    __shared__ long long s_gb[36], s_wb[36];    // staging / Wbar base offsets of each region
-    __shared__ int s_gs[36][2], s_ws[36][2];    // (y, x) strides in staging / Wbar
+    __shared__ double s_red[2][NW];
+    __shared__ int s_reg[6][6];               // [ordering pi][role rho] -> region
+    __shared__ int s_rd[36][9];               // per region: pi, rho, tau, lx, ly, lz, p, q, r
+    __shared__ long long s_gb[36], s_wb[36];  // staging / Wbar base offsets of each region
+    __shared__ int s_gs[36][2], s_ws[36][2];  // (y, x) strides in staging / Wbar
     __shared__ int s_ntile[2];
+    __shared__ unsigned char s_ncombo[36];    // (pi, rho) pairs of each region ...
+    __shared__ unsigned char s_combo[36][36]; // ... as pi*6 + rho, ascending
+    __shared__ unsigned char s_sof[36];       // ordering s with perm_compose(s, rho) = pi
 
     const Dims &d = P.d;
     const int o = d.o, v = d.v;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int rep = blockIdx.x;
     const F2Sub &R = P.sub[blockIdx.y];
     const int ijk[3] = {P.ijk[3 * rep], P.ijk[3 * rep + 1], P.ijk[3 * rep + 2]};
@@ -196,6 +233,8 @@ __global__ void __launch_bounds__(SB *SB *SB) k_f2t(F2P<StageT> P) {
         const int rfirst = (rfirst_at == rho), pfirst = (pfirst_at == pi);
         const int reg = pid * nrole + rid;
         s_reg[pi][rho] = reg;
+        for (int s2 = 0; s2 < 6; s2++)
+            if (perm_compose(s2, rho) == pi) s_sof[tid] = (unsigned char)s2;
         if (tid == 0) {
             s_ntile[0] = nrole;
             s_ntile[1] = npi;
@@ -214,9 +253,22 @@ __global__ void __launch_bounds__(SB *SB *SB) k_f2t(F2P<StageT> P) {
     for (int e = tid; e < NV; e += NT) s_ev[e] = 0.0;
     __syncthreads();
     const int nrole = s_ntile[0], npi = s_ntile[1];
+    const int nreg = nrole * npi;
 
-    // region descriptors are recomputed per use from (pi, rho); find the
-    // staging ordering tau of a sub-range ordering
+    // the (pi, rho) pairs of each region in ascending order (deterministic sums)
+    if (tid < 36) {
+        const int reg = s_reg[tid / 6][tid % 6];
+        int rank = 0, cnt = 0;
+        for (int t = 0; t < 36; t++)
+            if (s_reg[t / 6][t % 6] == reg) {
+                if (t < tid) rank++;
+                cnt++;
+            }
+        s_combo[reg][rank] = (unsigned char)tid;
+        if (rank == 0) s_ncombo[reg] = (unsigned char)cnt;
+    }
+
+    // region descriptors; find the staging ordering tau of a sub-range ordering
     auto block_of = [&](int start) {
         for (int t = 0; t < 3; t++)
             if (start >= P.ch.base[t] && start < P.ch.base[t] + P.ch.nabc[t]) return P.ch.blk[t];
@@ -231,8 +283,6 @@ __global__ void __launch_bounds__(SB *SB *SB) k_f2t(F2P<StageT> P) {
             if (P.ch.pb[t].bx == bx && P.ch.pb[t].by == by && P.ch.pb[t].bz == bz) break;
         return t;
     };
-
-    const int nreg = nrole * npi;
     if (tid < nreg) {
         const int *rd = s_rd[tid];
         const int tau = tau_of(rd[0]);
@@ -299,118 +349,96 @@ __global__ void __launch_bounds__(SB *SB *SB) k_f2t(F2P<StageT> P) {
     }
     __syncthreads();
 
-    // ---- one orbit item per thread ----
+    // ---- orbit items (IPT per thread) ----
+    const int i = ijk[0], j = ijk[1], k = ijk[2];
+    const int n_ijk = (i == k) ? 1 : ((i == j || j == k) ? 3 : 6);
+    const double e_ijk = P.mo_e[i] + P.mo_e[j] + P.mo_e[k];
     double e_loc = 0.0, dd_loc = 0.0;
-    const int loc[3] = {tid / (SB * SB), (tid / SB) % SB, tid % SB};
-    bool valid = loc[0] < R.len[0] && loc[1] < R.len[1] && loc[2] < R.len[2];
-    const int abc[3] = {R.st[0] + loc[0], R.st[1] + loc[1], R.st[2] + loc[2]};
-    if (valid && cs[1] == 0 && abc[0] < abc[1]) valid = false;
-    if (valid && cs[2] == cs[1] && abc[1] < abc[2]) valid = false;
-    if (valid) {
-        const int vl[3] = {cs[0] * SB + loc[0], cs[1] * SB + loc[1], cs[2] * SB + loc[2]};
-        double WW[6], X[6];
-        int idx[6][6];
+    StageT gres[IPT][12];
+    bool gvalid[IPT];
 #pragma unroll
-        for (int s = 0; s < 6; s++) {
-            double sw = 0.0, sv = 0.0;
+    for (int it = 0; it < IPT; it++) {
+        const int item = tid + it * NT;
+        const int loc[3] = {item / (SB * SB), (item / SB) % SB, item % SB};
+        bool valid = loc[0] < R.len[0] && loc[1] < R.len[1] && loc[2] < R.len[2];
+        const int abc[3] = {R.st[0] + loc[0], R.st[1] + loc[1], R.st[2] + loc[2]};
+        if (valid && cs[1] == 0 && abc[0] < abc[1]) valid = false;
+        if (valid && cs[2] == cs[1] && abc[1] < abc[2]) valid = false;
+        gvalid[it] = valid;
+        double ddi = 0.0;
+        if (valid) {
+            const int vl[3] = {cs[0] * SB + loc[0], cs[1] * SB + loc[1], cs[2] * SB + loc[2]};
+            double WW[6], X[6];
 #pragma unroll
-            for (int tau = 0; tau < 6; tau++) {
-                const int pi = perm_compose(s, tau);
-                int pp[3], pt[3];
-                perm_of(pi, pp);
-                perm_of(tau, pt);
-                const int id = s_reg[pi][tau] * REG + loc[pp[1]] * SY + loc[pp[0]] * SX + loc[pp[2]];
-                idx[s][tau] = id;
-                sw += (double)sW[id];
-                const int pair = pair_index(pt[0], pt[1]);
-                const int xl = vl[pp[0]], yl = vl[pp[1]], zl = vl[pp[2]];
-                sv += (double)tOV[(pair * NV + xl) * NVP + yl] * (double)tT1[pt[2] * NV + zl] +
-                      (double)tT2[(pair * NV + xl) * NVP + yl] * (double)tFV[pt[2] * NV + zl];
+            for (int s = 0; s < 6; s++) {
+                double sw = 0.0, sv = 0.0;
+#pragma unroll
+                for (int tau = 0; tau < 6; tau++) {
+                    const int pi = perm_compose(s, tau);
+                    int pp[3], pt[3];
+                    perm_of(pi, pp);
+                    perm_of(tau, pt);
+                    sw += (double)sW[s_reg[pi][tau] * REG + loc[pp[1]] * SY + loc[pp[0]] * SX + loc[pp[2]]];
+                    const int pair = pair_index(pt[0], pt[1]);
+                    const int xl = vl[pp[0]], yl = vl[pp[1]], zl = vl[pp[2]];
+                    sv += (double)tOV[(pair * NV + xl) * NVP + yl] * (double)tT1[pt[2] * NV + zl] +
+                          (double)tT2[(pair * NV + xl) * NVP + yl] * (double)tFV[pt[2] * NV + zl];
+                }
+                WW[s] = sw;
+                X[s] = sw + 0.5 * sv;
             }
-            WW[s] = sw;
-            X[s] = sw + 0.5 * sv;
-        }
-        double Z[6], RW[6];
+            double Z[6], RW[6];
 #pragma unroll
-        for (int s = 0; s < 6; s++) {
-            Z[s] = 4.0 * X[s] + X[perm_compose(s, 4)] + X[perm_compose(s, 3)] -
-                   2.0 * (X[perm_compose(s, 5)] + X[perm_compose(s, 1)] + X[perm_compose(s, 2)]);
-            RW[s] = 4.0 * WW[s] + WW[perm_compose(s, 4)] + WW[perm_compose(s, 3)] -
-                    2.0 * (WW[perm_compose(s, 5)] + WW[perm_compose(s, 1)] + WW[perm_compose(s, 2)]);
-        }
-        const int i = ijk[0], j = ijk[1], k = ijk[2];
-        const int n_ijk = (i == k) ? 1 : ((i == j || j == k) ? 3 : 6);
-        const int n_abc = (abc[0] == abc[2]) ? 1 : ((abc[0] == abc[1] || abc[1] == abc[2]) ? 3 : 6);
-        const double cfac = (double)(n_ijk * n_abc) / 18.0;
-        const double Dn = P.mo_e[i] + P.mo_e[j] + P.mo_e[k] - P.mo_e[o + abc[0]] - P.mo_e[o + abc[1]] -
-                          P.mo_e[o + abc[2]];
-        const double rD = 1.0 / Dn;
-        double esum = 0.0;
+            for (int s = 0; s < 6; s++) {
+                Z[s] = 4.0 * X[s] + X[perm_compose(s, 4)] + X[perm_compose(s, 3)] -
+                       2.0 * (X[perm_compose(s, 5)] + X[perm_compose(s, 1)] + X[perm_compose(s, 2)]);
+                RW[s] = 4.0 * WW[s] + WW[perm_compose(s, 4)] + WW[perm_compose(s, 3)] -
+                        2.0 * (WW[perm_compose(s, 5)] + WW[perm_compose(s, 1)] + WW[perm_compose(s, 2)]);
+            }
+            const int n_abc = (abc[0] == abc[2]) ? 1 : ((abc[0] == abc[1] || abc[1] == abc[2]) ? 3 : 6);
+            const double cfac = (double)(n_ijk * n_abc) / 18.0;
+            const double Dn = e_ijk - P.mo_e[o + abc[0]] - P.mo_e[o + abc[1]] - P.mo_e[o + abc[2]];
+            const double rD = 1.0 / Dn;
+            double esum = 0.0;
 #pragma unroll
-        for (int s = 0; s < 6; s++) esum += WW[s] * Z[s];
-        e_loc = cfac * esum * rD;
-        if (P.want_grad) {
-            const double g0 = P.ybar * cfac * rD;
-            const double dD = -P.ybar * cfac * esum * rD * rD;
-            dd_loc = dD;
-            if (n_ijk == 6 && n_abc == 6) {
-                // all 36 raw positions of the orbit are distinct
+            for (int s = 0; s < 6; s++) esum += WW[s] * Z[s];
+            e_loc += cfac * esum * rD;
+            if (P.want_grad) {
+                const double g0 = P.ybar * cfac * rD;
+                ddi = -P.ybar * cfac * esum * rD * rD;
 #pragma unroll
                 for (int s = 0; s < 6; s++) {
-                    const StageT gw = (StageT)(g0 * (Z[s] + RW[s]));
-                    const StageT gv = (StageT)(g0 * 0.5 * RW[s]);
-#pragma unroll
-                    for (int tau = 0; tau < 6; tau++) {
-                        sWb[idx[s][tau]] = gw;
-                        sW[idx[s][tau]] = gv;
-                    }
+                    gres[it][s] = (StageT)(g0 * (Z[s] + RW[s]));
+                    gres[it][6 + s] = (StageT)(g0 * 0.5 * RW[s]);
                 }
-            } else {
-                // repeated indices: several (s, tau) land on one raw position
-#pragma unroll
-                for (int s = 0; s < 6; s++)
-#pragma unroll
-                    for (int tau = 0; tau < 6; tau++) {
-                        sW[idx[s][tau]] = (StageT)0;
-                        sWb[idx[s][tau]] = (StageT)0;
-                    }
-#pragma unroll
-                for (int s = 0; s < 6; s++) {
-                    const StageT gw = (StageT)(g0 * (Z[s] + RW[s]));
-                    const StageT gv = (StageT)(g0 * 0.5 * RW[s]);
-#pragma unroll
-                    for (int tau = 0; tau < 6; tau++) {
-                        sWb[idx[s][tau]] += gw;
-                        sW[idx[s][tau]] += gv;
-                    }
-                }
+                if (SB * SB < 32) atomicAdd(&s_ev[vl[0]], -ddi);
+                atomicAdd(&s_ev[vl[1]], -ddi);
+                atomicAdd(&s_ev[vl[2]], -ddi);
             }
-            if (SB * SB < 32) atomicAdd(&s_ev[vl[0]], -dD);
-            atomicAdd(&s_ev[vl[1]], -dD);
-            atomicAdd(&s_ev[vl[2]], -dD);
         }
-    }
-    // with SB^2 >= 32 the a-slot index (tid / SB^2) is uniform across a warp: reduce first
-    if (SB * SB >= 32 && P.want_grad) {
-        double dsum = valid ? -dd_loc : 0.0;
-        for (int off = 16; off > 0; off >>= 1) dsum += __shfl_down_sync(0xffffffffu, dsum, off);
-        const int la = tid / (SB * SB);
-        if ((tid & 31) == 0 && la < R.len[0] && dsum != 0.0) atomicAdd(&s_ev[cs[0] * SB + la], dsum);
+        dd_loc += ddi;
+        // with SB^2 >= 32 the a-slot index (item / SB^2) is uniform across a warp: reduce first
+        if (SB * SB >= 32 && P.want_grad) {
+            double dsum = -ddi;
+            for (int off = 16; off > 0; off >>= 1) dsum += __shfl_down_sync(0xffffffffu, dsum, off);
+            const int la = item / (SB * SB);
+            if (lane == 0 && la < R.len[0] && dsum != 0.0) atomicAdd(&s_ev[cs[0] * SB + la], dsum);
+        }
     }
 
-    // ---- block reductions ----
+    // ---- block reductions: chunk energy partial, occupied-energy gradient ----
     for (int off = 16; off > 0; off >>= 1) {
         e_loc += __shfl_down_sync(0xffffffffu, e_loc, off);
         dd_loc += __shfl_down_sync(0xffffffffu, dd_loc, off);
     }
-    if ((tid & 31) == 0) {
-        s_red[0][tid >> 5] = e_loc;
-        s_red[1][tid >> 5] = dd_loc;
+    if (lane == 0) {
+        s_red[0][warp] = e_loc;
+        s_red[1][warp] = dd_loc;
     }
-    __syncthreads();
+    __syncthreads();   // all reads of the W tile are done: it becomes the item-result buffer
     if (tid == 0) {
         double es = 0.0, ds = 0.0;
-        for (int w = 0; w < (NT + 31) / 32; w++) {
+        for (int w = 0; w < NW; w++) {
             es += s_red[0][w];
             ds += s_red[1][w];
         }
@@ -421,38 +449,91 @@ __global__ void __launch_bounds__(SB *SB *SB) k_f2t(F2P<StageT> P) {
             atomicAdd(&P.mo_bar[ijk[2]], ds);
         }
     }
-
-    if (P.want_grad) {
-        for (int e = tid; e < NV; e += NT) {
-            const int sl = e / SB, l = e % SB;
-            if (l < R.len[sl] && s_ev[e] != 0.0) atomicAdd(&P.mo_bar[o + R.st[sl] + l], s_ev[e]);
+    if (!P.want_grad) return;
+#pragma unroll
+    for (int it = 0; it < IPT; it++)
+        if (gvalid[it]) {
+            const int item = tid + it * NT;
+#pragma unroll
+            for (int c = 0; c < 12; c++) sG[c * ITEMS + item] = gres[it][c];
         }
-        // ---- write back: Vbar in place, Wbar to its buffer, one z run per step ----
-        const float wscf = (P.split != 0) ? (float)*P.wscale : 1.0f;
-        for (int e = tid; e < nreg * SB * SB; e += NT) {
-            const int reg = e / (SB * SB), yy = (e / SB) % SB, xx = e % SB;
-            const int *rd = s_rd[reg];
-            const int lx = rd[3], ly = rd[4], lz = rd[5];
-            if (xx >= lx || yy >= ly) continue;
+    __syncthreads();
+    for (int e = tid; e < NV; e += NT) {
+        const int sl = e / SB, l = e % SB;
+        if (l < R.len[sl] && s_ev[e] != 0.0) atomicAdd(&P.mo_bar[o + R.st[sl] + l], s_ev[e]);
+    }
+
+    // ---- write back Wbar; V-term gradients from the run's Vbar ----
+    // One thread per (region, y, x) run of z values.  A warp's runs (G lanes)
+    // lie in one region, which fixes the columns (r, z) of the t1 / fvo sums.
+    constexpr int RPR = SB * SB;                 // runs per region
+    constexpr int GL = RPR < 32 ? RPR : 32;      // lanes per region group
+    const float wscf = (P.split != 0) ? (float)*P.wscale : 1.0f;
+    const int nrun = nreg * RPR;
+    const int nstep = (nrun + NT - 1) / NT;
+    for (int st = 0; st < nstep; st++) {
+        const int e = tid + st * NT;
+        const bool inrange = e < nrun;
+        const int reg = inrange ? e / RPR : 0;
+        const int yy = (e / SB) % SB, xx = e % SB;
+        const int *rd = s_rd[reg];
+        const int lx = rd[3], ly = rd[4], lz = rd[5];
+        const bool act = inrange && xx < lx && yy < ly;
+        int pp[3], pt[3];
+        perm_of(rd[0], pp);
+        perm_of(rd[1], pt);
+        auto cslot = [&](int j) { return j == 0 ? cs[0] : (j == 1 ? cs[1] : cs[2]); };
+        const int zl0 = cslot(pp[2]) * SB;
+        double colv[2 * SB];
+#pragma unroll
+        for (int c = 0; c < 2 * SB; c++) colv[c] = 0.0;
+        if (act) {
+            double wb[SB], vb[SB];
+#pragma unroll
+            for (int zz = 0; zz < SB; zz++) wb[zz] = vb[zz] = 0.0;
+            const int nc = s_ncombo[reg];
+            for (int c = 0; c < nc; c++) {
+                const int pr = s_combo[reg][c];
+                const int s = s_sof[pr];
+                int q3[3];
+                perm_of(pr / 6, q3);
+                // item slot j takes the region coordinate whose ordering slot is j
+                const int st0 = (q3[0] == 0) ? SB * SB : (q3[0] == 1 ? SB : 1);
+                const int st1 = (q3[1] == 0) ? SB * SB : (q3[1] == 1 ? SB : 1);
+                const int st2 = (q3[2] == 0) ? SB * SB : (q3[2] == 1 ? SB : 1);
+                const int base = xx * st0 + yy * st1;
+                const StageT *gw = sG + s * ITEMS, *gv = sG + (6 + s) * ITEMS;
+#pragma unroll
+                for (int zz = 0; zz < SB; zz++) {
+                    if (zz >= lz) continue;
+                    const int l0 = (q3[0] == 0) ? xx : ((q3[1] == 0) ? yy : zz);
+                    const int l1 = (q3[0] == 1) ? xx : ((q3[1] == 1) ? yy : zz);
+                    const int l2 = (q3[0] == 2) ? xx : ((q3[1] == 2) ? yy : zz);
+                    bool ok = true;
+                    if (cs[1] == 0 && l0 < l1) ok = false;
+                    if (cs[2] == cs[1] && l1 < l2) ok = false;
+                    if (ok) {
+                        const int item = base + zz * st2;
+                        wb[zz] += (double)gw[item];
+                        vb[zz] += (double)gv[item];
+                    }
+                }
+            }
+            // Wbar out
             const PermBlock &pb = P.ch.pb[rd[2]];
-            StageT *vdst = P.S + s_gb[reg] + (long long)yy * s_gs[reg][0] + (long long)xx * s_gs[reg][1];
-            const int si = reg * REG + yy * SY + xx * SX;
             const long long wl = s_wb[reg] + (long long)yy * s_ws[reg][0] + (long long)xx * s_ws[reg][1];
             const long long half = (long long)pb.Ty * o * pb.Tx * o * pb.rzp;
-            RunBuf<StageT, SB> bv;
-#pragma unroll
-            for (int zz = 0; zz < SB; zz++) bv.e[zz] = sW[si + zz];
-            st_run(vdst, bv, lz);
             if (P.split == 0) {
+                RunBuf<StageT, SB> bw;
 #pragma unroll
-                for (int zz = 0; zz < SB; zz++) bv.e[zz] = sWb[si + zz];
-                st_run(reinterpret_cast<StageT *>(P.SW) + pb.swoff + wl, bv, lz);
+                for (int zz = 0; zz < SB; zz++) bw.e[zz] = (StageT)wb[zz];
+                st_run(reinterpret_cast<StageT *>(P.SW) + pb.swoff + wl, bw, lz);
             } else if (P.split == 1) {
                 // exact power-of-two scaling, then a two-term 16-bit split in FP32
                 RunBuf<__half, SB> bh, bl;
 #pragma unroll
                 for (int zz = 0; zz < SB; zz++) {
-                    const float xs = (float)sWb[si + zz] * wscf;
+                    const float xs = (float)wb[zz] * wscf;
                     bh.e[zz] = __float2half_rn(xs);
                     bl.e[zz] = __float2half_rn(xs - __half2float(bh.e[zz]));
                 }
@@ -463,7 +544,7 @@ __global__ void __launch_bounds__(SB *SB *SB) k_f2t(F2P<StageT> P) {
                 RunBuf<__nv_bfloat16, SB> bh, bl;
 #pragma unroll
                 for (int zz = 0; zz < SB; zz++) {
-                    const float xs = (float)sWb[si + zz] * wscf;
+                    const float xs = (float)wb[zz] * wscf;
                     bh.e[zz] = __float2bfloat16_rn(xs);
                     bl.e[zz] = __float2bfloat16_rn(xs - __bfloat162float(bh.e[zz]));
                 }
@@ -471,34 +552,47 @@ __global__ void __launch_bounds__(SB *SB *SB) k_f2t(F2P<StageT> P) {
                 st_run(dst, bh, lz);
                 st_run(dst + half, bl, lz);
             }
+            // V-term gradients: v = ovov[p,x,q,y] t1[r,z] + t2[q,p,y,x] fvo[z,r]
+            const int p = rd[6], q = rd[7];
+            const int x = R.st[pp[0]] + xx, y = R.st[pp[1]] + yy;
+            const int pair = pair_index(pt[0], pt[1]);
+            const int te = (pair * NV + cslot(pp[0]) * SB + xx) * NVP + cslot(pp[1]) * SB + yy;
+            const double ovv = (double)tOV[te], t2v = (double)tT2[te];
+            const StageT *a1 = tT1 + pt[2] * NV + zl0, *f1 = tFV + pt[2] * NV + zl0;
+            double rs1 = 0.0, rs2 = 0.0;
+#pragma unroll
+            for (int zz = 0; zz < SB; zz++) {
+                rs1 += vb[zz] * (double)a1[zz];
+                rs2 += vb[zz] * (double)f1[zz];
+                colv[zz] = vb[zz] * ovv;
+                colv[SB + zz] = vb[zz] * t2v;
+            }
+            atomicAdd(&P.ovov_bar[(((long long)p * v + x) * o + q) * v + y], rs1);
+            atomicAdd(&P.t2_bar[(((long long)q * o + p) * v + y) * v + x], rs2);
+        }
+        // column sums over the region's runs: t1_bar[r, z], fvo_bar[z, r]
+        const double cv = group_reduce_scatter<2 * SB, GL>(colv, lane);
+        const int cidx = lane % (2 * SB);
+        if (inrange && (lane % GL) < 2 * SB && (cidx % SB) < lz && cv != 0.0) {
+            const int r = rd[8], z = R.st[pp[2]] + cidx % SB;
+            if (cidx < SB) atomicAdd(&P.t1_bar[(long long)r * v + z], cv);
+            else atomicAdd(&P.fvo_bar[(long long)z * o + r], cv);
         }
     }
+}
 
-    // ---- deterministic chunk energy: the last CTA sums the partials in a fixed order ----
-    __shared__ bool s_last;
-    __threadfence();
+// Sum of the per-CTA energy partials of one epilogue launch, in a fixed order.
+__global__ void k_f2_energy_sum(const double *__restrict__ e_part, int n, double *e_acc) {
+    __shared__ double s[256];
+    double acc = 0.0;
+    for (int b = threadIdx.x; b < n; b += blockDim.x) acc += e_part[b];
+    s[threadIdx.x] = acc;
     __syncthreads();
-    if (tid == 0) {
-        const unsigned prev = atomicAdd(P.counter, 1u);
-        s_last = (prev == gridDim.x * gridDim.y - 1);
-    }
-    __syncthreads();
-    if (s_last) {
-        __threadfence();
-        const int nblk = gridDim.x * gridDim.y;
-        double acc = 0.0;
-        for (int b = tid; b < nblk; b += NT) acc += ((volatile double *)P.e_part)[b];
-        for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) s[threadIdx.x] += s[threadIdx.x + h];
         __syncthreads();
-        if ((tid & 31) == 0) s_red[0][tid >> 5] = acc;
-        __syncthreads();
-        if (tid == 0) {
-            double tot = 0.0;
-            for (int w = 0; w < (NT + 31) / 32; w++) tot += s_red[0][w];
-            P.e_acc[0] += tot;
-            *P.counter = 0u;
-        }
     }
+    if (threadIdx.x == 0) *e_acc += s[0];
 }
 
 }  // namespace tb

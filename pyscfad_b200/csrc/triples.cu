@@ -40,8 +40,8 @@ static int g_kseg_f1 = 1;  // same for the W contraction
 // ---------------------------------------------------------------------------
 // optional per-kernel-class timing with CUDA events (on the launch stream)
 // ---------------------------------------------------------------------------
-enum ProfCat { P_PREP = 0, P_F1, P_F2, P_VGRAD, P_B1A, P_B1B, P_B1C, P_B1D, P_FOLD, P_NCAT };
-static const char *kProfNames[P_NCAT] = {"prep", "f1_contract", "f2_epilogue", "vgrad",
+enum ProfCat { P_PREP = 0, P_F1, P_F2, P_B1A, P_B1B, P_B1C, P_B1D, P_FOLD, P_NCAT };
+static const char *kProfNames[P_NCAT] = {"prep", "f1_contract", "f2_epilogue", 
                                          "b1a_ovvv_grad", "b1b_t2_grad", "b1c_ovoo_grad",
                                          "b1d_t2_ooov_grad", "fold"};
 struct ProfRec {
@@ -203,11 +203,6 @@ int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan
         P.off_GB1 = take(o * o * v * Kp * el);
         P.off_GA2 = take(o * o * v * o * el);
         P.off_GB2 = take(v * o * v * o * el);
-    }
-    if (want_grad) {
-        long long maxrows = (long long)nocc * nocc * d.Tv * d.Tv;
-        long long nblk = (maxrows + kVgRowsPerBlock - 1) / kVgRowsPerBlock;
-        P.off_vgpart = take((size_t)6 * nblk * 2 * kMaxCols * el);
     }
     P.off_ijk = take((size_t)P.n_ijk * 3 * sizeof(int));
     P.off_epart = take((size_t)P.n_ijk * P.f2_gy * el);
@@ -658,142 +653,6 @@ __global__ void __launch_bounds__(256) k_b1d_fp64(GemmLaunch<StageT> L) {
 // ---------------------------------------------------------------------------
 // V-term gradients from Vbar: ovov, t2 (row dots), t1, fvo (column sums)
 // ---------------------------------------------------------------------------
-template <typename StageT>
-struct VGParams {
-    Dims d;
-    ChunkDesc ch;
-    const StageT *SV;
-    const double *t1, *fvo, *ovov, *t2;
-    double *ovov_bar, *t2_bar;
-    double *part;         // [tau][block][2][kMaxCols] column partials
-    int nblk;             // blocks per ordering (grid.x)
-};
-
-constexpr int kVgUnroll = 2;
-
-// One block streams kVgRowsPerBlock rows (p,q,y,x) of Vbar_tau (each row = the
-// (r,z) plane, o*Tz values):
-//   ovov_bar[p,x,q,y] += sum_rz Vbar t1[r,z],  t2_bar[q,p,y,x] += sum_rz Vbar fvo[z,r]
-// and accumulates the column sums  sum_rows Vbar * ovov[p,x,q,y]  (-> t1_bar) and
-// sum_rows Vbar * t2[q,p,y,x]  (-> fvo_bar) into a per-block partial vector.
-template <typename StageT>
-__global__ void __launch_bounds__(256) k_vgrad(VGParams<StageT> P) {
-    const Dims &d = P.d;
-    const int o = d.o, v = d.v;
-    const int tau = blockIdx.y;
-    const PermBlock &pb = P.ch.pb[tau];
-    const int ncol = o * pb.Tz;
-    const long long nrow = (long long)o * o * pb.Ty * pb.Tx;
-    const long long row0 = (long long)blockIdx.x * kVgRowsPerBlock;
-    __shared__ double s_t1[kMaxCols], s_fv[kMaxCols], s_c1[kMaxCols], s_c2[kMaxCols];
-    for (int c = threadIdx.x; c < ncol; c += blockDim.x) {
-        const int r = c / pb.Tz, z = c % pb.Tz;
-        s_t1[c] = P.t1[(long long)r * v + pb.Z0 + z];
-        s_fv[c] = P.fvo[(long long)(pb.Z0 + z) * o + r];
-        s_c1[c] = 0.0;
-        s_c2[c] = 0.0;
-    }
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    constexpr int NC = kMaxCols / 32;
-    const int ncl = (ncol + 31) / 32;
-    double c1[NC], c2[NC];   // per-lane column partials (FP64: the sums run over many rows)
-#pragma unroll
-    for (int c = 0; c < NC; c++) {
-        c1[c] = 0.0;
-        c2[c] = 0.0;
-    }
-    long long row_end = row0 + kVgRowsPerBlock;
-    if (row_end > nrow) row_end = nrow;
-    for (long long rb = row0 + warp * kVgUnroll; rb < row_end; rb += 8 * kVgUnroll) {
-        double wv1[kVgUnroll], wv2[kVgUnroll], dot1[kVgUnroll], dot2[kVgUnroll];
-        long long io1[kVgUnroll], io2[kVgUnroll];
-#pragma unroll
-        for (int u = 0; u < kVgUnroll; u++) {
-            const long long row = rb + u;
-            wv1[u] = wv2[u] = 0.0;
-            io1[u] = io2[u] = -1;
-            dot1[u] = dot2[u] = 0.0;
-            if (row < row_end) {
-                const int x = row % pb.Tx;
-                const int y = (row / pb.Tx) % pb.Ty;
-                const long long pq = row / ((long long)pb.Tx * pb.Ty);
-                const int q = pq % o, p = pq / o;
-                const int xg = pb.X0 + x, yg = pb.Y0 + y;
-                io1[u] = (((long long)p * v + xg) * o + q) * v + yg;
-                io2[u] = (((long long)q * o + p) * v + yg) * v + xg;
-                wv1[u] = P.ovov[io1[u]];
-                wv2[u] = P.t2[io2[u]];
-            }
-        }
-#pragma unroll
-        for (int c = 0; c < NC; c++) {
-            if (c >= ncl) break;
-            const int col = lane + 32 * c;
-            if (col < ncol) {
-                const double a1 = s_t1[col], a2 = s_fv[col];
-#pragma unroll
-                for (int u = 0; u < kVgUnroll; u++) {
-                    if (io1[u] < 0) continue;
-                    const double val = (double)P.SV[pb.soff + (rb + u) * ncol + col];
-                    dot1[u] += val * a1;
-                    dot2[u] += val * a2;
-                    c1[c] += val * wv1[u];
-                    c2[c] += val * wv2[u];
-                }
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < kVgUnroll; u++) {
-            double a = dot1[u], b = dot2[u];
-            for (int off = 16; off > 0; off >>= 1) {
-                a += __shfl_down_sync(0xffffffffu, a, off);
-                b += __shfl_down_sync(0xffffffffu, b, off);
-            }
-            if (lane == 0 && io1[u] >= 0) {
-                P.ovov_bar[io1[u]] += a;
-                P.t2_bar[io2[u]] += b;
-            }
-        }
-    }
-#pragma unroll
-    for (int c = 0; c < NC; c++) {
-        const int col = lane + 32 * c;
-        if (c < ncl && col < ncol) {
-            atomicAdd(&s_c1[col], c1[c]);
-            atomicAdd(&s_c2[col], c2[c]);
-        }
-    }
-    __syncthreads();
-    double *part = P.part + ((long long)tau * P.nblk + blockIdx.x) * 2 * kMaxCols;
-    for (int c = threadIdx.x; c < ncol; c += blockDim.x) {
-        part[c] = s_c1[c];
-        part[kMaxCols + c] = s_c2[c];
-    }
-}
-
-// Column sums of the V-gradient partials -> t1_bar, fvo_bar (fixed summation order).
-template <typename StageT>
-__global__ void k_vgrad_reduce(VGParams<StageT> P, double *t1_bar, double *fvo_bar) {
-    const int tau = blockIdx.y;
-    const PermBlock &pb = P.ch.pb[tau];
-    const int o = P.d.o, v = P.d.v;
-    const int ncol = o * pb.Tz;
-    const long long nrow = (long long)o * o * pb.Ty * pb.Tx;
-    const int nb = (int)((nrow + kVgRowsPerBlock - 1) / kVgRowsPerBlock);
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= ncol) return;
-    double s1 = 0.0, s2 = 0.0;
-    for (int b = 0; b < nb; b++) {
-        const double *part = P.part + ((long long)tau * P.nblk + b) * 2 * kMaxCols;
-        s1 += part[c];
-        s2 += part[kMaxCols + c];
-    }
-    const int r = c / pb.Tz, z = c % pb.Tz;
-    atomicAdd(&t1_bar[(long long)r * v + pb.Z0 + z], s1);
-    atomicAdd(&fvo_bar[(long long)(pb.Z0 + z) * o + r], s2);
-}
-
 // ---------------------------------------------------------------------------
 // gradient fold back to the reference layouts
 // ---------------------------------------------------------------------------
@@ -955,7 +814,6 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
     double *GB2 = P.want_grad ? (double *)(ws + P.off_GB2) : nullptr;
     int *ijk = (int *)(ws + P.off_ijk);
     double *e_part = (double *)(ws + P.off_epart);
-    double *vg_part = P.want_grad ? (double *)(ws + P.off_vgpart) : nullptr;
     const size_t o = d.o, v = d.v, n = d.n;
 
     TB_CUDA(cudaMemsetAsync(ctrl, 0, kCtrlBytes, st));
@@ -1139,31 +997,14 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                     F.wscale = &ctrl->wscale;
                     F.ybar = io.ybar;
                     F.want_grad = P.want_grad;
-                    F.e_part = e_part; F.e_acc = &ctrl->e_acc; F.counter = &ctrl->counter;
+                    F.e_part = e_part;
                     F.mo_bar = io.mo_energy_bar;
-                    TB_KLAUNCH(P_F2, (k_f2t<StageT, kSB><<<dim3(P.n_ijk, F.nsub), kSB * kSB * kSB,
+                    F.t1_bar = io.t1_bar; F.fvo_bar = io.fvo_bar; F.ovov_bar = io.ovov_bar; F.t2_bar = io.t2_bar;
+                    TB_KLAUNCH(P_F2, (k_f2t<StageT, kSB><<<dim3(P.n_ijk, F.nsub), F2Smem<kSB>::NT,
                                                            f2_smem_bytes<StageT, kSB>(), st>>>(F)));
+                    TB_KLAUNCH(P_F2, k_f2_energy_sum<<<1, 256, 0, st>>>(e_part, P.n_ijk * F.nsub, &ctrl->e_acc));
                 }
                 if (!P.want_grad) continue;
-                // V-term gradients
-                {
-                    VGParams<StageT> VG;
-                    VG.d = d;
-                    VG.ch = ch;
-                    VG.SV = S;
-                    VG.t1 = io.t1; VG.fvo = io.fvo; VG.ovov = io.ovov; VG.t2 = io.t2;
-                    VG.ovov_bar = io.ovov_bar; VG.t2_bar = io.t2_bar;
-                    VG.part = vg_part;
-                    long long maxrows = 0;
-                    for (int t = 0; t < ch.nperm; t++) {
-                        long long r = (long long)d.o * d.o * ch.pb[t].Ty * ch.pb[t].Tx;
-                        if (r > maxrows) maxrows = r;
-                    }
-                    VG.nblk = (int)((maxrows + kVgRowsPerBlock - 1) / kVgRowsPerBlock);
-                    TB_KLAUNCH(P_VGRAD, k_vgrad<StageT><<<dim3(VG.nblk, ch.nperm), 256, 0, st>>>(VG));
-                    TB_KLAUNCH(P_VGRAD, k_vgrad_reduce<StageT><<<dim3((kMaxCols + 127) / 128, ch.nperm), 128, 0, st>>>(
-                                            VG, io.t1_bar, io.fvo_bar));
-                }
                 // W-term gradients
                 if (mixed) {
                     for (int t = 0; t < ch.nperm; t++) {

@@ -9,14 +9,12 @@ namespace tb {
 
 constexpr int kF2Threads = 256;   // chunk-epilogue block size
 constexpr int kMaxTv = 16;        // largest virtual block
-constexpr int kMaxCols = 1024;    // largest nocc * Tv handled by the V-gradient kernel
-constexpr int kVgRowsPerBlock = 1024;  // staged rows per V-gradient block
+constexpr int kMaxCols = 1024;    // largest nocc * Tv (one staged (r, z) row)
 constexpr int kCtrlBytes = 256;   // control block at workspace offset 0
 
 // Control block (workspace offset 0)
 struct Ctrl {
     int err;                      // device-side error bits (bounded waits that gave up)
-    unsigned counter;             // epilogue last-block counter
     double e_acc;                 // E(T) accumulator
     double scale[2];              // operand scales (A: ovvv/ovoo, B: t2), powers of two
     float out_scale;              // 1 / (scale[0] * scale[1])
@@ -41,7 +39,7 @@ struct Plan {
     size_t off_A1, off_B1, off_A2, off_B2, off_S, off_SW;
     size_t off_A1h, off_B1h, off_A2h, off_B2h;
     size_t off_GA1, off_GB1, off_GA2, off_GB2;
-    size_t off_ijk, off_epart, off_vgpart;
+    size_t off_ijk, off_epart;
     size_t total;
 };
 

@@ -127,6 +127,83 @@ __device__ __forceinline__ void ld_run(RunBuf<T, N> &b, const T *src, int n) {
     }
 }
 
+// Region bookkeeping of a CTA depends only on which of i, j, k coincide and
+// which sub-ranges coincide (4 x 4 patterns), so it is tabulated once on the
+// host and read from constant memory.  For a pattern:
+//   reg[pi*6 + rho]   region of (sub-range ordering pi, occupied ordering rho)
+//   rep[g]            representative pi*6 + rho of region g (first in order)
+//   combo[g][0..ncombo[g])  all pi*6 + rho of region g, ascending
+//   sof[pi*6 + rho]   the ordering s with perm_compose(s, rho) = pi
+struct F2Pattern {
+    unsigned char nrole, npi;
+    unsigned char reg[36];
+    unsigned char rep[36];
+    unsigned char ncombo[36];
+    unsigned char combo[36][36];
+    unsigned char sof[36];
+};
+constexpr int kF2Patterns = 16;
+__constant__ F2Pattern c_f2pat[kF2Patterns];
+
+// pattern index: 4 * (i==j==k ? 3 : i==j ? 1 : j==k ? 2 : 0) + (sub-ranges likewise)
+__host__ __device__ inline int f2_pattern_index(int i, int j, int k, int a, int b, int c) {
+    const int pij = (i == k) ? 3 : (i == j ? 1 : (j == k ? 2 : 0));
+    const int pab = (a == c) ? 3 : (a == b ? 1 : (b == c ? 2 : 0));
+    return 4 * pij + pab;
+}
+
+inline void f2_build_patterns(F2Pattern out[kF2Patterns]) {
+    const int vals[4][3] = {{2, 1, 0}, {1, 1, 0}, {1, 0, 0}, {0, 0, 0}};
+    for (int pij = 0; pij < 4; pij++)
+        for (int pab = 0; pab < 4; pab++) {
+            F2Pattern &T = out[4 * pij + pab];
+            const int *ijk = vals[pij], *st = vals[pab];
+            auto same = [&](const int *val, int ra, int rb) {
+                int qa[3], qb[3];
+                perm_of(ra, qa);
+                perm_of(rb, qb);
+                return val[qa[0]] == val[qb[0]] && val[qa[1]] == val[qb[1]] && val[qa[2]] == val[qb[2]];
+            };
+            // dense index of an ordering among the distinct orderings (first occurrence order)
+            auto dense = [&](const int *val, int r, int &count) {
+                int first_at = r;
+                for (int r2 = 5; r2 >= 0; r2--)
+                    if (same(val, r2, r)) first_at = r2;
+                int id = 0;
+                count = 0;
+                for (int r2 = 0; r2 < 6; r2++) {
+                    bool first = true;
+                    for (int r3 = 0; r3 < r2; r3++)
+                        if (same(val, r2, r3)) first = false;
+                    if (first) {
+                        count++;
+                        if (r2 < first_at) id++;
+                    }
+                }
+                return id;
+            };
+            int nrole = 0, npi = 0;
+            for (int t = 0; t < 36; t++) {
+                const int pi = t / 6, rho = t % 6;
+                const int rid = dense(ijk, rho, nrole), pid = dense(st, pi, npi);
+                T.reg[t] = (unsigned char)(pid * nrole + rid);
+                for (int s2 = 0; s2 < 6; s2++)
+                    if (perm_compose(s2, rho) == pi) T.sof[t] = (unsigned char)s2;
+            }
+            T.nrole = (unsigned char)nrole;
+            T.npi = (unsigned char)npi;
+            for (int g = 0; g < 36; g++) {
+                T.ncombo[g] = 0;
+                T.rep[g] = 0;
+            }
+            for (int t = 0; t < 36; t++) {
+                const int g = T.reg[t];
+                if (T.ncombo[g] == 0) T.rep[g] = (unsigned char)t;
+                T.combo[g][T.ncombo[g]++] = (unsigned char)t;
+            }
+        }
+}
+
 // Sum NV (power of two) per-lane values over aligned groups of G lanes
 // (NV <= G <= 32, G a power of two); afterwards lane l holds the group total
 // of value (l % NV).
@@ -164,14 +241,9 @@ __global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4) k_f2t(F2P<S
     StageT *tFV = tT1 + 3 * NV;
     __shared__ double s_ev[NV];
     __shared__ double s_red[2][NW];
-    __shared__ int s_reg[6][6];               // [ordering pi][role rho] -> region
     __shared__ int s_rd[36][9];               // per region: pi, rho, tau, lx, ly, lz, p, q, r
     __shared__ long long s_gb[36], s_wb[36];  // staging / Wbar base offsets of each region
     __shared__ int s_gs[36][2], s_ws[36][2];  // (y, x) strides in staging / Wbar
-    __shared__ int s_ntile[2];
-    __shared__ unsigned char s_ncombo[36];    // (pi, rho) pairs of each region ...
-    __shared__ unsigned char s_combo[36][36]; // ... as pi*6 + rho, ascending
-    __shared__ unsigned char s_sof[36];       // ordering s with perm_compose(s, rho) = pi
 
     const Dims &d = P.d;
     const int o = d.o, v = d.v;
@@ -185,88 +257,9 @@ __global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4) k_f2t(F2P<S
     cs[0] = 0;
     cs[1] = (R.st[1] == R.st[0]) ? 0 : 1;
     cs[2] = (R.st[2] == R.st[1]) ? cs[1] : ((R.st[2] == R.st[0]) ? 0 : 2);
-
-    // distinct occupied orderings (roles) and distinct sub-range orderings;
-    // thread (pi, rho) < 36 fills its table entry
-    if (tid < 36) {
-        const int pi = tid / 6, rho = tid % 6;
-        int pr[3], pp[3];
-        perm_of(rho, pr);
-        perm_of(pi, pp);
-        // dense index of a value = number of distinct values first seen before it
-        auto same_ijk = [&](int ra, int rb) {
-            int qa[3], qb[3];
-            perm_of(ra, qa);
-            perm_of(rb, qb);
-            return ijk[qa[0]] == ijk[qb[0]] && ijk[qa[1]] == ijk[qb[1]] && ijk[qa[2]] == ijk[qb[2]];
-        };
-        auto same_rng = [&](int pa, int pb2) {
-            int qa[3], qb[3];
-            perm_of(pa, qa);
-            perm_of(pb2, qb);
-            return R.st[qa[0]] == R.st[qb[0]] && R.st[qa[1]] == R.st[qb[1]] && R.st[qa[2]] == R.st[qb[2]];
-        };
-        int rfirst_at = rho, pfirst_at = pi;
-        for (int r2 = 5; r2 >= 0; r2--)
-            if (same_ijk(r2, rho)) rfirst_at = r2;
-        for (int p2 = 5; p2 >= 0; p2--)
-            if (same_rng(p2, pi)) pfirst_at = p2;
-        int rid = 0, nrole = 0, pid = 0, npi = 0;
-        for (int r2 = 0; r2 < 6; r2++) {
-            bool first = true;
-            for (int r3 = 0; r3 < r2; r3++)
-                if (same_ijk(r2, r3)) first = false;
-            if (first) {
-                nrole++;
-                if (r2 < rfirst_at) rid++;
-            }
-        }
-        for (int p2 = 0; p2 < 6; p2++) {
-            bool first = true;
-            for (int p3 = 0; p3 < p2; p3++)
-                if (same_rng(p2, p3)) first = false;
-            if (first) {
-                npi++;
-                if (p2 < pfirst_at) pid++;
-            }
-        }
-        const int rfirst = (rfirst_at == rho), pfirst = (pfirst_at == pi);
-        const int reg = pid * nrole + rid;
-        s_reg[pi][rho] = reg;
-        for (int s2 = 0; s2 < 6; s2++)
-            if (perm_compose(s2, rho) == pi) s_sof[tid] = (unsigned char)s2;
-        if (tid == 0) {
-            s_ntile[0] = nrole;
-            s_ntile[1] = npi;
-        }
-        if (rfirst && pfirst) {
-            s_rd[reg][0] = pi;
-            s_rd[reg][1] = rho;
-            s_rd[reg][3] = R.len[pp[0]];
-            s_rd[reg][4] = R.len[pp[1]];
-            s_rd[reg][5] = R.len[pp[2]];
-            s_rd[reg][6] = ijk[pr[0]];
-            s_rd[reg][7] = ijk[pr[1]];
-            s_rd[reg][8] = ijk[pr[2]];
-        }
-    }
+    const F2Pattern &pat = c_f2pat[f2_pattern_index(ijk[0], ijk[1], ijk[2], R.st[0], R.st[1], R.st[2])];
+    const int nreg = pat.nrole * pat.npi;
     for (int e = tid; e < NV; e += NT) s_ev[e] = 0.0;
-    __syncthreads();
-    const int nrole = s_ntile[0], npi = s_ntile[1];
-    const int nreg = nrole * npi;
-
-    // the (pi, rho) pairs of each region in ascending order (deterministic sums)
-    if (tid < 36) {
-        const int reg = s_reg[tid / 6][tid % 6];
-        int rank = 0, cnt = 0;
-        for (int t = 0; t < 36; t++)
-            if (s_reg[t / 6][t % 6] == reg) {
-                if (t < tid) rank++;
-                cnt++;
-            }
-        s_combo[reg][rank] = (unsigned char)tid;
-        if (rank == 0) s_ncombo[reg] = (unsigned char)cnt;
-    }
 
     // region descriptors; find the staging ordering tau of a sub-range ordering
     auto block_of = [&](int start) {
@@ -284,13 +277,25 @@ __global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4) k_f2t(F2P<S
         return t;
     };
     if (tid < nreg) {
-        const int *rd = s_rd[tid];
-        const int tau = tau_of(rd[0]);
-        s_rd[tid][2] = tau;
-        int pp[3];
-        perm_of(rd[0], pp);
+        const int pi = pat.rep[tid] / 6, rho = pat.rep[tid] % 6;
+        int pp[3], pr[3];
+        perm_of(pi, pp);
+        perm_of(rho, pr);
+        const int tau = tau_of(pi);
+        const int p = pr[0] == 0 ? ijk[0] : (pr[0] == 1 ? ijk[1] : ijk[2]);
+        const int q = pr[1] == 0 ? ijk[0] : (pr[1] == 1 ? ijk[1] : ijk[2]);
+        const int r = pr[2] == 0 ? ijk[0] : (pr[2] == 1 ? ijk[1] : ijk[2]);
+        int *rd = s_rd[tid];
+        rd[0] = pi;
+        rd[1] = rho;
+        rd[2] = tau;
+        rd[3] = R.len[pp[0]];
+        rd[4] = R.len[pp[1]];
+        rd[5] = R.len[pp[2]];
+        rd[6] = p;
+        rd[7] = q;
+        rd[8] = r;
         const PermBlock &pb = P.ch.pb[tau];
-        const int p = rd[6], q = rd[7], r = rd[8];
         const int xs = R.st[pp[0]] - pb.X0, ys = R.st[pp[1]] - pb.Y0, zs = R.st[pp[2]] - pb.Z0;
         // staging S_tau[p][q][y][x][r][z]
         const long long gy = (long long)pb.Tx * o * pb.Tz, gx = (long long)o * pb.Tz;
@@ -305,42 +310,81 @@ __global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4) k_f2t(F2P<S
     }
     __syncthreads();
 
-    // ---- load the distinct regions, one (y, x) run of z values per thread step ----
-    for (int e = tid; e < nreg * SB * SB; e += NT) {
-        const int reg = e / (SB * SB), yy = (e / SB) % SB, xx = e % SB;
-        const int *rd = s_rd[reg];
-        const int lx = rd[3], ly = rd[4], lz = rd[5];
-        if (xx >= lx || yy >= ly) continue;
-        const StageT *src = P.S + s_gb[reg] + (long long)yy * s_gs[reg][0] + (long long)xx * s_gs[reg][1];
-        StageT *dst = sW + reg * REG + yy * SY + xx * SX;
-        RunBuf<StageT, SB> b;
-        ld_run(b, src, lz);
+    // ---- load the distinct regions, one (y, x) run of z values per thread step;
+    //      LB runs are fetched before any is stored, so their latencies overlap ----
+    // distinct sub-ranges: the tables need only the blocks of two different ranges
+    const bool distinct_rng = (cs[1] == 1 && cs[2] == 2);
+    {
+        constexpr int LB = 3;
+        const int nrun = nreg * SB * SB;
+        for (int e0 = tid; e0 < nrun; e0 += LB * NT) {
+            RunBuf<StageT, SB> b[LB];
+            StageT *dst[LB];
+            int lzs[LB];
 #pragma unroll
-        for (int zz = 0; zz < SB; zz++)
-            if (zz < lz) dst[zz] = b.e[zz];
-    }
-    // ---- tables for the V terms ----
-    for (int e = tid; e < 6 * NV * NV; e += NT) {
-        const int pair = e / (NV * NV), xl = (e / NV) % NV, yl = e % NV;
-        const int te = (pair * NV + xl) * NVP + yl;
-        const int sp = pair / 2, rem = pair % 2;
-        const int sq = (rem < sp) ? rem : rem + 1;   // inverse of pair_index
-        const int sx = xl / SB, sy = yl / SB;
-        StageT ov = 0, tt = 0;
-        if (xl % SB < R.len[sx] && yl % SB < R.len[sy]) {
-            const int x = R.st[sx] + xl % SB, y = R.st[sy] + yl % SB;
-            const int p = ijk[sp], q = ijk[sq];
-            ov = (StageT)P.ovov[(((long long)p * v + x) * o + q) * v + y];
-            tt = (StageT)P.t2[(((long long)q * o + p) * v + y) * v + x];
+            for (int u = 0; u < LB; u++) {
+                const int e = e0 + u * NT;
+                dst[u] = nullptr;
+                lzs[u] = 0;
+                if (e < nrun) {
+                    const int reg = e / (SB * SB), yy = (e / SB) % SB, xx = e % SB;
+                    const int *rd = s_rd[reg];
+                    if (xx < rd[3] && yy < rd[4]) {
+                        lzs[u] = rd[5];
+                        ld_run(b[u], P.S + s_gb[reg] + (long long)yy * s_gs[reg][0] + (long long)xx * s_gs[reg][1],
+                               lzs[u]);
+                        dst[u] = sW + reg * REG + yy * SY + xx * SX;
+                    }
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < LB; u++)
+                if (dst[u] != nullptr) {
+#pragma unroll
+                    for (int zz = 0; zz < SB; zz++)
+                        if (zz < lzs[u]) dst[u][zz] = b[u].e[zz];
+                }
         }
-        tOV[te] = ov;
-        tT2[te] = tt;
+    }
+    // ---- tables for the V terms (TB entries fetched per batch) ----
+    {
+        constexpr int TB = 4;
+        for (int e0 = tid; e0 < 6 * NV * NV; e0 += TB * NT) {
+            double ov[TB], tt[TB];
+            int te[TB];
+#pragma unroll
+            for (int u = 0; u < TB; u++) {
+                const int e = e0 + u * NT;
+                ov[u] = tt[u] = 0.0;
+                te[u] = -1;
+                if (e < 6 * NV * NV) {
+                    const int pair = e / (NV * NV), xl = (e / NV) % NV, yl = e % NV;
+                    te[u] = (pair * NV + xl) * NVP + yl;
+                    const int sp = pair / 2, rem = pair % 2;
+                    const int sq = (rem < sp) ? rem : rem + 1;   // inverse of pair_index
+                    const int sx = xl / SB, sy = yl / SB;
+                    if (xl % SB < R.len[sx] && yl % SB < R.len[sy] && !(distinct_rng && sx == sy)) {
+                        const int x = R.st[sx] + xl % SB, y = R.st[sy] + yl % SB;
+                        const int p = (sp == 0) ? ijk[0] : (sp == 1 ? ijk[1] : ijk[2]);
+                        const int q = (sq == 0) ? ijk[0] : (sq == 1 ? ijk[1] : ijk[2]);
+                        ov[u] = P.ovov[(((long long)p * v + x) * o + q) * v + y];
+                        tt[u] = P.t2[(((long long)q * o + p) * v + y) * v + x];
+                    }
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < TB; u++)
+                if (te[u] >= 0) {
+                    tOV[te[u]] = (StageT)ov[u];
+                    tT2[te[u]] = (StageT)tt[u];
+                }
+        }
     }
     for (int e = tid; e < 3 * NV; e += NT) {
         const int sr = e / NV, zl = e % NV, sz = zl / SB;
         StageT a1 = 0, f1 = 0;
         if (zl % SB < R.len[sz]) {
-            const int z = R.st[sz] + zl % SB, r = ijk[sr];
+            const int z = R.st[sz] + zl % SB, r = (sr == 0) ? ijk[0] : (sr == 1 ? ijk[1] : ijk[2]);
             a1 = (StageT)P.t1[(long long)r * v + z];
             f1 = (StageT)P.fvo[(long long)z * o + r];
         }
@@ -378,7 +422,7 @@ __global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4) k_f2t(F2P<S
                     int pp[3], pt[3];
                     perm_of(pi, pp);
                     perm_of(tau, pt);
-                    sw += (double)sW[s_reg[pi][tau] * REG + loc[pp[1]] * SY + loc[pp[0]] * SX + loc[pp[2]]];
+                    sw += (double)sW[pat.reg[pi * 6 + tau] * REG + loc[pp[1]] * SY + loc[pp[0]] * SX + loc[pp[2]]];
                     const int pair = pair_index(pt[0], pt[1]);
                     const int xl = vl[pp[0]], yl = vl[pp[1]], zl = vl[pp[2]];
                     sv += (double)tOV[(pair * NV + xl) * NVP + yl] * (double)tT1[pt[2] * NV + zl] +
@@ -464,65 +508,84 @@ __global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4) k_f2t(F2P<S
     }
 
     // ---- write back Wbar; V-term gradients from the run's Vbar ----
-    // One thread per (region, y, x) run of z values.  A warp's runs (G lanes)
-    // lie in one region, which fixes the columns (r, z) of the t1 / fvo sums.
+    // A group of GL lanes takes whole regions (RPL runs of z values per lane),
+    // so the columns (r, z) of the t1 / fvo sums are fixed per group and the
+    // column partials of all its runs are reduced once per region.
     constexpr int RPR = SB * SB;                 // runs per region
     constexpr int GL = RPR < 32 ? RPR : 32;      // lanes per region group
+    constexpr int RPL = RPR / GL;                // runs per lane
+    constexpr int NG = NT / GL;                  // groups per CTA
+    // every region holds one (pi, rho) pair and no ordering constraint applies
+    const bool simple = (n_ijk == 6) && distinct_rng;
     const float wscf = (P.split != 0) ? (float)*P.wscale : 1.0f;
-    const int nrun = nreg * RPR;
-    const int nstep = (nrun + NT - 1) / NT;
-    for (int st = 0; st < nstep; st++) {
-        const int e = tid + st * NT;
-        const bool inrange = e < nrun;
-        const int reg = inrange ? e / RPR : 0;
-        const int yy = (e / SB) % SB, xx = e % SB;
+    const int grp = tid / GL, gl = tid % GL;
+    const int nround = (nreg + NG - 1) / NG;
+    for (int rr = 0; rr < nround; rr++) {
+        const int reg_ = grp + rr * NG;
+        const bool inrange = reg_ < nreg;
+        const int reg = inrange ? reg_ : 0;
         const int *rd = s_rd[reg];
         const int lx = rd[3], ly = rd[4], lz = rd[5];
-        const bool act = inrange && xx < lx && yy < ly;
         int pp[3], pt[3];
         perm_of(rd[0], pp);
         perm_of(rd[1], pt);
         auto cslot = [&](int j) { return j == 0 ? cs[0] : (j == 1 ? cs[1] : cs[2]); };
+        auto stride = [&](int j) { return j == 0 ? SB * SB : (j == 1 ? SB : 1); };
         const int zl0 = cslot(pp[2]) * SB;
+        const int p = rd[6], q = rd[7], r = rd[8];
+        const int pair = pair_index(pt[0], pt[1]);
+        const StageT *a1 = tT1 + pt[2] * NV + zl0, *f1 = tFV + pt[2] * NV + zl0;
+        const PermBlock &pb = P.ch.pb[rd[2]];
+        const long long half = (long long)pb.Ty * o * pb.Tx * o * pb.rzp;
         double colv[2 * SB];
 #pragma unroll
         for (int c = 0; c < 2 * SB; c++) colv[c] = 0.0;
-        if (act) {
-            double wb[SB], vb[SB];
 #pragma unroll
-            for (int zz = 0; zz < SB; zz++) wb[zz] = vb[zz] = 0.0;
-            const int nc = s_ncombo[reg];
-            for (int c = 0; c < nc; c++) {
-                const int pr = s_combo[reg][c];
-                const int s = s_sof[pr];
-                int q3[3];
-                perm_of(pr / 6, q3);
-                // item slot j takes the region coordinate whose ordering slot is j
-                const int st0 = (q3[0] == 0) ? SB * SB : (q3[0] == 1 ? SB : 1);
-                const int st1 = (q3[1] == 0) ? SB * SB : (q3[1] == 1 ? SB : 1);
-                const int st2 = (q3[2] == 0) ? SB * SB : (q3[2] == 1 ? SB : 1);
-                const int base = xx * st0 + yy * st1;
-                const StageT *gw = sG + s * ITEMS, *gv = sG + (6 + s) * ITEMS;
+        for (int u = 0; u < RPL; u++) {
+            const int run = gl + u * GL;
+            const int yy = run / SB, xx = run % SB;
+            if (!(inrange && xx < lx && yy < ly)) continue;
+            double wb[SB], vb[SB];
+            if (simple) {
+                const int s = pat.sof[rd[0] * 6 + rd[1]];
+                const int base = xx * stride(pp[0]) + yy * stride(pp[1]), st2 = stride(pp[2]);
+                const StageT *gw = sG + s * ITEMS + base, *gv = sG + (6 + s) * ITEMS + base;
 #pragma unroll
                 for (int zz = 0; zz < SB; zz++) {
-                    if (zz >= lz) continue;
-                    const int l0 = (q3[0] == 0) ? xx : ((q3[1] == 0) ? yy : zz);
-                    const int l1 = (q3[0] == 1) ? xx : ((q3[1] == 1) ? yy : zz);
-                    const int l2 = (q3[0] == 2) ? xx : ((q3[1] == 2) ? yy : zz);
-                    bool ok = true;
-                    if (cs[1] == 0 && l0 < l1) ok = false;
-                    if (cs[2] == cs[1] && l1 < l2) ok = false;
-                    if (ok) {
-                        const int item = base + zz * st2;
-                        wb[zz] += (double)gw[item];
-                        vb[zz] += (double)gv[item];
+                    wb[zz] = (zz < lz) ? (double)gw[zz * st2] : 0.0;
+                    vb[zz] = (zz < lz) ? (double)gv[zz * st2] : 0.0;
+                }
+            } else {
+#pragma unroll
+                for (int zz = 0; zz < SB; zz++) wb[zz] = vb[zz] = 0.0;
+                const int nc = pat.ncombo[reg];
+                for (int c = 0; c < nc; c++) {
+                    const int pr = pat.combo[reg][c];
+                    const int s = pat.sof[pr];
+                    int q3[3];
+                    perm_of(pr / 6, q3);
+                    // item slot j takes the region coordinate whose ordering slot is j
+                    const int base = xx * stride(q3[0]) + yy * stride(q3[1]), st2 = stride(q3[2]);
+                    const StageT *gw = sG + s * ITEMS, *gv = sG + (6 + s) * ITEMS;
+#pragma unroll
+                    for (int zz = 0; zz < SB; zz++) {
+                        if (zz >= lz) continue;
+                        const int l0 = (q3[0] == 0) ? xx : ((q3[1] == 0) ? yy : zz);
+                        const int l1 = (q3[0] == 1) ? xx : ((q3[1] == 1) ? yy : zz);
+                        const int l2 = (q3[0] == 2) ? xx : ((q3[1] == 2) ? yy : zz);
+                        bool ok = true;
+                        if (cs[1] == 0 && l0 < l1) ok = false;
+                        if (cs[2] == cs[1] && l1 < l2) ok = false;
+                        if (ok) {
+                            const int item = base + zz * st2;
+                            wb[zz] += (double)gw[item];
+                            vb[zz] += (double)gv[item];
+                        }
                     }
                 }
             }
             // Wbar out
-            const PermBlock &pb = P.ch.pb[rd[2]];
             const long long wl = s_wb[reg] + (long long)yy * s_ws[reg][0] + (long long)xx * s_ws[reg][1];
-            const long long half = (long long)pb.Ty * o * pb.Tx * o * pb.rzp;
             if (P.split == 0) {
                 RunBuf<StageT, SB> bw;
 #pragma unroll
@@ -553,19 +616,16 @@ __global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4) k_f2t(F2P<S
                 st_run(dst + half, bl, lz);
             }
             // V-term gradients: v = ovov[p,x,q,y] t1[r,z] + t2[q,p,y,x] fvo[z,r]
-            const int p = rd[6], q = rd[7];
             const int x = R.st[pp[0]] + xx, y = R.st[pp[1]] + yy;
-            const int pair = pair_index(pt[0], pt[1]);
             const int te = (pair * NV + cslot(pp[0]) * SB + xx) * NVP + cslot(pp[1]) * SB + yy;
             const double ovv = (double)tOV[te], t2v = (double)tT2[te];
-            const StageT *a1 = tT1 + pt[2] * NV + zl0, *f1 = tFV + pt[2] * NV + zl0;
             double rs1 = 0.0, rs2 = 0.0;
 #pragma unroll
             for (int zz = 0; zz < SB; zz++) {
                 rs1 += vb[zz] * (double)a1[zz];
                 rs2 += vb[zz] * (double)f1[zz];
-                colv[zz] = vb[zz] * ovv;
-                colv[SB + zz] = vb[zz] * t2v;
+                colv[zz] += vb[zz] * ovv;
+                colv[SB + zz] += vb[zz] * t2v;
             }
             atomicAdd(&P.ovov_bar[(((long long)p * v + x) * o + q) * v + y], rs1);
             atomicAdd(&P.t2_bar[(((long long)q * o + p) * v + y) * v + x], rs2);
@@ -573,8 +633,8 @@ __global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4) k_f2t(F2P<S
         // column sums over the region's runs: t1_bar[r, z], fvo_bar[z, r]
         const double cv = group_reduce_scatter<2 * SB, GL>(colv, lane);
         const int cidx = lane % (2 * SB);
-        if (inrange && (lane % GL) < 2 * SB && (cidx % SB) < lz && cv != 0.0) {
-            const int r = rd[8], z = R.st[pp[2]] + cidx % SB;
+        if (inrange && gl < 2 * SB && (cidx % SB) < lz && cv != 0.0) {
+            const int z = R.st[pp[2]] + cidx % SB;
             if (cidx < SB) atomicAdd(&P.t1_bar[(long long)r * v + z], cv);
             else atomicAdd(&P.fvo_bar[(long long)z * o + r], cv);
         }

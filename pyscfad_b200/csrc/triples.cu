@@ -790,11 +790,20 @@ template <typename StageT>
 static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
     constexpr int kSB = sizeof(StageT) == 4 ? 8 : 4;   // epilogue sub-block edge
     {
-        static bool f2_attr = false;
-        if (!f2_attr) {
+        // once per device (and element type): shared-memory opt-in and the
+        // constant tables of the epilogue's region patterns
+        constexpr int kMaxDev = 64;
+        static bool f2_ready[kMaxDev] = {};
+        int dev = 0;
+        TB_CUDA(cudaGetDevice(&dev));
+        if (dev < 0 || dev >= kMaxDev) return TRIPLES_ERR_UNSUPPORTED;
+        if (!f2_ready[dev]) {
             TB_CUDA(cudaFuncSetAttribute(k_f2t<StageT, kSB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)f2_smem_bytes<StageT, kSB>()));
-            f2_attr = true;
+            static F2Pattern pats[kF2Patterns];
+            f2_build_patterns(pats);
+            TB_CUDA(cudaMemcpyToSymbol(c_f2pat, pats, sizeof(pats)));
+            f2_ready[dev] = true;
         }
     }
     const Dims d = P.d;

@@ -184,7 +184,7 @@ def load_traffic(workload, precision):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "mixed_bf16", "fp64"])
@@ -312,26 +312,51 @@ def main():
             peaks = json.load(f)
     except (OSError, ValueError):
         pass
-    dom = max((k for k in prof if k in flops), key=lambda k: prof[k][0], default=None)
-    roof = None
-    if dom and prof[dom][0] > 0:
-        per_launch_flops = flops[dom] * args.steps / max(prof[dom][1], 1)
-        avg_s = prof[dom][0] / 1e3 / max(prof[dom][1], 1)
-        achieved = per_launch_flops / avg_s / 1e12
-        traffic = load_traffic(args.workload, args.precision).get(dom)
-        if args.precision == "fp64":
-            peak, note = 40.0, "nominal B200 FP64 (no measured FP64 peak on this pool)"
-        elif "bf16_tflops_sustained" in peaks:
-            peak, note = float(peaks["bf16_tflops_sustained"]), "of measured (cuBLAS bf16, sustained)"
+    # per kernel class: tensor classes against the GEMM peak (algorithmic flops),
+    # the epilogue against HBM bandwidth (algorithmic bytes: each raw amplitude
+    # W read once, its adjoint Wbar written once); the dominant class by time
+    # is the headline roofline
+    elem = float(o) ** 3 * float(v) ** 3
+    sz = 8 if args.precision == "fp64" else 4
+    algo_bytes = {"f2_epilogue": elem * 2 * sz}
+    if args.precision == "fp64":
+        tpeak, tnote = 40.0, "nominal B200 FP64 (no measured FP64 peak on this pool)"
+    elif "bf16_tflops_sustained" in peaks:
+        tpeak, tnote = float(peaks["bf16_tflops_sustained"]), "of measured (cuBLAS bf16, sustained)"
+    else:
+        tpeak, tnote = 1400.0, "of fallback (sustained)"
+    if "hbm_gbs" in peaks:
+        hpeak, hnote = float(peaks["hbm_gbs"]), "of measured (copy)"
+    else:
+        hpeak, hnote = 6650.0, "of fallback"
+    traffic_tab = load_traffic(args.workload, args.precision)
+    total_ms = sum(m for m, _ in prof.values()) or 1.0
+    classes = {}
+    for k, (ms, cnt) in prof.items():
+        if cnt <= 0 or ms <= 0:
+            continue
+        avg_s = ms / 1e3 / cnt
+        if k in flops and k != "step":
+            ach = flops[k] * args.steps / cnt / avg_s / 1e12
+            ent = {"bound": "tensor", "achieved": ach, "peak": tpeak, "unit": "TFLOP/s", "frac": ach / tpeak}
+            if args.precision != "fp64":
+                ent["frac_emulated"] = ach / (tpeak / 3)   # 3 split products per FP32-level product
+        elif k in algo_bytes:
+            ach = algo_bytes[k] * args.steps / cnt / avg_s / 1e9
+            ent = {"bound": "hbm", "achieved": ach, "peak": hpeak, "unit": "GB/s", "frac": ach / hpeak}
         else:
-            peak, note = 1400.0, "of fallback (sustained)"
-        roof = {"bound": "tensor", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": achieved / peak, "traffic": traffic, "peak_note": note,
-                "launches": prof[dom][1], "avg_launch_ms": avg_s * 1e3}
-        if args.precision != "fp64":
-            roof["split_products"] = 3
-            roof["peak_emulated"] = peak / 3
-            roof["frac_emulated"] = achieved / (peak / 3)
+            continue
+        ent.update({"kernel": k, "launches": cnt, "avg_launch_ms": avg_s * 1e3, "share": ms / total_ms})
+        classes[k] = ent
+    roof = None
+    if classes:
+        dom = max(classes, key=lambda k: prof[k][0])
+        roof = dict(classes[dom])
+        roof["traffic"] = traffic_tab.get(dom)
+        roof["peak_note"] = hnote if roof["bound"] == "hbm" else tnote
+        roof["classes"] = {k: {kk: (round(vv, 4) if isinstance(vv, float) else vv) for kk, vv in c.items()
+                               if kk in ("bound", "achieved", "frac", "frac_emulated", "share")}
+                           for k, c in classes.items()}
 
     line = {
         "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
@@ -346,6 +371,7 @@ def main():
                    "e_t": e_val},
         "e2e": {"value": e2e_value, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(sum(c for _, c in prof.values())),
+        "triplets_per_s": world * args.steps * (o * (o + 1) * (o + 2) // 6) / t_dev,
         "kernel_ms": {k: round(m, 3) for k, (m, _) in prof.items()},
         "roofline": roof,
         "clocks": clk,

@@ -87,6 +87,35 @@ int triples_energy_vjp(void *stream, int precision, int nocc, int nvir, int ovvv
                        double *ovoo_bar, double *ovov_bar, double *ovvv_bar,
                        double *fvo_bar);
 
+/* Size of the fixed device scratch behind triples_energy_vjp_static. */
+#define TRIPLES_STATIC_SCRATCH_BYTES ((size_t)64 << 20)
+
+/* triples_energy_vjp without a workspace argument and without any device
+ * allocation, for callers that may not allocate device memory (code that runs
+ * inside another framework's memory pool, or a host program that must keep
+ * its device footprint fixed).  No counterpart in the reference, which
+ * allocates its own scratch with malloc.
+ * The scratch is a fixed array of TRIPLES_STATIC_SCRATCH_BYTES (64 MiB) in
+ * the library, held by every device that loads it until the process exits.
+ * Problems with triples_workspace_size(precision, nocc, nvir, ovvv_packed, 1)
+ * above that limit are rejected with TRIPLES_ERR_WORKSPACE before any GPU
+ * work (for example FP64 fits nocc = 5 with nvir up to 57, mixed nocc = 8 with
+ * nvir up to 41).
+ * The first call on a device looks up the array's device address and does the
+ * library's one-time kernel set-up; make that first call before any stream
+ * capture.  Each call clears the parts of the scratch that must start at zero.
+ * All calls share the one array: calls whose GPU work overlaps (other streams,
+ * other host threads) race and must be serialised by the caller.  Inputs,
+ * outputs and results are exactly those of triples_energy_vjp. */
+int triples_energy_vjp_static(void *stream, int precision, int nocc, int nvir, int ovvv_packed,
+                              const double *mo_energy, const double *t1, const double *t2,
+                              const double *ovoo, const double *ovov, const double *ovvv,
+                              const double *fvo, double ybar,
+                              double *e_out,
+                              double *mo_energy_bar, double *t1_bar, double *t2_bar,
+                              double *ovoo_bar, double *ovov_bar, double *ovvv_bar,
+                              double *fvo_bar);
+
 /* Synchronises `stream` and reports device-side failures of the last call
  * that used `workspace` (bounded waits that gave up): TRIPLES_OK or
  * TRIPLES_ERR_DEVICE_TIMEOUT. */

@@ -1140,6 +1140,7 @@ int profile_read(int max_cats, double *ms, int *launches) {
 
 const char *profile_name(int cat) { return (cat >= 0 && cat < P_NCAT) ? kProfNames[cat] : ""; }
 int last_cuda_error() { return g_last_cuda_error; }
+void set_last_cuda_error(int e) { g_last_cuda_error = e; }
 
 }  // namespace tb
 
@@ -1190,6 +1191,50 @@ int triples_energy_vjp(void *stream, int precision, int nocc, int nvir, int ovvv
     io.mo_energy_bar = mo_energy_bar; io.t1_bar = t1_bar; io.t2_bar = t2_bar; io.ovoo_bar = ovoo_bar;
     io.ovov_bar = ovov_bar; io.ovvv_bar = ovvv_bar; io.fvo_bar = fvo_bar;
     return triples_call(stream, precision, nocc, nvir, ovvv_packed, 1, io, workspace_bytes);
+}
+
+// Fixed scratch for callers that may not allocate device memory themselves
+// (for example code running inside another framework's memory pool or a
+// host program that must keep its device footprint fixed).  Every device
+// that loads this library holds the array until the process exits.  The
+// call clears what must start at zero (its control block and gradient
+// accumulators) on each use, so the last call's leftovers do no harm; two
+// calls whose GPU work overlaps share the array and race.
+static constexpr size_t kStaticScratchBytes = TRIPLES_STATIC_SCRATCH_BYTES;
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+static constexpr int kStaticMaxDevices = 64;
+static void *g_static_scratch_addr[kStaticMaxDevices] = {};
+
+int triples_energy_vjp_static(void *stream, int precision, int nocc, int nvir, int ovvv_packed,
+                              const double *mo_energy, const double *t1, const double *t2,
+                              const double *ovoo, const double *ovov, const double *ovvv,
+                              const double *fvo, double ybar, double *e_out, double *mo_energy_bar,
+                              double *t1_bar, double *t2_bar, double *ovoo_bar, double *ovov_bar,
+                              double *ovvv_bar, double *fvo_bar) {
+    const size_t need = triples_workspace_size(precision, nocc, nvir, ovvv_packed, 1);
+    if (need == 0) return TRIPLES_ERR_INVALID_ARGUMENT;
+    if (need > kStaticScratchBytes) return TRIPLES_ERR_WORKSPACE;   // problem too large for the fixed scratch
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        tb::set_last_cuda_error((int)e);
+        return TRIPLES_ERR_CUDA;
+    }
+    if (dev < 0 || dev >= kStaticMaxDevices) return TRIPLES_ERR_UNSUPPORTED;
+    if (g_static_scratch_addr[dev] == nullptr) {
+        // once per device, with that device current: the device address of the
+        // array (its host-side name is only a stand-in for the symbol)
+        void *addr = nullptr;
+        e = cudaGetSymbolAddress(&addr, g_static_scratch);
+        if (e != cudaSuccess || addr == nullptr) {
+            tb::set_last_cuda_error((int)e);
+            return TRIPLES_ERR_CUDA;
+        }
+        g_static_scratch_addr[dev] = addr;
+    }
+    return triples_energy_vjp(stream, precision, nocc, nvir, ovvv_packed, mo_energy, t1, t2, ovoo, ovov, ovvv,
+                              fvo, ybar, g_static_scratch_addr[dev], kStaticScratchBytes, e_out, mo_energy_bar,
+                              t1_bar, t2_bar, ovoo_bar, ovov_bar, ovvv_bar, fvo_bar);
 }
 
 int triples_check_device_status(void *stream, const void *workspace) {

@@ -50,6 +50,22 @@ def _env_int(name, default):
         return default
 
 
+def max_over_ranks(x, device=None):
+    """Largest value of x over all ranks (the slowest replica sets the job time)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t)
+
+
+def job_throughput(world, steps, flops_per_step, t_max):
+    """Whole-job TFLOP/s: every replica ran `steps` steps; the job took t_max seconds."""
+    return world * steps * flops_per_step / t_max / 1e12
+
+
 def algorithmic_flops(o, v):
     """Per step and per kernel class (the tensor contractions only)."""
     main = 2.0 * o ** 3 * v ** 4
@@ -181,6 +197,44 @@ def load_traffic(workload, precision):
         return {}
 
 
+def run_accuracy(args, o, v, naux):
+    """Precision report: the mixed modes against the FP64 path on the same seeded
+    inputs, with the FP64-vs-FP64 difference of two summation orders (block
+    sizes 16 and 8) as the noise floor."""
+    import numpy as np
+    import torch
+
+    from pyscfad_b200 import triples
+    from pyscfad_b200.synthetic import make_inputs_torch
+
+    dev = torch.device("cuda", 0)
+    inp = make_inputs_torch(o, v, naux, seed=args.seed, device=dev, fvo_sigma=1e-3, scale=args.scale)
+    il, jl = torch.tril_indices(v, v, device=dev)
+    inp["ovvv"] = inp["ovvv"][:, :, il, jl].contiguous()
+    xs = [inp[k] for k in triples.KEYS]
+
+    def run(prec, tv=0):
+        triples.set_block_size(tv)
+        e, g = triples.energy_vjp(*xs, ybar=1.0, precision=prec, device=dev)
+        torch.cuda.synchronize()
+        triples.set_block_size(0)
+        return float(e), {k: t.cpu().numpy() for k, t in g.items()}
+
+    e64, g64 = run("fp64", 16)
+    e64b, _ = run("fp64", 8)
+
+    def relerr(a, b):
+        return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+    out = {"workload": args.workload, "nocc": o, "nvir": v, "naux": naux, "scale": args.scale,
+           "e_fp64": e64, "fp64_noise_abs": abs(e64 - e64b), "fp64_noise_rel": abs(e64 - e64b) / abs(e64)}
+    for prec in ("mixed", "mixed_bf16"):
+        e, g = run(prec)
+        out[prec] = {"e": e, "abs_dE": abs(e - e64), "rel_dE": abs(e - e64) / abs(e64),
+                     "grad_rel_err": {k: relerr(g[k], g64[k]) for k in g64}}
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -192,6 +246,11 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--cpu-target", type=float, default=8.0, help="seconds per CPU backward sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--accuracy", action="store_true",
+                    help="instead of timing: mixed modes vs FP64 on the same inputs (|dE|, relative "
+                         "errors, FP64 summation-order noise floor), one JSON line")
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="scale of the Cholesky-like factors (a small value gives a physically sized E(T))")
     args = ap.parse_args()
 
     world = _env_int("WORLD_SIZE", 1)
@@ -201,6 +260,9 @@ def main():
 
     if args.impl == "reference":
         run_reference(args, o, v, rank)
+        return
+    if args.accuracy:
+        run_accuracy(args, o, v, naux)
         return
 
     import torch
@@ -266,15 +328,12 @@ def main():
     lib.triples_profile_enable(0)
     prof = {lib.triples_profile_name(i).decode(): (ms[i], cnt[i]) for i in range(ncat)}
     t_dev = s0.elapsed_time(s1) / 1e3
-    if world > 1:
-        t = torch.tensor([t_dev], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_dev = float(t)
+    t_dev = max_over_ranks(t_dev, dev)
     _lib.check(triples.device_status(dev), "timed steps")
     del g
 
     flops = algorithmic_flops(o, v)
-    value = world * args.steps * flops["step"] / t_dev / 1e12
+    value = job_throughput(world, args.steps, flops["step"], t_dev)
 
     # end-to-end through the public API with host buffers
     host_in = [a.cpu().pin_memory() for a in dev_args]
@@ -301,11 +360,8 @@ def main():
     torch.cuda.synchronize()
     barrier()
     t_e2e = e0.elapsed_time(e1) / 1e3
-    if world > 1:
-        t = torch.tensor([t_e2e], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t)
-    e2e_value = world * args.steps * flops["step"] / t_e2e / 1e12
+    t_e2e = max_over_ranks(t_e2e, dev)
+    e2e_value = job_throughput(world, args.steps, flops["step"], t_e2e)
 
     # roofline of the dominant kernel class
     peaks = {}

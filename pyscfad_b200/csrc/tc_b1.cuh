@@ -47,7 +47,9 @@ struct TcB1Cfg {
     static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
     static constexpr int STAGES = (200 * 1024) / STAGE_BYTES;
     static constexpr int SMEM = STAGES * STAGE_BYTES + 256 + 1024;
-    static constexpr int TMEM_COLS = 2 * BN < 32 ? 32 : 2 * BN;
+    static constexpr int NACC = 4;   // TMEM accumulators: the epilogue sums them in pairs
+    static constexpr int TMEM_COLS = NACC * BN < 32 ? 32 : NACC * BN;
+    static_assert(NACC * BN <= 512, "TMEM holds 512 columns");
 };
 
 template <bool A_MN, int BN>
@@ -59,8 +61,8 @@ __global__ void __launch_bounds__(kB1Threads, 1)
     uint64_t *full = (uint64_t *)(smem + C::STAGES * C::STAGE_BYTES);
     uint64_t *empty = full + C::STAGES;
     uint64_t *tfull = empty + C::STAGES;
-    uint64_t *tempty = tfull + 2;
-    uint64_t *drain = tempty + 2;
+    uint64_t *tempty = tfull + C::NACC;
+    uint64_t *drain = tempty + C::NACC;
     uint32_t *tmem_slot = (uint32_t *)(drain + 1);
     __shared__ int s_abort;
 
@@ -71,7 +73,7 @@ __global__ void __launch_bounds__(kB1Threads, 1)
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        for (int a = 0; a < 2; a++) {
+        for (int a = 0; a < C::NACC; a++) {
             mbar_init(&tfull[a], 1);
             mbar_init(&tempty[a], 8);
         }
@@ -173,8 +175,8 @@ __global__ void __launch_bounds__(kB1Threads, 1)
         bool ok = true;
         for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
             for (int k0 = 0; k0 < nk && ok; k0 += P.kseg, seg++) {
-                const int acc = seg & 1;
-                const uint32_t accph = (seg >> 1) & 1;
+                const int acc = seg % C::NACC;
+                const uint32_t accph = (seg / C::NACC) & 1;
                 if (!mbar_wait(&tempty[acc], accph ^ 1u, abortp)) {
                     ok = false;
                     break;
@@ -239,10 +241,14 @@ __global__ void __launch_bounds__(kB1Threads, 1)
             double accd[HC];
 #pragma unroll
             for (int j = 0; j < HC; j++) accd[j] = 0.0;
-            for (int k0 = 0; k0 < nk; k0 += P.kseg, seg++) {
-                const int acc = seg & 1;
-                const uint32_t accph = (seg >> 1) & 1;
-                if (!mbar_wait(&tfull[acc], accph, abortp)) {
+            // segments in pairs: the two partials are added in FP32 (one rounding),
+            // then once into the FP64 sum
+            const int nseg = (nk + P.kseg - 1) / P.kseg;
+            for (int s0 = 0; s0 < nseg; s0 += 2, seg += 2) {
+                const bool two = s0 + 1 < nseg;
+                const int accA = seg % C::NACC, accB = (seg + 1) % C::NACC;
+                if (!mbar_wait(&tfull[accA], (uint32_t)((seg / C::NACC) & 1), abortp) ||
+                    (two && !mbar_wait(&tfull[accB], (uint32_t)(((seg + 1) / C::NACC) & 1), abortp))) {
                     *abortp = 1;
                     atomicOr(P.err, 32);
                     ok = false;
@@ -250,17 +256,25 @@ __global__ void __launch_bounds__(kB1Threads, 1)
                 }
                 tc_fence_after();
 #pragma unroll
-                for (int c = 0; c < HC / 32; c++) {
-                    uint32_t vv[32];
-                    tmem_ld32(tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * BN + half * HC + c * 32),
-                              vv);
+                for (int c = 0; c < HC / 8; c++) {
+                    const uint32_t lane_base = tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(half * HC + c * 8);
+                    uint32_t va[8], vb[8];
+                    tmem_ld8(lane_base + (uint32_t)(accA * BN), va);
+                    if (two) tmem_ld8(lane_base + (uint32_t)(accB * BN), vb);
                     tmem_ld_wait();
 #pragma unroll
-                    for (int j = 0; j < 32; j++) accd[c * 32 + j] += (double)__uint_as_float(vv[j]);
+                    for (int j = 0; j < 8; j++) {
+                        const float sum = two ? __uint_as_float(va[j]) + __uint_as_float(vb[j]) : __uint_as_float(va[j]);
+                        accd[c * 8 + j] += (double)sum;
+                    }
                 }
                 tc_fence_before();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&tempty[acc]);
+                if (lane == 0) {
+                    mbar_arrive(&tempty[accA]);
+                    if (two) mbar_arrive(&tempty[accB]);
+                }
+                if (!two) seg -= 1;   // an odd tail used one accumulator
             }
             if (!ok) break;
             const int b = t / per_batch, rem = t % per_batch;

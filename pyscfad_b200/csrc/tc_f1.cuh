@@ -27,12 +27,16 @@ struct TcCfg {
     static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
     static constexpr int STAGES = (BN >= 256) ? 2 : 3;
     static constexpr int BAR_BYTES = 256;
-    static constexpr int SMEM = STAGES * STAGE_BYTES + BAR_BYTES + 1024;
+    static constexpr int STORE_BYTES = 8 * 32 * 32 * 4;   // one 32 x 32 FP32 store box per epilogue warp
+    static constexpr int SMEM = STAGES * STAGE_BYTES + STORE_BYTES + BAR_BYTES + 1024;
     static constexpr int RT = BN / 16;
     static constexpr int TMEM_COLS = 2 * BN;
 };
 
 struct TcF1Params {
+    CUtensorMap tmS[6];       // per ordering with full 16 x 16 (x, z) blocks: S_tau as
+                              // [p][q][y][x][r*16+z], box {32, 16, 1, 1, 2}, 128B swizzle
+    int tmS_ok[6];            // 1 where tmS is valid (else plain stores)
     Dims d;
     ChunkDesc ch;
     int cum[7];        // prefix over orderings of tile counts
@@ -71,11 +75,13 @@ __device__ __forceinline__ F1Tile f1_decode(const TcF1Params &P, int t) {
 template <int BN>
 __global__ void __launch_bounds__(kF1Threads, 1)
     k_f1_tc(const __grid_constant__ CUtensorMap tmA1, const __grid_constant__ CUtensorMap tmB1,
-            const __grid_constant__ CUtensorMap tmA2, const __grid_constant__ CUtensorMap tmB2, TcF1Params P) {
+            const __grid_constant__ CUtensorMap tmA2, const __grid_constant__ CUtensorMap tmB2,
+            const __grid_constant__ TcF1Params P) {
     using C = TcCfg<BN>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    uint64_t *full = (uint64_t *)(smem + C::STAGES * C::STAGE_BYTES);
+    float *sstore = (float *)(smem + C::STAGES * C::STAGE_BYTES);   // 1024-byte aligned boxes
+    uint64_t *full = (uint64_t *)(smem + C::STAGES * C::STAGE_BYTES + C::STORE_BYTES);
     uint64_t *empty = full + C::STAGES;
     uint64_t *tfull = empty + C::STAGES;
     uint64_t *tempty = tfull + 2;
@@ -271,7 +277,41 @@ __global__ void __launch_bounds__(kF1Threads, 1)
             const bool vrow = (p < o) && (x < pb.Tx);
             float *dst = P.S + pb.soff +
                          ((((long long)(p * o + T.q) * pb.Ty + T.y) * pb.Tx + x) * o) * pb.Tz;
-            if (vrow) {
+            if (P.tmS_ok[T.tau]) {
+                // Full blocks: each 32 x 32 piece (lane = row = 16 p-local x 16 x) goes to
+                // this warp's 128B-swizzled shared box and leaves as one TMA store, so the
+                // rows reach HBM as whole 128-byte lines instead of 32 scattered 16-byte
+                // pieces per warp store.
+                float *box = sstore + (warp - 2) * 32 * 32;
+                const int p0 = T.mt * 8 + quarter * 2;
+#pragma unroll
+                for (int c = 0; c < HC / 32; c++) {
+                    if (c > 0) {
+                        if (lane == 0) bulk_wait_read0();
+                        __syncwarp();
+                    }
+#pragma unroll
+                    for (int ch = 0; ch < 8; ch++) {
+                        float4 w;
+                        w.x = accf[c * 32 + ch * 4 + 0] * sc;
+                        w.y = accf[c * 32 + ch * 4 + 1] * sc;
+                        w.z = accf[c * 32 + ch * 4 + 2] * sc;
+                        w.w = accf[c * 32 + ch * 4 + 3] * sc;
+                        if (vrow)
+                            wmax = fmaxf(wmax, fmaxf(fmaxf(fabsf(w.x), fabsf(w.y)), fmaxf(fabsf(w.z), fabsf(w.w))));
+                        *reinterpret_cast<float4 *>(box + lane * 32 + 4 * (ch ^ (lane & 7))) = w;
+                    }
+                    fence_proxy_async_smem();
+                    __syncwarp();
+                    const int rz0 = T.nt * BN + half * HC + c * 32;
+                    if (lane == 0 && p0 < o && rz0 < o * 16) {
+                        tma_store_5d(&P.tmS[T.tau], box, rz0, 0, T.y, T.q, p0);
+                        bulk_commit();
+                    }
+                }
+                if (lane == 0) bulk_wait_read0();
+                __syncwarp();
+            } else if (vrow) {
 #pragma unroll
                 for (int h = 0; h < HC / 16; h++) {
                     const int r = T.nt * C::RT + half * (HC / 16) + h;
@@ -302,6 +342,7 @@ __global__ void __launch_bounds__(kF1Threads, 1)
                 }
             }
         }
+        if (lane == 0) bulk_wait0();   // this warp's stores complete before the CTA retires
         for (int off = 16; off > 0; off >>= 1) wmax = fmaxf(wmax, __shfl_xor_sync(0xffffffffu, wmax, off));
         if (lane == 0 && wmax > 0.f) atomicMax(P.wmax_bits, __float_as_uint(wmax));
     }

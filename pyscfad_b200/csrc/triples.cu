@@ -775,6 +775,22 @@ static int make_tmap5(CUtensorMap *tm, void *base, bool bf16, const uint64_t dim
     return r == CUDA_SUCCESS ? TRIPLES_OK : TRIPLES_ERR_CUDA;
 }
 
+// 5-D map over S_tau, an FP32 [p][q][y][x][rz] array (rz innermost, o*16 values),
+// used by the W-contraction epilogue to store 32 x 32 pieces; 128B swizzle.
+static int make_tmap_stage(CUtensorMap *tm, float *base, int o, int Tx, int Ty) {
+    EncodeTiledFn enc = get_encode_fn();
+    if (!enc) return TRIPLES_ERR_UNSUPPORTED;
+    const cuuint64_t gdim[5] = {(cuuint64_t)o * 16, (cuuint64_t)Tx, (cuuint64_t)Ty, (cuuint64_t)o, (cuuint64_t)o};
+    cuuint64_t gstr[4];
+    gstr[0] = gdim[0] * sizeof(float);
+    for (int i = 1; i < 4; i++) gstr[i] = gstr[i - 1] * gdim[i];
+    const cuuint32_t box[5] = {32, 16, 1, 1, 2}, es[5] = {1, 1, 1, 1, 1};
+    CUresult r = enc(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, base, gdim, gstr, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? TRIPLES_OK : TRIPLES_ERR_CUDA;
+}
+
 static int num_sms() {
     static int n = 0;
     if (!n) {
@@ -955,6 +971,15 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                     T.err = &ctrl->err;
                     T.bf16 = bf16 ? 1 : 0;
                     T.kseg = g_kseg_f1;
+                    for (int t = 0; t < 6; t++) T.tmS_ok[t] = 0;
+                    for (int t = 0; t < ch.nperm; t++) {
+                        const PermBlock &pb = ch.pb[t];
+                        if (pb.Tx == 16 && pb.Tz == 16 && d.o >= 2) {
+                            const int trc = make_tmap_stage(&T.tmS[t], (float *)S + pb.soff, d.o, pb.Tx, pb.Ty);
+                            if (trc != TRIPLES_OK) return trc;
+                            T.tmS_ok[t] = 1;
+                        }
+                    }
                     const int tiles = T.cum[ch.nperm];
                     const int grid = tiles < num_sms() ? tiles : num_sms();
                     TB_KLAUNCH(P_F1, k_f1_tc<BN><<<grid, kF1Threads, TcCfg<BN>::SMEM, st>>>(tmA1, tmB1, tmA2, tmB2, T));

@@ -1029,6 +1029,7 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                                                                            ch.base[1], ch.nabc[1], ch.base[2], ch.nabc[2],
                                                                            io.ybar, bf16 ? 0 : 1));
                     F.wscale = &ctrl->wscale;
+                    }
                     F.ybar = io.ybar;
                     F.want_grad = P.want_grad;
                     F.e_part = e_part;
@@ -1267,7 +1268,10 @@ int triples_check_device_status(void *stream, const void *workspace) {
     tb::Ctrl c;
     cudaError_t e = cudaMemcpyAsync(&c, workspace, sizeof(c), cudaMemcpyDeviceToHost, (cudaStream_t)stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize((cudaStream_t)stream);
-    if (e != cudaSuccess) return TRIPLES_ERR_CUDA;
+    if (e != cudaSuccess) {
+        tb::set_last_cuda_error((int)e);
+        return TRIPLES_ERR_CUDA;
+    }
     return c.err ? TRIPLES_ERR_DEVICE_TIMEOUT : TRIPLES_OK;
 }
 

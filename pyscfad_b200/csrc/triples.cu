@@ -1029,7 +1029,6 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                                                                            ch.base[1], ch.nabc[1], ch.base[2], ch.nabc[2],
                                                                            io.ybar, bf16 ? 0 : 1));
                     F.wscale = &ctrl->wscale;
-                    }
                     F.ybar = io.ybar;
                     F.want_grad = P.want_grad;
                     F.e_part = e_part;

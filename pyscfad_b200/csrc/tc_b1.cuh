@@ -15,7 +15,7 @@
 // (the adjoint GEMMs of get_eris_amps_bar, ccsd_t_vjp.c:139-246, batched over
 // all occupied indices).  The second operand is always MN-major.  Products:
 // hi*hi + hi*lo + lo*hi into FP32 TMEM; the epilogue adds the descaled tile
-// into the FP64 gradient buffer (each output tile has a single owner).
+// into the FP64 gradient buffer.
 #pragma once
 #include "common.cuh"
 #include "tc_f1.cuh"
@@ -23,12 +23,20 @@
 
 namespace tb {
 
+// One launch covers one kind for ALL orderings tau of a chunk (tiles numbered
+// ordering by ordering), so small per-ordering tile counts do not leave SMs
+// idle.  Orderings that share an X (or Z) block write the same gradient rows,
+// hence the FP64 atomic adds in the epilogue.
 struct TcB1Params {
+    CUtensorMap tmA[6];     // per ordering: Wbar_tau (first operand)
+    CUtensorMap tmB[6];     // per ordering: second operand
     Dims d;
-    PermBlock pb;
+    PermBlock pb[6];
+    int nperm;
     int kind;
-    int nbatch, ntile_m, ntile_n;
-    int nk_outer, nk_inner;
+    int nbatch[6], ntile_m[6], ntile_n;
+    int nk_outer[6], nk_inner[6];
+    int cum[7];             // prefix of tile counts over orderings
     double *G;
     const double *wscale;   // device: per-chunk Wbar scale
     const double *oscale;   // device: scale of the second operand
@@ -54,7 +62,7 @@ struct TcB1Cfg {
 
 template <bool A_MN, int BN>
 __global__ void __launch_bounds__(kB1Threads, 1)
-    k_b1_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, TcB1Params P) {
+    k_b1_tc(const __grid_constant__ TcB1Params P) {
     using C = TcB1Cfg<A_MN, BN>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -81,8 +89,10 @@ __global__ void __launch_bounds__(kB1Threads, 1)
         fence_mbar_init();
     }
     if (warp == 0 && lane == 0) {
-        tma_prefetch_desc(&tmA);
-        tma_prefetch_desc(&tmB);
+        for (int t = 0; t < P.nperm; t++) {
+            tma_prefetch_desc(&P.tmA[t]);
+            tma_prefetch_desc(&P.tmB[t]);
+        }
     }
     if (warp == 1) {
         tmem_alloc(tmem_slot, C::TMEM_COLS);
@@ -93,12 +103,19 @@ __global__ void __launch_bounds__(kB1Threads, 1)
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
     volatile int *abortp = &s_abort;
-    const int per_batch = P.ntile_m * P.ntile_n;
-    const int total = P.nbatch * per_batch;
-    const int nk = P.nk_outer * P.nk_inner;
-    const PermBlock &pb = P.pb;
+    const int total = P.cum[P.nperm];
     const int o = P.d.o;
-    const int Ty = pb.Ty, Tz = pb.Tz;
+    // tile t -> ordering, batch, M tile, N tile
+    auto decode = [&](int t, int &tau, int &b, int &mt, int &nt) {
+        tau = 0;
+        while (tau + 1 < P.nperm && t >= P.cum[tau + 1]) tau++;
+        int rem = t - P.cum[tau];
+        const int per_batch = P.ntile_m[tau] * P.ntile_n;
+        b = rem / per_batch;
+        rem %= per_batch;
+        mt = rem / P.ntile_n;
+        nt = rem % P.ntile_n;
+    };
 
     if (warp == 0 && lane == 0) {
         // ---------------- TMA producer ----------------
@@ -109,8 +126,12 @@ __global__ void __launch_bounds__(kB1Threads, 1)
         for (int s = 0; s < C::STAGES; s++) pending[s] = false;
         bool ok = true;
         for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
-            const int b = t / per_batch, rem = t % per_batch;
-            const int mt = rem / P.ntile_n, nt = rem % P.ntile_n;
+            int tau, b, mt, nt;
+            decode(t, tau, b, mt, nt);
+            const PermBlock &pb = P.pb[tau];
+            const int Ty = pb.Ty, Tz = pb.Tz;
+            const int nk = P.nk_outer[tau] * P.nk_inner[tau];
+            const CUtensorMap *tmA = &P.tmA[tau], *tmB = &P.tmB[tau];
             for (int kb = 0; kb < nk; kb++) {
                 if (!mbar_wait(&empty[stage], phase ^ 1u, abortp)) {
                     ok = false;
@@ -120,32 +141,32 @@ __global__ void __launch_bounds__(kB1Threads, 1)
                 mbar_expect_tx(&full[stage], C::STAGE_BYTES);
                 uint8_t *sA = smem + stage * C::STAGE_BYTES;
                 uint8_t *sB = sA + 2 * C::A_BYTES;
-                const int ko = kb / P.nk_inner, ki = kb % P.nk_inner;
+                const int ko = kb / P.nk_inner[tau], ki = kb % P.nk_inner[tau];
                 for (int h = 0; h < 2; h++) {
                     uint8_t *a = sA + h * C::A_BYTES;
                     uint8_t *bb = sB + h * C::B_BYTES;
                     switch (P.kind) {
                     case 0:   // batch y, K = (q = ko, rz block = ki)
-                        tma_load_5d(a, &tmA, &full[stage], ki * 64, ko, 0, mt * 8, h * Ty + b);
+                        tma_load_5d(a, tmA, &full[stage], ki * 64, ko, 0, mt * 8, h * Ty + b);
                         for (int j = 0; j < BN / 64; j++)
-                            tma_load_5d(bb + j * 8192, &tmB, &full[stage], nt * BN + j * 64, pb.Z0, ki * 64 / Tz, ko, h);
+                            tma_load_5d(bb + j * 8192, tmB, &full[stage], nt * BN + j * 64, pb.Z0, ki * 64 / Tz, ko, h);
                         break;
                     case 1:   // batch q, K = (y = ko, p group = ki)
                         for (int j = 0; j < 2; j++)
-                            tma_load_5d(a + j * 8192, &tmA, &full[stage], mt * 128 + j * 64, b, 0, ki * 4, h * Ty + ko);
+                            tma_load_5d(a + j * 8192, tmA, &full[stage], mt * 128 + j * 64, b, 0, ki * 4, h * Ty + ko);
                         for (int j = 0; j < BN / 64; j++)
-                            tma_load_5d(bb + j * 8192, &tmB, &full[stage], nt * BN + j * 64, pb.X0, ki * 4, pb.Y0 + ko, h);
+                            tma_load_5d(bb + j * 8192, tmB, &full[stage], nt * BN + j * 64, pb.X0, ki * 4, pb.Y0 + ko, h);
                         break;
                     case 2:   // batch q, K = (y = ko, rz block = ki)
-                        tma_load_5d(a, &tmA, &full[stage], ki * 64, b, 0, mt * 8, h * Ty + ko);
+                        tma_load_5d(a, tmA, &full[stage], ki * 64, b, 0, mt * 8, h * Ty + ko);
                         for (int j = 0; j < BN / 64; j++)
-                            tma_load_5d(bb + j * 8192, &tmB, &full[stage], nt * BN + j * 64, pb.Z0, ki * 64 / Tz, pb.Y0 + ko, h);
+                            tma_load_5d(bb + j * 8192, tmB, &full[stage], nt * BN + j * 64, pb.Z0, ki * 64 / Tz, pb.Y0 + ko, h);
                         break;
                     default:  // batch y, K = (q = ko, p group = ki)
                         for (int j = 0; j < 2; j++)
-                            tma_load_5d(a + j * 8192, &tmA, &full[stage], mt * 128 + j * 64, ko, 0, ki * 4, h * Ty + b);
+                            tma_load_5d(a + j * 8192, tmA, &full[stage], mt * 128 + j * 64, ko, 0, ki * 4, h * Ty + b);
                         for (int j = 0; j < BN / 64; j++)
-                            tma_load_5d(bb + j * 8192, &tmB, &full[stage], nt * BN + j * 64, pb.X0, ki * 4, ko, h);
+                            tma_load_5d(bb + j * 8192, tmB, &full[stage], nt * BN + j * 64, pb.X0, ki * 4, ko, h);
                         break;
                     }
                 }
@@ -174,6 +195,9 @@ __global__ void __launch_bounds__(kB1Threads, 1)
         int seg = 0;   // running segment counter (same sequence as the epilogue)
         bool ok = true;
         for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+            int tau, b, mt, nt;
+            decode(t, tau, b, mt, nt);
+            const int nk = P.nk_outer[tau] * P.nk_inner[tau];
             for (int k0 = 0; k0 < nk && ok; k0 += P.kseg, seg++) {
                 const int acc = seg % C::NACC;
                 const uint32_t accph = (seg / C::NACC) & 1;
@@ -238,6 +262,11 @@ __global__ void __launch_bounds__(kB1Threads, 1)
         int seg = 0;
         bool ok = true;
         for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+            int tau, b, mt, nt;
+            decode(t, tau, b, mt, nt);
+            const PermBlock &pb = P.pb[tau];
+            const int Tz = pb.Tz;
+            const int nk = P.nk_outer[tau] * P.nk_inner[tau];
             double accd[HC];
 #pragma unroll
             for (int j = 0; j < HC; j++) accd[j] = 0.0;
@@ -277,8 +306,6 @@ __global__ void __launch_bounds__(kB1Threads, 1)
                 if (!two) seg -= 1;   // an odd tail used one accumulator
             }
             if (!ok) break;
-            const int b = t / per_batch, rem = t % per_batch;
-            const int mt = rem / P.ntile_n, nt = rem % P.ntile_n;
             long long roff = -1;
             if (P.kind == 0 || P.kind == 2) {
                 const int p = mt * 8 + row / 16, x = row % 16;
@@ -304,7 +331,7 @@ __global__ void __launch_bounds__(kB1Threads, 1)
 #pragma unroll
                 for (int j = 0; j < HC; j++) {
                     const int col = c0 + j;
-                    if (col < ncol) P.G[roff + col] += sc * accd[j];
+                    if (col < ncol) atomicAdd(&P.G[roff + col], sc * accd[j]);
                 }
             }
         }

@@ -1041,51 +1041,77 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                 if (!P.want_grad) continue;
                 // W-term gradients
                 if (mixed) {
+                    // one launch per kind over all orderings of the chunk
+                    const uint32_t bK[5] = {64, 1, 16, 8, 1};
+                    const uint32_t bM[5] = {64, 1, 16, 4, 1};
+                    CUtensorMap wk[6], wm[6];
+                    int lzs[6];
                     for (int t = 0; t < ch.nperm; t++) {
                         const PermBlock &pb = ch.pb[t];
                         const uint64_t dW[5] = {(uint64_t)pb.rzp, o, (uint64_t)pb.Tx, o, (uint64_t)(2 * pb.Ty)};
-                        const uint32_t bK[5] = {64, 1, 16, 8, 1};
-                        const uint32_t bM[5] = {64, 1, 16, 4, 1};
-                        CUtensorMap tmWk, tmWm;
                         void *wbase = (char *)SW + 2 * pb.swoff * 2;
                         int rc;
-                        if ((rc = make_tmap5(&tmWk, wbase, bf16, dW, bK)) != TRIPLES_OK) return rc;
-                        if ((rc = make_tmap5(&tmWm, wbase, bf16, dW, bM)) != TRIPLES_OK) return rc;
-                        int lz = 0;
-                        while ((1 << lz) < pb.Tz) lz++;
-                        TcB1Params B;
-                        B.d = d;
-                        B.pb = pb;
-                        B.wscale = &ctrl->wscale;
-                        B.err = &ctrl->err;
-                        B.bf16 = bf16 ? 1 : 0;
-                        B.kseg = g_kseg;
-                        const int nsm = num_sms();
-                        auto grid_of = [&](const TcB1Params &q) {
-                            int tiles = q.nbatch * q.ntile_m * q.ntile_n;
-                            return tiles < nsm ? tiles : nsm;
-                        };
-                        // ovvv gradient
-                        B.kind = 0; B.nbatch = pb.Ty; B.ntile_m = (d.o + 7) / 8; B.ntile_n = (d.v + 127) / 128;
-                        B.nk_outer = d.o; B.nk_inner = (d.o * pb.Tz + 63) / 64;
-                        B.G = GA1; B.oscale = &ctrl->scale[1]; B.sign = 1.0;
-                        TB_KLAUNCH(P_B1A, (k_b1_tc<false, 128><<<grid_of(B), kB1Threads, TcB1Cfg<false, 128>::SMEM, st>>>(tmWk, tmB1z[lz], B)));
-                        // t2 gradient, ovvv term
-                        B.kind = 1; B.nbatch = d.o; B.ntile_m = (d.o * pb.Tz + 127) / 128; B.ntile_n = (d.v + 127) / 128;
-                        B.nk_outer = pb.Ty; B.nk_inner = (d.o + 3) / 4;
-                        B.G = GB1; B.oscale = &ctrl->scale[0]; B.sign = 1.0;
-                        TB_KLAUNCH(P_B1B, (k_b1_tc<true, 128><<<grid_of(B), kB1Threads, TcB1Cfg<true, 128>::SMEM, st>>>(tmWm, tmA1m, B)));
-                        // ovoo gradient
-                        B.kind = 2; B.nbatch = d.o; B.ntile_m = (d.o + 7) / 8; B.ntile_n = (d.o + 63) / 64;
-                        B.nk_outer = pb.Ty; B.nk_inner = (d.o * pb.Tz + 63) / 64;
-                        B.G = GA2; B.oscale = &ctrl->scale[1]; B.sign = -1.0;
-                        TB_KLAUNCH(P_B1C, (k_b1_tc<false, 64><<<grid_of(B), kB1Threads, TcB1Cfg<false, 64>::SMEM, st>>>(tmWk, tmB2z[lz], B)));
-                        // t2 gradient, ooov term
-                        B.kind = 3; B.nbatch = pb.Ty; B.ntile_m = (d.o * pb.Tz + 127) / 128; B.ntile_n = (d.o + 63) / 64;
-                        B.nk_outer = d.o; B.nk_inner = (d.o + 3) / 4;
-                        B.G = GB2; B.oscale = &ctrl->scale[0]; B.sign = 1.0;
-                        TB_KLAUNCH(P_B1D, (k_b1_tc<true, 64><<<grid_of(B), kB1Threads, TcB1Cfg<true, 64>::SMEM, st>>>(tmWm, tmA2m, B)));
+                        if ((rc = make_tmap5(&wk[t], wbase, bf16, dW, bK)) != TRIPLES_OK) return rc;
+                        if ((rc = make_tmap5(&wm[t], wbase, bf16, dW, bM)) != TRIPLES_OK) return rc;
+                        lzs[t] = 0;
+                        while ((1 << lzs[t]) < pb.Tz) lzs[t]++;
                     }
+                    const int nsm = num_sms();
+                    TcB1Params B;
+                    B.d = d;
+                    B.nperm = ch.nperm;
+                    for (int t = 0; t < ch.nperm; t++) B.pb[t] = ch.pb[t];
+                    B.wscale = &ctrl->wscale;
+                    B.err = &ctrl->err;
+                    B.bf16 = bf16 ? 1 : 0;
+                    B.kseg = g_kseg;
+                    auto grid_of = [&]() {
+                        B.cum[0] = 0;
+                        for (int t = 0; t < ch.nperm; t++)
+                            B.cum[t + 1] = B.cum[t] + B.nbatch[t] * B.ntile_m[t] * B.ntile_n;
+                        const int tiles = B.cum[ch.nperm];
+                        return tiles < nsm ? tiles : nsm;
+                    };
+                    // ovvv gradient
+                    B.kind = 0; B.ntile_n = (d.v + 127) / 128;
+                    B.G = GA1; B.oscale = &ctrl->scale[1]; B.sign = 1.0;
+                    for (int t = 0; t < ch.nperm; t++) {
+                        const PermBlock &pb = ch.pb[t];
+                        B.tmA[t] = wk[t]; B.tmB[t] = tmB1z[lzs[t]];
+                        B.nbatch[t] = pb.Ty; B.ntile_m[t] = (d.o + 7) / 8;
+                        B.nk_outer[t] = d.o; B.nk_inner[t] = (d.o * pb.Tz + 63) / 64;
+                    }
+                    TB_KLAUNCH(P_B1A, (k_b1_tc<false, 128><<<grid_of(), kB1Threads, TcB1Cfg<false, 128>::SMEM, st>>>(B)));
+                    // t2 gradient, ovvv term
+                    B.kind = 1; B.ntile_n = (d.v + 127) / 128;
+                    B.G = GB1; B.oscale = &ctrl->scale[0]; B.sign = 1.0;
+                    for (int t = 0; t < ch.nperm; t++) {
+                        const PermBlock &pb = ch.pb[t];
+                        B.tmA[t] = wm[t]; B.tmB[t] = tmA1m;
+                        B.nbatch[t] = d.o; B.ntile_m[t] = (d.o * pb.Tz + 127) / 128;
+                        B.nk_outer[t] = pb.Ty; B.nk_inner[t] = (d.o + 3) / 4;
+                    }
+                    TB_KLAUNCH(P_B1B, (k_b1_tc<true, 128><<<grid_of(), kB1Threads, TcB1Cfg<true, 128>::SMEM, st>>>(B)));
+                    // ovoo gradient
+                    B.kind = 2; B.ntile_n = (d.o + 63) / 64;
+                    B.G = GA2; B.oscale = &ctrl->scale[1]; B.sign = -1.0;
+                    for (int t = 0; t < ch.nperm; t++) {
+                        const PermBlock &pb = ch.pb[t];
+                        B.tmA[t] = wk[t]; B.tmB[t] = tmB2z[lzs[t]];
+                        B.nbatch[t] = d.o; B.ntile_m[t] = (d.o + 7) / 8;
+                        B.nk_outer[t] = pb.Ty; B.nk_inner[t] = (d.o * pb.Tz + 63) / 64;
+                    }
+                    TB_KLAUNCH(P_B1C, (k_b1_tc<false, 64><<<grid_of(), kB1Threads, TcB1Cfg<false, 64>::SMEM, st>>>(B)));
+                    // t2 gradient, ooov term
+                    B.kind = 3; B.ntile_n = (d.o + 63) / 64;
+                    B.G = GB2; B.oscale = &ctrl->scale[0]; B.sign = 1.0;
+                    for (int t = 0; t < ch.nperm; t++) {
+                        const PermBlock &pb = ch.pb[t];
+                        B.tmA[t] = wm[t]; B.tmB[t] = tmA2m;
+                        B.nbatch[t] = pb.Ty; B.ntile_m[t] = (d.o * pb.Tz + 127) / 128;
+                        B.nk_outer[t] = d.o; B.nk_inner[t] = (d.o + 3) / 4;
+                    }
+                    TB_KLAUNCH(P_B1D, (k_b1_tc<true, 64><<<grid_of(), kB1Threads, TcB1Cfg<true, 64>::SMEM, st>>>(B)));
                 } else {
                 GemmLaunch<StageT> L;
                 L.d = d;

@@ -74,7 +74,7 @@ struct F2Smem {
     static constexpr int ITEMS = SB * SB * SB;
     static constexpr int NT = (SB == 8) ? 256 : ITEMS;     // threads per CTA
     static constexpr int IPT = ITEMS / NT;                  // items per thread
-    static_assert(12 * ITEMS <= 36 * REG, "item results overlay the W tile");
+    static_assert(12 * REG <= 36 * REG, "item results overlay the W tile");
 };
 
 template <typename StageT, int SB>
@@ -234,7 +234,7 @@ __global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4) k_f2t(F2P<S
     constexpr int NW = NT / 32;
     extern __shared__ __align__(16) uint8_t f2_smem[];
     StageT *sW = reinterpret_cast<StageT *>(f2_smem);
-    StageT *sG = sW;                      // item results [12][ITEMS] once W is consumed
+    StageT *sG = sW;                      // item results [12][REG] (padded) once W is consumed
     StageT *tOV = sW + 36 * REG;
     StageT *tT2 = tOV + C::TAB;
     StageT *tT1 = tT2 + C::TAB;
@@ -499,7 +499,10 @@ __global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4) k_f2t(F2P<S
         if (gvalid[it]) {
             const int item = tid + it * NT;
 #pragma unroll
-            for (int c = 0; c < 12; c++) sG[c * ITEMS + item] = gres[it][c];
+            // item (l0, l1, l2) at l0*SY + l1*SX + l2 in each of the 12 planes: the
+            // padded strides keep the write-back gathers within 2-way bank conflicts
+            const int gi = (item / (SB * SB)) * SY + ((item / SB) % SB) * SX + item % SB;
+            for (int c = 0; c < 12; c++) sG[c * REG + gi] = gres[it][c];
         }
     __syncthreads();
     for (int e = tid; e < NV; e += NT) {
@@ -530,7 +533,7 @@ __global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4) k_f2t(F2P<S
         perm_of(rd[0], pp);
         perm_of(rd[1], pt);
         auto cslot = [&](int j) { return j == 0 ? cs[0] : (j == 1 ? cs[1] : cs[2]); };
-        auto stride = [&](int j) { return j == 0 ? SB * SB : (j == 1 ? SB : 1); };
+        auto stride = [&](int j) { return j == 0 ? SY : (j == 1 ? SX : 1); };   // item-result layout
         const int zl0 = cslot(pp[2]) * SB;
         const int p = rd[6], q = rd[7], r = rd[8];
         const int pair = pair_index(pt[0], pt[1]);
@@ -549,7 +552,7 @@ __global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4) k_f2t(F2P<S
             if (simple) {
                 const int s = pat.sof[rd[0] * 6 + rd[1]];
                 const int base = xx * stride(pp[0]) + yy * stride(pp[1]), st2 = stride(pp[2]);
-                const StageT *gw = sG + s * ITEMS + base, *gv = sG + (6 + s) * ITEMS + base;
+                const StageT *gw = sG + s * REG + base, *gv = sG + (6 + s) * REG + base;
 #pragma unroll
                 for (int zz = 0; zz < SB; zz++) {
                     wb[zz] = (zz < lz) ? (double)gw[zz * st2] : 0.0;
@@ -566,7 +569,7 @@ __global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4) k_f2t(F2P<S
                     perm_of(pr / 6, q3);
                     // item slot j takes the region coordinate whose ordering slot is j
                     const int base = xx * stride(q3[0]) + yy * stride(q3[1]), st2 = stride(q3[2]);
-                    const StageT *gw = sG + s * ITEMS, *gv = sG + (6 + s) * ITEMS;
+                    const StageT *gw = sG + s * REG, *gv = sG + (6 + s) * REG;
 #pragma unroll
                     for (int zz = 0; zz < SB; zz++) {
                         if (zz >= lz) continue;

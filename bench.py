@@ -213,24 +213,48 @@ def run_accuracy(args, o, v, naux):
     inp["ovvv"] = inp["ovvv"][:, :, il, jl].contiguous()
     xs = [inp[k] for k in triples.KEYS]
 
+    a0, a1 = args.slice if args.slice else (0, 0)
+    stream = torch.cuda.current_stream(dev)
+
     def run(prec, tv=0):
         triples.set_block_size(tv)
-        e, g = triples.energy_vjp(*xs, ybar=1.0, precision=prec, device=dev)
-        torch.cuda.synchronize()
-        triples.set_block_size(0)
-        return float(e), {k: t.cpu().numpy() for k, t in g.items()}
+        triples.set_chunk_range(a0, a1)
+        try:
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            t0.record(stream)
+            e, g = triples.energy_vjp(*xs, ybar=1.0, precision=prec, device=dev)
+            t1.record(stream)
+            torch.cuda.synchronize()
+        finally:
+            triples.set_block_size(0)
+            triples.set_chunk_range(0, 0)
+        return float(e), {k: t.cpu().numpy() for k, t in g.items()}, t0.elapsed_time(t1) / 1e3
 
-    e64, g64 = run("fp64", 16)
-    e64b, _ = run("fp64", 8)
+    if args.slice:   # one-time set-up of both paths outside the timed calls
+        triples.set_chunk_range(0, 1)
+        for prec in ("fp64", "mixed", "mixed_bf16"):
+            triples.energy_vjp(*xs, ybar=1.0, precision=prec, device=dev)
+        torch.cuda.synchronize()
+        triples.set_chunk_range(0, 0)
+    e64, g64, t64 = run("fp64", 16)
+    e64b = e64 if args.slice else run("fp64", 8)[0]
 
     def relerr(a, b):
         return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
 
     out = {"workload": args.workload, "nocc": o, "nvir": v, "naux": naux, "scale": args.scale,
-           "e_fp64": e64, "fp64_noise_abs": abs(e64 - e64b), "fp64_noise_rel": abs(e64 - e64b) / abs(e64)}
+           "e_fp64": e64, "fp64_seconds": t64}
+    if args.slice:
+        frac = triples.chunk_fraction(v, a0, a1)
+        out.update({"slice_blocks": [a0, a1], "slice_fraction_of_amplitudes": frac,
+                    "fp64_seconds_full_extrapolated": t64 / frac})
+    else:
+        out.update({"fp64_noise_abs": abs(e64 - e64b), "fp64_noise_rel": abs(e64 - e64b) / abs(e64)})
     for prec in ("mixed", "mixed_bf16"):
-        e, g = run(prec)
-        out[prec] = {"e": e, "abs_dE": abs(e - e64), "rel_dE": abs(e - e64) / abs(e64),
+        e, g, tm = run(prec)
+        out[prec] = {"e": e, "abs_dE": abs(e - e64), "rel_dE": abs(e - e64) / abs(e64), "seconds": tm,
+                     "speedup_vs_fp64": t64 / tm,
                      "grad_rel_err": {k: relerr(g[k], g64[k]) for k in g64}}
     print(json.dumps(out))
 
@@ -249,6 +273,9 @@ def main():
     ap.add_argument("--accuracy", action="store_true",
                     help="instead of timing: mixed modes vs FP64 on the same inputs (|dE|, relative "
                          "errors, FP64 summation-order noise floor), one JSON line")
+    ap.add_argument("--slice", type=int, nargs=2, metavar=("A0", "A1"), default=None,
+                    help="with --accuracy: only the chunks whose largest virtual block is in [A0, A1), "
+                         "timed in both precisions (FP64 vs mixed on identical work)")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="scale of the Cholesky-like factors (a small value gives a physically sized E(T))")
     args = ap.parse_args()

@@ -132,6 +132,15 @@ int triples_last_cuda_error(void);
  * performance, not results beyond FP64 summation order. */
 void triples_set_block_size(int tv);
 
+/* Measurement: restrict the next calls to the chunks whose largest virtual
+ * block index lies in [a0, a1) (a1 <= 0: no upper bound; (0, 0) restores the
+ * full problem).  The energy and gradients are then the partial sums over
+ * those chunks, which add up exactly over a partition of the blocks; used to
+ * time or compare precisions on a slice of a problem too large to run whole
+ * (the reference's own slicing is ccsd_t_energy_vjp's a0/a1 job range,
+ * pyscfadlib/pyscfadlib/vjp/cc/ccsd_t_vjp.c:332-346). */
+void triples_set_chunk_range(int a0, int a1);
+
 /* Measurement: when enabled, every kernel launched by the calls above is
  * bracketed by CUDA events on the caller's stream (enabling clears earlier
  * records).  triples_profile_read() synchronises on those events and fills

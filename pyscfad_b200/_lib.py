@@ -63,6 +63,8 @@ def load():
     lib.triples_set_accumulation_segment.argtypes = [_c_int]
     lib.triples_set_block_size.restype = None
     lib.triples_set_block_size.argtypes = [_c_int]
+    lib.triples_set_chunk_range.restype = None
+    lib.triples_set_chunk_range.argtypes = [_c_int, _c_int]
     _lib = lib
     return lib
 

@@ -23,6 +23,7 @@ namespace tb {
 
 static thread_local int g_last_cuda_error = 0;
 static int g_tv_override = 0;
+static int g_chunk_a0 = 0, g_chunk_a1 = 0;   // chunk slice by largest virtual block (a1 <= 0: all)
 static int g_kseg = 1;     // K blocks per FP32 accumulation segment of the adjoint contractions
 static int g_kseg_f1 = 1;  // same for the W contraction
 
@@ -943,7 +944,8 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
         }
     }
 
-    for (int A = 0; A < P.nb; A++)
+    for (int A = 0; A < P.nb; A++) {
+        if (A < g_chunk_a0 || (g_chunk_a1 > 0 && A >= g_chunk_a1)) continue;
         for (int B = 0; B <= A; B++)
             for (int C = 0; C <= B; C++) {
                 ChunkDesc ch;
@@ -1138,6 +1140,7 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                 }
                 }
             }
+    }
 
     if (P.want_grad) {
         if (P.packed) {
@@ -1161,6 +1164,10 @@ int run_triples(const Plan &P, cudaStream_t st, const TriplesIO &io) {
 }
 
 void set_block_size(int tv) { g_tv_override = tv; }
+void set_chunk_range(int a0, int a1) {
+    g_chunk_a0 = a0 > 0 ? a0 : 0;
+    g_chunk_a1 = a1;
+}
 void set_kseg(int k) {
     g_kseg = k > 0 ? k : 1;
     g_kseg_f1 = g_kseg;
@@ -1317,6 +1324,8 @@ int triples_last_cuda_error(void) { return tb::last_cuda_error(); }
 const char *triples_version(void) { return "0.1.0"; }
 
 void triples_set_block_size(int tv) { tb::set_block_size(tv); }
+
+void triples_set_chunk_range(int a0, int a1) { tb::set_chunk_range(a0, a1); }
 
 void triples_set_accumulation_segment(int kblocks) { tb::set_kseg(kblocks); }
 

@@ -57,6 +57,37 @@ def set_block_size(tv: int):
     _lib.load().triples_set_block_size(int(tv))
 
 
+def set_chunk_range(a0: int = 0, a1: int = 0):
+    """Restrict later calls to chunks whose largest virtual block is in [a0, a1);
+    (0, 0) restores the full problem (see triples_set_chunk_range)."""
+    _lib.load().triples_set_chunk_range(int(a0), int(a1))
+
+
+def block_sizes(nvir: int, tv: int = 16):
+    """Virtual block sizes of the chunk decomposition: nvir // tv blocks of tv,
+    then the remainder split into descending powers of two."""
+    sizes = [tv] * (nvir // tv)
+    rem, bit = nvir - tv * (nvir // tv), tv >> 1
+    while bit:
+        if rem & bit:
+            sizes.append(bit)
+        bit >>= 1
+    return sizes
+
+
+def chunk_fraction(nvir: int, a0: int, a1: int, tv: int = 16) -> float:
+    """Fraction of all raw amplitudes o^3 v^3 that the chunks with largest block
+    in [a0, a1) hold (each chunk holds o^3 * (distinct orderings) * nA nB nC)."""
+    n = block_sizes(nvir, tv)
+    tot = 0
+    for A in range(a0, min(a1, len(n))):
+        for B in range(A + 1):
+            for C in range(B + 1):
+                nperm = len({(A, B, C), (A, C, B), (B, A, C), (B, C, A), (C, A, B), (C, B, A)})
+                tot += nperm * n[A] * n[B] * n[C]
+    return tot / float(nvir) ** 3
+
+
 def workspace_size(nocc, nvir, packed=True, want_grad=True, precision="fp64") -> int:
     return int(_lib.load().triples_workspace_size(_lib.PRECISION[precision], nocc, nvir,
                                                   int(packed), int(want_grad)))

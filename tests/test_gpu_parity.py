@@ -87,3 +87,27 @@ def test_repeated_calls_are_stable():
     inp, e_ref, _, _ = G.load("o4v9_fvo")
     es = [_run(inp, packed=True)[0] for _ in range(3)]
     assert max(es) - min(es) <= 1e-14 * abs(e_ref)
+
+
+@pytest.mark.parametrize("tv", [4, 16])
+def test_fp64_chunk_slices_partition_the_problem(tv):
+    """Energies and gradients of chunk slices that partition the virtual
+    blocks add up to the full result (the basis of slice timing)."""
+    triples.set_block_size(tv)
+    inp, e_ref, g_ref, _ = G.load("o5v19_fvo")
+    nb = len(triples.block_sizes(inp.t1.shape[1], tv))
+    cut = nb // 2
+    try:
+        parts = []
+        for a0, a1 in ((0, cut), (cut, nb)):
+            triples.set_chunk_range(a0, a1)
+            parts.append(_run(inp, packed=True))
+    finally:
+        triples.set_chunk_range(0, 0)
+    e = parts[0][0] + parts[1][0]
+    assert abs(e - e_ref) <= FP64_E_RTOL * abs(e_ref)
+    for k in G.KEYS:
+        if k == "ovvv":
+            continue
+        assert _relerr(parts[0][1][k] + parts[1][1][k], g_ref[k]) < FP64_G_RTOL, k
+    assert abs(parts[0][0]) > 0 and abs(parts[1][0]) > 0

@@ -197,6 +197,72 @@ def load_traffic(workload, precision):
         return {}
 
 
+def run_batched(args):
+    """Many small uneven problems: one CUDA-graph replay of the whole batch against
+    one E+VJP call per problem on one stream (each call being the kernel sequence
+    of one problem)."""
+    import numpy as np
+    import torch
+
+    from pyscfad_b200 import triples
+    from pyscfad_b200.batched import Autotuner, BatchedTriples
+    from pyscfad_b200.synthetic import make_inputs_torch
+
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(args.seed)
+    probs = []
+    for i in range(args.instances):
+        o = int(rng.integers(4, 13))
+        v = int(rng.integers(20, 81))
+        inp = make_inputs_torch(o, v, 4 * (o + v), seed=args.seed + 1000 + i, device=dev)
+        il, jl = torch.tril_indices(v, v, device=dev)
+        inp["ovvv"] = inp["ovvv"][:, :, il, jl].contiguous()
+        probs.append({k: inp[k] for k in triples.KEYS})
+    t0 = time.perf_counter()
+    bt = BatchedTriples(probs, precision=args.precision, lanes=8, autotuner=Autotuner())
+    t_tune = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    bt.capture()
+    t_cap = time.perf_counter() - t0
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def timed(fn, reps):
+        for _ in range(max(args.warmup, 1)):
+            fn()
+        torch.cuda.synchronize()
+        ev[0].record()
+        for _ in range(reps):
+            fn()
+        ev[1].record()
+        torch.cuda.synchronize()
+        return ev[0].elapsed_time(ev[1]) / 1e3 / reps
+
+    t_graph = timed(bt.run, max(args.steps, 3))
+    e_graph = np.array([e for e, _ in bt.results()])
+    bt.check()
+    # one call per problem, default block size, one stream
+
+    def one_by_one():
+        for p in probs:
+            triples.energy_vjp(*(p[k] for k in triples.KEYS), precision=args.precision, device=dev, check=False)
+
+    t_single = timed(one_by_one, 1)
+    t_lanes = timed(bt.run_eager, 1)
+    n = len(probs)
+    line = {"metric": "(T) E+VJP instances/s, batched uneven problems", "impl": "ours",
+            "config": {"workload": "batched_c3", "instances": n, "nocc": "U{4..12}", "nvir": "U{20..80}",
+                       "naux": "4(o+v)", "precision": args.precision, "lanes": bt.lanes},
+            "unit": "instances/s", "higher_is_better": True,
+            "graph_instances_per_s": n / t_graph, "graph_ms_per_batch": t_graph * 1e3,
+            "one_call_per_instance_per_s": n / t_single, "eager_lanes_per_s": n / t_lanes,
+            "speedup_graph_vs_one_call_per_instance": t_single / t_graph,
+            "autotune_s": t_tune, "capture_s": t_cap,
+            "tuned_block_sizes": {str(k): v for k, v in sorted(
+                {tv: sum(1 for p in bt.problems if p.tv == tv) for tv in (4, 8, 16)}.items())},
+            "e_sum": float(e_graph.sum())}
+    print(json.dumps(line))
+
+
 def run_accuracy(args, o, v, naux):
     """Precision report: the mixed modes against the FP64 path on the same seeded
     inputs, with the FP64-vs-FP64 difference of two summation orders (block
@@ -276,6 +342,10 @@ def main():
     ap.add_argument("--slice", type=int, nargs=2, metavar=("A0", "A1"), default=None,
                     help="with --accuracy: only the chunks whose largest virtual block is in [A0, A1), "
                          "timed in both precisions (FP64 vs mixed on identical work)")
+    ap.add_argument("--batched", action="store_true",
+                    help="instead of the headline: 256 uneven problems (nocc 4-12, nvir 20-80, naux 4(o+v)) "
+                         "as one CUDA-graph launch vs one call per problem; one JSON line")
+    ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--scale", type=float, default=1.0,
                     help="scale of the Cholesky-like factors (a small value gives a physically sized E(T))")
     args = ap.parse_args()
@@ -290,6 +360,9 @@ def main():
         return
     if args.accuracy:
         run_accuracy(args, o, v, naux)
+        return
+    if args.batched:
+        run_batched(args)
         return
 
     import torch

@@ -187,10 +187,16 @@ int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan
     size_t off = 0;
     auto take = [&](size_t bytes) { size_t at = off; off = align256(off + bytes); return at; };
     P.off_ctrl = take(kCtrlBytes);
-    P.off_A1 = take(v * o * v * Kp * el);
-    P.off_B1 = take(o * o * v * Kp * el);
-    P.off_A2 = take(o * o * v * o * el);
-    P.off_B2 = take(v * o * v * o * el);
+    // FP64 operand layouts: only the FP64 contractions read them (the split
+    // operands of the mixed modes are built straight from the inputs)
+    if (!mixed) {
+        P.off_A1 = take(v * o * v * Kp * el);
+        P.off_B1 = take(o * o * v * Kp * el);
+        P.off_A2 = take(o * o * v * o * el);
+        P.off_B2 = take(v * o * v * o * el);
+    } else {
+        P.off_A1 = P.off_B1 = P.off_A2 = P.off_B2 = 0;
+    }
     if (mixed) {
         P.off_A1h = take(2 * v * o * v * P.Kp8 * 2);
         P.off_B1h = take(2 * o * o * v * P.Kp8 * 2);
@@ -856,12 +862,14 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
         TB_CUDA(cudaMemsetAsync(io.fvo_bar, 0, v * o * sizeof(double), st));
     }
 
-    // FP64 operand layouts (used by the FP64 contractions)
-    TB_KLAUNCH(P_PREP, k_prep_A1<<<dim3((d.Kp + 31) / 32, (d.v + 31) / 32, (unsigned)(o * v)), dim3(32, 8), 0, st>>>(
-        io.ovvv, P.packed, d, A1));
-    TB_KLAUNCH(P_PREP, k_prep_B1<<<(unsigned)(o * o * v), 128, 0, st>>>(io.t2, d, B1));
-    TB_KLAUNCH(P_PREP, k_prep_A2<<<grid1d((long long)o * o * v * o, 256), 256, 0, st>>>(io.ovoo, d, A2));
-    TB_KLAUNCH(P_PREP, k_prep_B2<<<grid1d((long long)v * o * v * o, 256), 256, 0, st>>>(io.t2, d, B2));
+    // FP64 operand layouts (used by the FP64 contractions only)
+    if (!mixed) {
+        TB_KLAUNCH(P_PREP, k_prep_A1<<<dim3((d.Kp + 31) / 32, (d.v + 31) / 32, (unsigned)(o * v)), dim3(32, 8), 0, st>>>(
+            io.ovvv, P.packed, d, A1));
+        TB_KLAUNCH(P_PREP, k_prep_B1<<<(unsigned)(o * o * v), 128, 0, st>>>(io.t2, d, B1));
+        TB_KLAUNCH(P_PREP, k_prep_A2<<<grid1d((long long)o * o * v * o, 256), 256, 0, st>>>(io.ovoo, d, A2));
+        TB_KLAUNCH(P_PREP, k_prep_B2<<<grid1d((long long)v * o * v * o, 256), 256, 0, st>>>(io.t2, d, B2));
+    }
 
     // 16-bit split operands and tensor maps (tensor-core path)
     constexpr int BN = 256;

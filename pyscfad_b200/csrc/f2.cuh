@@ -207,19 +207,19 @@ inline void f2_build_patterns(F2Pattern out[kF2Patterns]) {
 // Sum NV (power of two) per-lane values over aligned groups of G lanes
 // (NV <= G <= 32, G a power of two); afterwards lane l holds the group total
 // of value (l % NV).
-template <int NV, int G>
-__device__ __forceinline__ double group_reduce_scatter(double (&v)[NV], int lane) {
+template <int NV, int G, typename T>
+__device__ __forceinline__ T group_reduce_scatter(T (&v)[NV], int lane) {
 #pragma unroll
     for (int h = NV / 2; h >= 1; h /= 2) {
         const bool up = (lane & h) != 0;
 #pragma unroll
         for (int i = 0; i < h; i++) {
-            const double send = up ? v[i] : v[i + h];
-            const double keep = up ? v[i + h] : v[i];
+            const T send = up ? v[i] : v[i + h];
+            const T keep = up ? v[i + h] : v[i];
             v[i] = keep + __shfl_xor_sync(0xffffffffu, send, h);
         }
     }
-    double r = v[0];
+    T r = v[0];
 #pragma unroll
     for (int h = NV; h < G; h *= 2) r += __shfl_xor_sync(0xffffffffu, r, h);
     return r;
@@ -415,7 +415,8 @@ __global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4) k_f2t(F2P<S
             double WW[6], X[6];
 #pragma unroll
             for (int s = 0; s < 6; s++) {
-                double sw = 0.0, sv = 0.0;
+                double sw = 0.0;
+                StageT sv = 0;   // V term: products of staged (StageT) factors
 #pragma unroll
                 for (int tau = 0; tau < 6; tau++) {
                     const int pi = perm_compose(s, tau);
@@ -425,11 +426,11 @@ __global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4) k_f2t(F2P<S
                     sw += (double)sW[pat.reg[pi * 6 + tau] * REG + loc[pp[1]] * SY + loc[pp[0]] * SX + loc[pp[2]]];
                     const int pair = pair_index(pt[0], pt[1]);
                     const int xl = vl[pp[0]], yl = vl[pp[1]], zl = vl[pp[2]];
-                    sv += (double)tOV[(pair * NV + xl) * NVP + yl] * (double)tT1[pt[2] * NV + zl] +
-                          (double)tT2[(pair * NV + xl) * NVP + yl] * (double)tFV[pt[2] * NV + zl];
+                    sv += tOV[(pair * NV + xl) * NVP + yl] * tT1[pt[2] * NV + zl] +
+                          tT2[(pair * NV + xl) * NVP + yl] * tFV[pt[2] * NV + zl];
                 }
                 WW[s] = sw;
-                X[s] = sw + 0.5 * sv;
+                X[s] = sw + 0.5 * (double)sv;
             }
             double Z[6], RW[6];
 #pragma unroll
@@ -540,27 +541,30 @@ __global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4) k_f2t(F2P<S
         const StageT *a1 = tT1 + pt[2] * NV + zl0, *f1 = tFV + pt[2] * NV + zl0;
         const PermBlock &pb = P.ch.pb[rd[2]];
         const long long half = (long long)pb.Ty * o * pb.Tx * o * pb.rzp;
-        double colv[2 * SB];
+        // V-term partials in the staging precision (FP32 in the mixed modes: 8-term
+        // row sums and the warp's 64-run column sums), added to the FP64 gradients
+        StageT colv[2 * SB];
 #pragma unroll
-        for (int c = 0; c < 2 * SB; c++) colv[c] = 0.0;
+        for (int c = 0; c < 2 * SB; c++) colv[c] = 0;
 #pragma unroll
         for (int u = 0; u < RPL; u++) {
             const int run = gl + u * GL;
             const int yy = run / SB, xx = run % SB;
             if (!(inrange && xx < lx && yy < ly)) continue;
-            double wb[SB], vb[SB];
+            StageT wb[SB], vb[SB];
             if (simple) {
                 const int s = pat.sof[rd[0] * 6 + rd[1]];
                 const int base = xx * stride(pp[0]) + yy * stride(pp[1]), st2 = stride(pp[2]);
                 const StageT *gw = sG + s * REG + base, *gv = sG + (6 + s) * REG + base;
 #pragma unroll
                 for (int zz = 0; zz < SB; zz++) {
-                    wb[zz] = (zz < lz) ? (double)gw[zz * st2] : 0.0;
-                    vb[zz] = (zz < lz) ? (double)gv[zz * st2] : 0.0;
+                    wb[zz] = (zz < lz) ? gw[zz * st2] : (StageT)0;
+                    vb[zz] = (zz < lz) ? gv[zz * st2] : (StageT)0;
                 }
             } else {
+                double wd[SB], vd[SB];   // several (s, tau) per position: sum in FP64
 #pragma unroll
-                for (int zz = 0; zz < SB; zz++) wb[zz] = vb[zz] = 0.0;
+                for (int zz = 0; zz < SB; zz++) wd[zz] = vd[zz] = 0.0;
                 const int nc = pat.ncombo[reg];
                 for (int c = 0; c < nc; c++) {
                     const int pr = pat.combo[reg][c];
@@ -581,10 +585,15 @@ __global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4) k_f2t(F2P<S
                         if (cs[2] == cs[1] && l1 < l2) ok = false;
                         if (ok) {
                             const int item = base + zz * st2;
-                            wb[zz] += (double)gw[item];
-                            vb[zz] += (double)gv[item];
+                            wd[zz] += (double)gw[item];
+                            vd[zz] += (double)gv[item];
                         }
                     }
+                }
+#pragma unroll
+                for (int zz = 0; zz < SB; zz++) {
+                    wb[zz] = (StageT)wd[zz];
+                    vb[zz] = (StageT)vd[zz];
                 }
             }
             // Wbar out
@@ -621,20 +630,20 @@ __global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4) k_f2t(F2P<S
             // V-term gradients: v = ovov[p,x,q,y] t1[r,z] + t2[q,p,y,x] fvo[z,r]
             const int x = R.st[pp[0]] + xx, y = R.st[pp[1]] + yy;
             const int te = (pair * NV + cslot(pp[0]) * SB + xx) * NVP + cslot(pp[1]) * SB + yy;
-            const double ovv = (double)tOV[te], t2v = (double)tT2[te];
-            double rs1 = 0.0, rs2 = 0.0;
+            const StageT ovv = tOV[te], t2v = tT2[te];
+            StageT rs1 = 0, rs2 = 0;
 #pragma unroll
             for (int zz = 0; zz < SB; zz++) {
-                rs1 += vb[zz] * (double)a1[zz];
-                rs2 += vb[zz] * (double)f1[zz];
+                rs1 += vb[zz] * a1[zz];
+                rs2 += vb[zz] * f1[zz];
                 colv[zz] += vb[zz] * ovv;
                 colv[SB + zz] += vb[zz] * t2v;
             }
-            atomicAdd(&P.ovov_bar[(((long long)p * v + x) * o + q) * v + y], rs1);
-            atomicAdd(&P.t2_bar[(((long long)q * o + p) * v + y) * v + x], rs2);
+            atomicAdd(&P.ovov_bar[(((long long)p * v + x) * o + q) * v + y], (double)rs1);
+            atomicAdd(&P.t2_bar[(((long long)q * o + p) * v + y) * v + x], (double)rs2);
         }
         // column sums over the region's runs: t1_bar[r, z], fvo_bar[z, r]
-        const double cv = group_reduce_scatter<2 * SB, GL>(colv, lane);
+        const double cv = (double)group_reduce_scatter<2 * SB, GL>(colv, lane);
         const int cidx = lane % (2 * SB);
         if (inrange && gl < 2 * SB && (cidx % SB) < lz && cv != 0.0) {
             const int z = R.st[pp[2]] + cidx % SB;

@@ -31,7 +31,7 @@ struct GemmArgsT {
     double *C;
     Map4 cm, cn;
     double alpha, alpha2;
-    int accumulate;
+    int accumulate;   // 1: C += result (2: as an FP64 atomic add, for tiles that share outputs)
 };
 using GemmArgs = GemmArgsT<double>;
 
@@ -163,6 +163,10 @@ __device__ void gemm_fp64_tile(const GemmArgsT<TA> &g, int m0, int n0, GemmSmem 
             if (n >= g.N) continue;
             long long off = cmo + apply(g.cn, n);
             double val = g.alpha * acc[i][j];
+            if (g.accumulate == 2) {
+                atomicAdd(&g.C[off], val);
+                continue;
+            }
             if (g.accumulate) val += g.C[off];
             g.C[off] = val;
         }

@@ -563,8 +563,10 @@ __global__ void __launch_bounds__(256) k_b1a_fp64(GemmLaunch<StageT> L) {
 template <typename StageT>
 __global__ void __launch_bounds__(256) k_b1b_fp64(GemmLaunch<StageT> L) {
     __shared__ GemmSmem sm;
-    const int q = blockIdx.z;
-    const PermBlock &pb = L.ch.pb[L.tau_only];
+    // grid.z = (ordering, q): all orderings of the chunk in one launch; orderings
+    // that share a block write the same gradient rows, hence the atomic adds
+    const int q = blockIdx.z % L.d.o;
+    const PermBlock &pb = L.ch.pb[blockIdx.z / L.d.o];
     const Dims &d = L.d;
     const int o = d.o, v = d.v, Kp = d.Kp;
     const long long oTz = (long long)o * pb.Tz;
@@ -585,7 +587,7 @@ __global__ void __launch_bounds__(256) k_b1b_fp64(GemmLaunch<StageT> L) {
     g.cn = map1(1);
     g.alpha = 1.0;
     g.alpha2 = 0.0;
-    g.accumulate = 1;
+    g.accumulate = 2;
     const int m0 = blockIdx.x * kGBM, n0 = blockIdx.y * kGBN;
     if (m0 >= g.M || n0 >= g.N) return;
     gemm_fp64_tile(g, m0, n0, sm);
@@ -595,8 +597,10 @@ __global__ void __launch_bounds__(256) k_b1b_fp64(GemmLaunch<StageT> L) {
 template <typename StageT>
 __global__ void __launch_bounds__(256) k_b1c_fp64(GemmLaunch<StageT> L) {
     __shared__ GemmSmem sm;
-    const int q = blockIdx.z;
-    const PermBlock &pb = L.ch.pb[L.tau_only];
+    // grid.z = (ordering, q): all orderings of the chunk in one launch; orderings
+    // that share a block write the same gradient rows, hence the atomic adds
+    const int q = blockIdx.z % L.d.o;
+    const PermBlock &pb = L.ch.pb[blockIdx.z / L.d.o];
     const Dims &d = L.d;
     const int o = d.o, v = d.v;
     const long long oTz = (long long)o * pb.Tz;
@@ -617,7 +621,7 @@ __global__ void __launch_bounds__(256) k_b1c_fp64(GemmLaunch<StageT> L) {
     g.cn = map1(1);
     g.alpha = -1.0;
     g.alpha2 = 0.0;
-    g.accumulate = 1;
+    g.accumulate = 2;
     const int m0 = blockIdx.x * kGBM, n0 = blockIdx.y * kGBN;
     if (m0 >= g.M || n0 >= g.N) return;
     gemm_fp64_tile(g, m0, n0, sm);
@@ -1137,15 +1141,14 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                 L.G = GB2;
                 TB_KLAUNCH(P_B1D, k_b1d_fp64<StageT><<<dim3((d.o * maxTz + kGBM - 1) / kGBM, (d.o + kGBN - 1) / kGBN, L.cum[ch.nperm]),
                                      256, 0, st>>>(L));
-                for (int t = 0; t < ch.nperm; t++) {
-                    L.tau_only = t;
-                    L.G = GB1;
-                    TB_KLAUNCH(P_B1B, k_b1b_fp64<StageT><<<dim3((d.o * ch.pb[t].Tz + kGBM - 1) / kGBM, (d.v + kGBN - 1) / kGBN, d.o),
-                                         256, 0, st>>>(L));
-                    L.G = GA2;
-                    TB_KLAUNCH(P_B1C, k_b1c_fp64<StageT><<<dim3((d.o * ch.pb[t].Tx + kGBM - 1) / kGBM, (d.o + kGBN - 1) / kGBN, d.o),
-                                         256, 0, st>>>(L));
-                }
+                L.G = GB1;
+                TB_KLAUNCH(P_B1B, k_b1b_fp64<StageT><<<dim3((d.o * maxTz + kGBM - 1) / kGBM, (d.v + kGBN - 1) / kGBN,
+                                                             (unsigned)(d.o * ch.nperm)),
+                                     256, 0, st>>>(L));
+                L.G = GA2;
+                TB_KLAUNCH(P_B1C, k_b1c_fp64<StageT><<<dim3((d.o * maxTx + kGBM - 1) / kGBM, (d.o + kGBN - 1) / kGBN,
+                                                             (unsigned)(d.o * ch.nperm)),
+                                     256, 0, st>>>(L));
                 }
             }
     }

@@ -228,7 +228,7 @@ __device__ __forceinline__ T group_reduce_scatter(T (&v)[NV], int lane) {
 template <typename StageT, int SB>
 __global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4) k_f2t(F2P<StageT> P) {
     using C = F2Smem<SB>;
-    constexpr int NT = C::NT, IPT = C::IPT, ITEMS = C::ITEMS;
+    constexpr int NT = C::NT, IPT = C::IPT;
     constexpr int REG = C::REG, NV = C::NV, NVP = C::NVP;
     constexpr int SX = C::SX, SY = C::SY;
     constexpr int NW = NT / 32;
@@ -499,10 +499,10 @@ __global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4) k_f2t(F2P<S
     for (int it = 0; it < IPT; it++)
         if (gvalid[it]) {
             const int item = tid + it * NT;
-#pragma unroll
             // item (l0, l1, l2) at l0*SY + l1*SX + l2 in each of the 12 planes: the
             // padded strides keep the write-back gathers within 2-way bank conflicts
             const int gi = (item / (SB * SB)) * SY + ((item / SB) % SB) * SX + item % SB;
+#pragma unroll
             for (int c = 0; c < 12; c++) sG[c * REG + gi] = gres[it][c];
         }
     __syncthreads();

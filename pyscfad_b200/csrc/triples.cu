@@ -480,7 +480,6 @@ struct GemmLaunch {
     Dims d;
     ChunkDesc ch;
     int cum[7];      // prefix sums used to decode blockIdx.z
-    int tau_only;    // >= 0: restrict to this ordering
     const double *A1, *B1, *A2, *B2;
     StageT *S;       // staging
     double *G;       // gradient target
@@ -536,7 +535,6 @@ __global__ void __launch_bounds__(256) k_b1a_fp64(GemmLaunch<StageT> L) {
     const int o = d.o, v = d.v, Kp = d.Kp;
     const int y = b - L.cum[t];
     const long long oTz = (long long)o * pb.Tz;
-    const long long sq = (long long)pb.Ty * pb.Tx * oTz;   // stride of q in S
     GemmArgsT<StageT> g;
     g.M = o * pb.Tx;
     g.N = v;
@@ -569,8 +567,6 @@ __global__ void __launch_bounds__(256) k_b1b_fp64(GemmLaunch<StageT> L) {
     const PermBlock &pb = L.ch.pb[blockIdx.z / L.d.o];
     const Dims &d = L.d;
     const int o = d.o, v = d.v, Kp = d.Kp;
-    const long long oTz = (long long)o * pb.Tz;
-    const long long sq = (long long)pb.Ty * pb.Tx * oTz;
     GemmArgsT<StageT> g;
     g.M = o * pb.Tz;
     g.N = v;
@@ -604,7 +600,6 @@ __global__ void __launch_bounds__(256) k_b1c_fp64(GemmLaunch<StageT> L) {
     const Dims &d = L.d;
     const int o = d.o, v = d.v;
     const long long oTz = (long long)o * pb.Tz;
-    const long long sq = (long long)pb.Ty * pb.Tx * oTz;
     GemmArgsT<StageT> g;
     g.M = o * pb.Tx;
     g.N = o;
@@ -637,8 +632,6 @@ __global__ void __launch_bounds__(256) k_b1d_fp64(GemmLaunch<StageT> L) {
     const Dims &d = L.d;
     const int o = d.o, v = d.v;
     const int y = b - L.cum[t];
-    const long long oTz = (long long)o * pb.Tz;
-    const long long sq = (long long)pb.Ty * pb.Tx * oTz;
     GemmArgsT<StageT> g;
     g.M = o * pb.Tz;
     g.N = o;
@@ -1001,7 +994,6 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                     GemmLaunch<double> L;
                     L.d = d;
                     L.ch = ch;
-                    L.tau_only = -1;
                     L.A1 = A1; L.B1 = B1; L.A2 = A2; L.B2 = B2;
                     L.S = (double *)S;
                     L.G = nullptr;
@@ -1130,7 +1122,6 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                 GemmLaunch<StageT> L;
                 L.d = d;
                 L.ch = ch;
-                L.tau_only = -1;
                 L.A1 = A1; L.B1 = B1; L.A2 = A2; L.B2 = B2;
                 L.S = reinterpret_cast<StageT *>(SW);
                 L.cum[0] = 0;

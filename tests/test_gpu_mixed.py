@@ -66,3 +66,34 @@ def test_mixed_random_vs_oracle(o, v, naux, seed):
     assert abs(e - e_ref) <= 1e-6 * abs(e_ref)
     for k in G.KEYS:
         assert _relerr(g[k], g_ref[k]) < 1e-5, k
+
+
+@pytest.mark.parametrize("precision", ["mixed", "mixed_bf16"])
+def test_mixed_energy_only_matches_energy_vjp(precision):
+    """triples_energy (no adjoint buffers) gives the energy of triples_energy_vjp."""
+    inp = make_inputs(9, 37, 70, seed=31, fvo_sigma=1e-3)
+    e_vjp, _ = _run(inp, True, precision)
+    e = float(triples.energy(inp.mo_energy, inp.t1, inp.t2, inp.ovoo, inp.ovov, inp.ovvv_tril(), inp.fvo,
+                             precision=precision, device="cuda"))
+    assert abs(e - e_vjp) <= 1e-12 * abs(e_vjp)
+
+
+def test_mixed_adjoint_seed_scales_gradients():
+    inp = make_inputs(7, 29, 60, seed=32, fvo_sigma=1e-3)
+    args = (inp.mo_energy, inp.t1, inp.t2, inp.ovoo, inp.ovov, inp.ovvv_tril(), inp.fvo)
+    _, g1 = triples.energy_vjp(*args, ybar=1.0, precision="mixed", device="cuda")
+    _, g3 = triples.energy_vjp(*args, ybar=-2.5, precision="mixed", device="cuda")
+    for k in G.KEYS:
+        a, b = g3[k].cpu().numpy(), -2.5 * g1[k].cpu().numpy()
+        assert _relerr(a, b) < 1e-9, k
+
+
+@pytest.mark.parametrize("o,v", [(1, 1), (2, 17), (3, 31), (13, 9)])
+def test_mixed_odd_shapes_vs_oracle(o, v):
+    """Ragged sizes: nvir not a multiple of 8 or of the block size, tiny nocc."""
+    inp = make_inputs(o, v, 4 * (o + v), seed=40 + o + v, fvo_sigma=1e-3)
+    e_ref, g_ref = O.oracle_energy_vjp(inp)
+    e, g = _run(inp, False, "mixed")
+    assert abs(e - e_ref) <= 1e-6 * max(abs(e_ref), 1e-12)
+    for k in G.KEYS:
+        assert _relerr(g[k], g_ref[k]) < 1e-5, k

@@ -78,14 +78,19 @@ def test_mixed_energy_only_matches_energy_vjp(precision):
     assert abs(e - e_vjp) <= 1e-12 * abs(e_vjp)
 
 
-def test_mixed_adjoint_seed_scales_gradients():
+@pytest.mark.parametrize("ybar,tol", [(-2.0, 1e-12), (-2.5, 1e-6)])
+def test_mixed_adjoint_seed_scales_gradients(ybar, tol):
+    """A power-of-two seed only shifts the per-chunk power-of-two scale of the
+    split adjoint, so the gradients scale exactly (up to FP64 summation order);
+    any other seed changes the fp16 rounding of the split and agrees to the
+    mixed-precision level."""
     inp = make_inputs(7, 29, 60, seed=32, fvo_sigma=1e-3)
     args = (inp.mo_energy, inp.t1, inp.t2, inp.ovoo, inp.ovov, inp.ovvv_tril(), inp.fvo)
     _, g1 = triples.energy_vjp(*args, ybar=1.0, precision="mixed", device="cuda")
-    _, g3 = triples.energy_vjp(*args, ybar=-2.5, precision="mixed", device="cuda")
+    _, g3 = triples.energy_vjp(*args, ybar=ybar, precision="mixed", device="cuda")
     for k in G.KEYS:
-        a, b = g3[k].cpu().numpy(), -2.5 * g1[k].cpu().numpy()
-        assert _relerr(a, b) < 1e-9, k
+        a, b = g3[k].cpu().numpy(), ybar * g1[k].cpu().numpy()
+        assert _relerr(a, b) < tol, k
 
 
 @pytest.mark.parametrize("o,v", [(1, 1), (2, 17), (3, 31), (13, 9)])

@@ -87,6 +87,38 @@ int triples_energy_vjp(void *stream, int precision, int nocc, int nvir, int ovvv
                        double *ovoo_bar, double *ovov_bar, double *ovvv_bar,
                        double *fvo_bar);
 
+/* LNO (T): the triples energy of a local-natural-orbital fragment, in which
+ * the first occupied index of the projected amplitude runs through the
+ * projector mat[o,o] (pyscfad/lno/ccsd_t.py:42, mat = ulo^T ulo):
+ *   E = (1/3) sum_{ijk,abc} (sum_l mat[l,i] W[l,j,k]) Z[i,j,k] / D[i,j,k]
+ * in the index convention of triples_energy (mat = identity gives E(T)).
+ * Only precision TRIPLES_PRECISION_FP64 and nocc <= 64 are supported
+ * (TRIPLES_ERR_UNSUPPORTED otherwise).  Other arguments, layouts and
+ * workspace rules are those of triples_energy / triples_energy_vjp;
+ * triples_lno_workspace_size sizes the workspace of these two calls.
+ * Replaces lnoccsdt_contract (pyscfadlib/pyscfadlib/vjp/cc/lno_ccsd_t.c:96)
+ * with the 2/3 of pyscfad/lno/ccsd_t.py:111, and lnoccsdt_energy_vjp
+ * (pyscfadlib/pyscfadlib/vjp/cc/lno_ccsd_t_vjp.c:400) with the host-side
+ * preparation and fold of _ccsd_t_energy_bwd (pyscfad/lno/ccsd_t.py:121-235).
+ * mat_bar[o,o] is the cotangent of mat (overwritten, like every gradient). */
+size_t triples_lno_workspace_size(int precision, int nocc, int nvir, int ovvv_packed, int want_grad);
+
+int triples_lno_energy(void *stream, int precision, int nocc, int nvir, int ovvv_packed,
+                       const double *mat, const double *mo_energy, const double *t1,
+                       const double *t2, const double *ovoo, const double *ovov,
+                       const double *ovvv, const double *fvo,
+                       void *workspace, size_t workspace_bytes, double *e_out);
+
+int triples_lno_energy_vjp(void *stream, int precision, int nocc, int nvir, int ovvv_packed,
+                           const double *mat, const double *mo_energy, const double *t1,
+                           const double *t2, const double *ovoo, const double *ovov,
+                           const double *ovvv, const double *fvo, double ybar,
+                           void *workspace, size_t workspace_bytes,
+                           double *e_out, double *mat_bar,
+                           double *mo_energy_bar, double *t1_bar, double *t2_bar,
+                           double *ovoo_bar, double *ovov_bar, double *ovvv_bar,
+                           double *fvo_bar);
+
 /* Size of the fixed device scratch behind triples_energy_vjp_static. */
 #define TRIPLES_STATIC_SCRATCH_BYTES ((size_t)64 << 20)
 

@@ -177,6 +177,61 @@ def ref_energy_vjp(inp, ybar=1.0):
     return e, g
 
 
+def ref_lno_energy(inp, mat, a0=0, a1=None):
+    """lnoccsdt_contract with a projector mat[o,o] on the first occupied index,
+    times 2/3 (pyscfad/lno/ccsd_t.py:76-113, lno_ccsd_t.c:96-138)."""
+    lib = _lib("ref")
+    o, v = inp.nocc, inp.nvir
+    a1 = v if a1 is None else a1
+    t1T, t2T, vooo, vvop = _ref_layouts(inp)
+    mat = np.ascontiguousarray(mat, dtype=np.float64)
+    mo_energy = np.ascontiguousarray(inp.mo_energy)
+    fvo = np.ascontiguousarray(inp.fvo)
+    et = np.zeros(1)
+    lib.lnoccsdt_contract(_ptr(et), _ptr(mat), _ptr(mo_energy), _ptr(t1T), _ptr(t2T),
+                          _ptr(vooo), _ptr(fvo), ctypes.c_int(o), ctypes.c_int(v),
+                          ctypes.c_int(a0), ctypes.c_int(a1), _ptr(vvop))
+    return float(et[0]) * 2.0 / 3.0
+
+
+def ref_lno_energy_vjp(inp, mat, ybar=1.0):
+    """E and gradients of the LNO (T) energy, from the reference's
+    lnoccsdt_energy_vjp (lno_ccsd_t_vjp.c:400-566) called as one block over all
+    jobs the way pyscfad/lno/ccsd_t.py:120-235 does for (a0, a1) = (0, nvir),
+    mapped to the independent reference-layout arrays (ovvv gradient unpacked)
+    plus mat."""
+    lib = _lib("ref")
+    o, v = inp.nocc, inp.nvir
+    n = o + v
+    e = ref_lno_energy(inp, mat)
+    t1T, t2T, vooo, vvop = _ref_layouts(inp)
+    mat = np.ascontiguousarray(mat, dtype=np.float64)
+    mo_energy = np.ascontiguousarray(inp.mo_energy)
+    fvo = np.ascontiguousarray(inp.fvo)
+    bars = dict(mat=np.zeros_like(mat), mo_energy=np.zeros(n), t1T=np.zeros_like(t1T),
+                t2T=np.zeros_like(t2T), vooo=np.zeros_like(vooo), fvo=np.zeros_like(fvo))
+    vvop_bar = np.zeros_like(vvop)
+    lib.lnoccsdt_energy_vjp(
+        _ptr(mat), _ptr(mo_energy), _ptr(t1T), _ptr(t2T), _ptr(vooo), _ptr(fvo),
+        ctypes.c_double(ybar * 2.0 / 3.0), ctypes.c_int(o), ctypes.c_int(v),
+        ctypes.c_int(0), ctypes.c_int(v), ctypes.c_int(0), ctypes.c_int(v),
+        _ptr(vvop), _ptr(vvop), _ptr(vvop), _ptr(vvop),
+        _ptr(bars["mat"]), _ptr(bars["mo_energy"]), _ptr(bars["t1T"]), _ptr(bars["t2T"]),
+        _ptr(bars["vooo"]), _ptr(bars["fvo"]),
+        _ptr(vvop_bar), _ptr(vvop_bar), _ptr(vvop_bar), _ptr(vvop_bar))
+    g = dict(
+        mat=bars["mat"],
+        mo_energy=bars["mo_energy"],
+        t1=np.ascontiguousarray(bars["t1T"].T),
+        t2=np.ascontiguousarray(bars["t2T"].transpose(3, 2, 0, 1)),
+        ovoo=np.ascontiguousarray(bars["vooo"].transpose(1, 0, 3, 2)),
+        ovov=np.ascontiguousarray(vvop_bar[:, :, :, :o].transpose(2, 0, 3, 1)),
+        ovvv=np.ascontiguousarray(vvop_bar[:, :, :, o:].transpose(2, 0, 3, 1)),
+        fvo=bars["fvo"],
+    )
+    return e, g
+
+
 def fold_ovvv_tril(ovvv_bar):
     """ccsd_t.py:184-191: symmetrise over the last two indices, halve the
     diagonal, pack the lower triangle -> [o,v,v(v+1)/2]."""
@@ -241,3 +296,76 @@ def np_energy(inp):
                 ZZ = r3(WW + 0.5 * VV) / d3
                 et += np.einsum('ijk,ijk', WW, ZZ)
     return 2.0 * et
+
+
+# --------------------------------------------------------------------------
+# NumPy restatement of the LNO (T) energy and its adjoint (tiny sizes only):
+# the energy of lnoccsdt_contract (pyscfadlib/pyscfadlib/vjp/cc/lno_ccsd_t.c:6-29,
+# job weights 73-94) times 2/3 (pyscfad/lno/ccsd_t.py:111), and the chain rule
+# of lnoccsdt_energy_vjp (lno_ccsd_t_vjp.c:9-122 and 145-297), written over the
+# full index range [p,q,r,x,y,z] instead of a >= b >= c jobs.
+# --------------------------------------------------------------------------
+_PERMS6 = ((0, 1, 2), (0, 2, 1), (1, 0, 2), (1, 2, 0), (2, 0, 1), (2, 1, 0))
+# r3 of pyscfad/cc/ccsd_t_slow.py:84-87 as (axis order, coefficient)
+_R3 = (((0, 1, 2), 4.0), ((1, 2, 0), 1.0), ((2, 0, 1), 1.0),
+       ((2, 1, 0), -2.0), ((0, 2, 1), -2.0), ((1, 0, 2), -2.0))
+
+
+def _sym6(a):
+    """sum over the six simultaneous permutations of (p,q,r) with (x,y,z)."""
+    return sum(a.transpose(*s, *(3 + np.array(s))) for s in _PERMS6)
+
+
+def _r3_virt(a, adjoint=False):
+    out = np.zeros_like(a)
+    for s, c in _R3:
+        axes = np.argsort(s) if adjoint else np.array(s)
+        out += c * a.transpose(0, 1, 2, *(3 + axes))
+    return out
+
+
+def np_lno_energy_vjp(inp, mat, ybar=1.0, want_grad=True):
+    """(E, grads) of the LNO (T) energy with projector mat[o,o] on the first
+    occupied index; grads in the layouts of ``ref_lno_energy_vjp`` (ovvv
+    unpacked) plus "mat".  mat = identity gives the canonical E(T)."""
+    o, v = inp.nocc, inp.nvir
+    w = (np.einsum('pxfy,rqzf->pqrxyz', inp.ovvv, inp.t2)
+         - np.einsum('pxmq,rmzy->pqrxyz', inp.ovoo, inp.t2))
+    vv = (np.einsum('pxqy,rz->pqrxyz', inp.ovov, inp.t1)
+          + np.einsum('qpyx,zr->pqrxyz', inp.t2, inp.fvo))
+    WW, VV = _sym6(w), _sym6(vv)
+    Z = _r3_virt(WW + 0.5 * VV)
+    eo, ev = inp.mo_energy[:o], inp.mo_energy[o:]
+    D = (eo[:, None, None, None, None, None] + eo[None, :, None, None, None, None]
+         + eo[None, None, :, None, None, None] - ev[None, None, None, :, None, None]
+         - ev[None, None, None, None, :, None] - ev[None, None, None, None, None, :])
+    Q = Z / D
+    Wt = np.einsum('li,ljkxyz->ijkxyz', mat, WW)
+    e = float(np.einsum('ijkxyz,ijkxyz->', Wt, Q)) / 3.0
+    if not want_grad:
+        return e, None
+    Qbar = ybar / 3.0 * Wt
+    Wtbar = ybar / 3.0 * Q
+    g = {"mat": np.einsum('ljkxyz,ijkxyz->li', WW, Wtbar)}
+    Zbar = Qbar / D
+    Dbar = -Qbar * Q / D
+    Xbar = _r3_virt(Zbar, adjoint=True)
+    wbar = _sym6(np.einsum('li,ijkxyz->ljkxyz', mat, Wtbar) + Xbar)
+    vbar = _sym6(0.5 * Xbar)
+    mob = np.zeros(o + v)
+    for ax in range(6):
+        part = Dbar.sum(axis=tuple(a for a in range(6) if a != ax))
+        if ax < 3:
+            mob[:o] += part
+        else:
+            mob[o:] -= part
+    g["mo_energy"] = mob
+    g["t1"] = np.einsum('pqrxyz,pxqy->rz', vbar, inp.ovov)
+    g["fvo"] = np.einsum('pqrxyz,qpyx->zr', vbar, inp.t2)
+    g["ovov"] = np.einsum('pqrxyz,rz->pxqy', vbar, inp.t1)
+    g["t2"] = (np.einsum('pqrxyz,zr->qpyx', vbar, inp.fvo)
+               + np.einsum('pqrxyz,pxfy->rqzf', wbar, inp.ovvv)
+               - np.einsum('pqrxyz,pxmq->rmzy', wbar, inp.ovoo))
+    g["ovvv"] = np.einsum('pqrxyz,rqzf->pxfy', wbar, inp.t2)
+    g["ovoo"] = -np.einsum('pqrxyz,rmzy->pxmq', wbar, inp.t2)
+    return e, g

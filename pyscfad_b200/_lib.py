@@ -47,6 +47,13 @@ def load():
     lib.triples_energy_vjp.restype = _c_int
     lib.triples_energy_vjp.argtypes = ([_vp, _c_int, _c_int, _c_int, _c_int] + [_vp] * 7 +
                                        [_c_double, _vp, _c_size, _vp] + [_vp] * 7)
+    lib.triples_lno_workspace_size.restype = _c_size
+    lib.triples_lno_workspace_size.argtypes = [_c_int] * 5
+    lib.triples_lno_energy.restype = _c_int
+    lib.triples_lno_energy.argtypes = [_vp, _c_int, _c_int, _c_int, _c_int] + [_vp] * 8 + [_vp, _c_size, _vp]
+    lib.triples_lno_energy_vjp.restype = _c_int
+    lib.triples_lno_energy_vjp.argtypes = ([_vp, _c_int, _c_int, _c_int, _c_int] + [_vp] * 8 +
+                                           [_c_double, _vp, _c_size, _vp] + [_vp] * 8)
     lib.triples_status_string.restype = ctypes.c_char_p
     lib.triples_status_string.argtypes = [_c_int]
     lib.triples_last_cuda_error.restype = _c_int

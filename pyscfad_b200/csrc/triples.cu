@@ -16,6 +16,7 @@
 #include "tc_f1.cuh"
 #include "f2.cuh"
 #include "tc_b1.cuh"
+#include "lno.cuh"
 #include "pyscfad_b200.h"
 #include "triples_internal.h"
 
@@ -41,10 +42,10 @@ static int g_kseg_f1 = 1;  // same for the W contraction
 // ---------------------------------------------------------------------------
 // optional per-kernel-class timing with CUDA events (on the launch stream)
 // ---------------------------------------------------------------------------
-enum ProfCat { P_PREP = 0, P_F1, P_F2, P_B1A, P_B1B, P_B1C, P_B1D, P_FOLD, P_NCAT };
-static const char *kProfNames[P_NCAT] = {"prep", "f1_contract", "f2_epilogue", 
+enum ProfCat { P_PREP = 0, P_F1, P_F2, P_B1A, P_B1B, P_B1C, P_B1D, P_FOLD, P_LNO, P_NCAT };
+static const char *kProfNames[P_NCAT] = {"prep", "f1_contract", "f2_epilogue",
                                          "b1a_ovvv_grad", "b1b_t2_grad", "b1c_ovoo_grad",
-                                         "b1d_t2_ooov_grad", "fold"};
+                                         "b1d_t2_ooov_grad", "fold", "lno_epilogue"};
 struct ProfRec {
     int cat;
     cudaEvent_t a, b;
@@ -143,11 +144,13 @@ static long long chunk_stage_elems(const ChunkDesc &ch, const Dims &d) {
     return s;
 }
 
-int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan &P) {
+int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan &P, int lno) {
     if (nocc < 1 || nvir < 1 || nocc > kMaxCols || nvir > 32767) return TRIPLES_ERR_INVALID_ARGUMENT;
     if (precision < TRIPLES_PRECISION_FP64 || precision > TRIPLES_PRECISION_MIXED_BF16)
         return TRIPLES_ERR_INVALID_ARGUMENT;
+    if (lno && (precision != TRIPLES_PRECISION_FP64 || nocc > kLnoMaxO)) return TRIPLES_ERR_UNSUPPORTED;
     P = Plan{};
+    P.lno = lno ? 1 : 0;
     P.prec = precision;
     P.want_grad = want_grad ? 1 : 0;
     P.packed = packed ? 1 : 0;
@@ -213,6 +216,11 @@ int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan
     }
     P.off_ijk = take((size_t)P.n_ijk * 3 * sizeof(int));
     P.off_epart = take((size_t)P.n_ijk * P.f2_gy * el);
+    if (P.lno) {
+        // WW / Wbar-of-WW, X / VVbar, Q, Wt / Zbar: whole-chunk FP64 arrays
+        for (int k = 0; k < 4; k++) P.off_L[k] = take(P.stage_elems * el);
+        P.off_lpart = take((size_t)6 * kLnoGrid * el);
+    }
     P.total = off;
     return TRIPLES_OK;
 }
@@ -806,6 +814,54 @@ static int num_sms() {
     return n;
 }
 
+// LNO chunk epilogue (FP64): energy of the projected amplitudes and, with
+// want_grad, mat_bar, the D and V-term gradients and the FP64 Wbar staging
+// that the adjoint contractions read next.
+static int lno_chunk(const Plan &P, const ChunkDesc &ch, cudaStream_t st, const TriplesIO &io, char *ws,
+                     Ctrl *ctrl, const double *S, double *SW) {
+    LnoArgs A;
+    A.d = P.d;
+    A.ch = ch;
+    for (int k = 0; k < 27; k++) A.tau_of[k] = 0;
+    for (int sx = 0; sx < 3; sx++)
+        for (int sy = 0; sy < 3; sy++)
+            for (int sz = 0; sz < 3; sz++)
+                for (int t = 0; t < ch.nperm; t++)
+                    if (ch.pb[t].bx == ch.blk[sx] && ch.pb[t].by == ch.blk[sy] && ch.pb[t].bz == ch.blk[sz])
+                        A.tau_of[(sx * 3 + sy) * 3 + sz] = (signed char)t;
+    A.S = S;
+    A.B0 = (double *)(ws + P.off_L[0]);
+    A.B1 = (double *)(ws + P.off_L[1]);
+    A.B2 = (double *)(ws + P.off_L[2]);
+    A.B3 = (double *)(ws + P.off_L[3]);
+    A.mat = io.mat; A.mo_e = io.mo_energy; A.t1 = io.t1; A.t2 = io.t2; A.ovov = io.ovov; A.fvo = io.fvo;
+    A.SW = SW;
+    A.mat_bar = io.mat_bar; A.mo_bar = io.mo_energy_bar; A.t1_bar = io.t1_bar; A.t2_bar = io.t2_bar;
+    A.ovov_bar = io.ovov_bar; A.fvo_bar = io.fvo_bar;
+    A.ybar = io.ybar;
+    A.part = (double *)(ws + P.off_lpart);
+    long long maxpos = 0;
+    for (int t = 0; t < ch.nperm; t++) {
+        const long long np = (long long)P.d.o * P.d.o * P.d.o * ch.pb[t].Tx * ch.pb[t].Ty * ch.pb[t].Tz;
+        if (np > maxpos) maxpos = np;
+    }
+    long long gx = (maxpos + kLnoThreads - 1) / kLnoThreads;
+    if (gx > kLnoGrid) gx = kLnoGrid;
+    const dim3 grid((unsigned)gx, (unsigned)ch.nperm);
+    TB_KLAUNCH(P_LNO, k_lno_ww<<<grid, kLnoThreads, 0, st>>>(A));
+    TB_KLAUNCH(P_LNO, k_lno_q<<<grid, kLnoThreads, 0, st>>>(A));
+    TB_KLAUNCH(P_LNO, k_lno_project<<<grid, kLnoThreads, 0, st>>>(A, A.B0, A.B3, 1, 1.0));
+    TB_KLAUNCH(P_LNO, k_lno_energy<<<grid, kLnoThreads, 0, st>>>(A));
+    TB_KLAUNCH(P_LNO, k_f2_energy_sum<<<1, 256, 0, st>>>(A.part, (int)gx * ch.nperm, &ctrl->e_acc));
+    if (!P.want_grad) return TRIPLES_OK;
+    TB_KLAUNCH(P_LNO, k_lno_matbar<<<grid, kLnoThreads, 0, st>>>(A));
+    TB_KLAUNCH(P_LNO, k_lno_zbar<<<grid, kLnoThreads, 0, st>>>(A));
+    TB_KLAUNCH(P_LNO, k_lno_project<<<grid, kLnoThreads, 0, st>>>(A, A.B2, A.B0, 0, io.ybar / 3.0));
+    TB_KLAUNCH(P_LNO, k_lno_xbar<<<grid, kLnoThreads, 0, st>>>(A));
+    TB_KLAUNCH(P_LNO, k_lno_scatter<<<grid, kLnoThreads, 0, st>>>(A));
+    return TRIPLES_OK;
+}
+
 template <typename StageT>
 static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
     constexpr int kSB = sizeof(StageT) == 4 ? 8 : 4;   // epilogue sub-block edge
@@ -857,6 +913,7 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
         TB_CUDA(cudaMemsetAsync(io.t2_bar, 0, o * o * v * v * sizeof(double), st));
         TB_CUDA(cudaMemsetAsync(io.ovov_bar, 0, o * v * o * v * sizeof(double), st));
         TB_CUDA(cudaMemsetAsync(io.fvo_bar, 0, v * o * sizeof(double), st));
+        if (P.lno) TB_CUDA(cudaMemsetAsync(io.mat_bar, 0, o * o * sizeof(double), st));
     }
 
     // FP64 operand layouts (used by the FP64 contractions only)
@@ -1003,8 +1060,12 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                                      L.cum[ch.nperm]),
                                 256, 0, st>>>(L));
                 }
-                // F2: energy (+ adjoint of the raw amplitudes)
-                {
+                if (P.lno) {
+                    // projected energy: whole-chunk epilogue instead of the orbit tiles
+                    const int rc = lno_chunk(P, ch, st, io, ws, ctrl, (const double *)S, (double *)SW);
+                    if (rc != TRIPLES_OK) return rc;
+                } else {
+                    // F2: energy (+ adjoint of the raw amplitudes)
                     F2P<StageT> F;
                     F.d = d;
                     F.ch = ch;
@@ -1251,6 +1312,54 @@ int triples_energy_vjp(void *stream, int precision, int nocc, int nvir, int ovvv
     io.mo_energy_bar = mo_energy_bar; io.t1_bar = t1_bar; io.t2_bar = t2_bar; io.ovoo_bar = ovoo_bar;
     io.ovov_bar = ovov_bar; io.ovvv_bar = ovvv_bar; io.fvo_bar = fvo_bar;
     return triples_call(stream, precision, nocc, nvir, ovvv_packed, 1, io, workspace_bytes);
+}
+
+// ---- LNO (projected) energy ----
+size_t triples_lno_workspace_size(int precision, int nocc, int nvir, int ovvv_packed, int want_grad) {
+    tb::Plan P;
+    if (tb::make_plan(precision, nocc, nvir, ovvv_packed, want_grad, P, 1) != TRIPLES_OK) return 0;
+    return P.total;
+}
+
+static int triples_lno_call(void *stream, int precision, int nocc, int nvir, int ovvv_packed, int want_grad,
+                            const tb::TriplesIO &io, size_t workspace_bytes) {
+    tb::Plan P;
+    int rc = tb::make_plan(precision, nocc, nvir, ovvv_packed, want_grad, P, 1);
+    if (rc != TRIPLES_OK) return rc;
+    if (!io.workspace || workspace_bytes < P.total) return TRIPLES_ERR_WORKSPACE;
+    if (!io.mat || !io.mo_energy || !io.t1 || !io.t2 || !io.ovoo || !io.ovov || !io.ovvv || !io.fvo || !io.e_out)
+        return TRIPLES_ERR_INVALID_ARGUMENT;
+    if (want_grad && (!io.mat_bar || !io.mo_energy_bar || !io.t1_bar || !io.t2_bar || !io.ovoo_bar ||
+                      !io.ovov_bar || !io.ovvv_bar || !io.fvo_bar))
+        return TRIPLES_ERR_INVALID_ARGUMENT;
+    return tb::run_triples(P, (cudaStream_t)stream, io);
+}
+
+int triples_lno_energy(void *stream, int precision, int nocc, int nvir, int ovvv_packed, const double *mat,
+                       const double *mo_energy, const double *t1, const double *t2, const double *ovoo,
+                       const double *ovov, const double *ovvv, const double *fvo, void *workspace,
+                       size_t workspace_bytes, double *e_out) {
+    tb::TriplesIO io{};
+    io.mat = mat;
+    io.mo_energy = mo_energy; io.t1 = t1; io.t2 = t2; io.ovoo = ovoo; io.ovov = ovov;
+    io.ovvv = ovvv; io.fvo = fvo; io.ybar = 1.0; io.workspace = workspace; io.e_out = e_out;
+    return triples_lno_call(stream, precision, nocc, nvir, ovvv_packed, 0, io, workspace_bytes);
+}
+
+int triples_lno_energy_vjp(void *stream, int precision, int nocc, int nvir, int ovvv_packed, const double *mat,
+                           const double *mo_energy, const double *t1, const double *t2, const double *ovoo,
+                           const double *ovov, const double *ovvv, const double *fvo, double ybar,
+                           void *workspace, size_t workspace_bytes, double *e_out, double *mat_bar,
+                           double *mo_energy_bar, double *t1_bar, double *t2_bar, double *ovoo_bar,
+                           double *ovov_bar, double *ovvv_bar, double *fvo_bar) {
+    tb::TriplesIO io{};
+    io.mat = mat;
+    io.mo_energy = mo_energy; io.t1 = t1; io.t2 = t2; io.ovoo = ovoo; io.ovov = ovov;
+    io.ovvv = ovvv; io.fvo = fvo; io.ybar = ybar; io.workspace = workspace; io.e_out = e_out;
+    io.mat_bar = mat_bar;
+    io.mo_energy_bar = mo_energy_bar; io.t1_bar = t1_bar; io.t2_bar = t2_bar; io.ovoo_bar = ovoo_bar;
+    io.ovov_bar = ovov_bar; io.ovvv_bar = ovvv_bar; io.fvo_bar = fvo_bar;
+    return triples_lno_call(stream, precision, nocc, nvir, ovvv_packed, 1, io, workspace_bytes);
 }
 
 // Fixed scratch for callers that may not allocate device memory themselves

@@ -11,6 +11,7 @@ constexpr int kF2Threads = 256;   // chunk-epilogue block size
 constexpr int kMaxTv = 16;        // largest virtual block
 constexpr int kMaxCols = 1024;    // largest nocc * Tv (one staged (r, z) row)
 constexpr int kCtrlBytes = 256;   // control block at workspace offset 0
+constexpr int kLnoGrid = 1184;    // LNO kernels: blocks per ordering (8 per SM)
 
 // Control block (workspace offset 0)
 struct Ctrl {
@@ -29,6 +30,7 @@ static_assert(sizeof(Ctrl) <= kCtrlBytes, "control block too large");
 struct Plan {
     Dims d;
     int prec, want_grad, packed;
+    int lno;         // projected (LNO) energy: FP64 only, chunk work arrays off_L
     int nb;          // number of virtual blocks
     int n_ijk;       // occupied triplet representatives i >= j >= k
     int max_items;   // largest |A||B||C| over chunks
@@ -40,18 +42,21 @@ struct Plan {
     size_t off_A1h, off_B1h, off_A2h, off_B2h;
     size_t off_GA1, off_GB1, off_GA2, off_GB2;
     size_t off_ijk, off_epart;
+    size_t off_L[4], off_lpart;
     size_t total;
 };
 
 struct TriplesIO {
     const double *mo_energy, *t1, *t2, *ovoo, *ovov, *ovvv, *fvo;
+    const double *mat;             // LNO projector [o,o] (lno plans only)
     double ybar;
     void *workspace;
     double *e_out;
     double *mo_energy_bar, *t1_bar, *t2_bar, *ovoo_bar, *ovov_bar, *ovvv_bar, *fvo_bar;
+    double *mat_bar;
 };
 
-int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan &P);
+int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan &P, int lno = 0);
 int run_triples(const Plan &P, cudaStream_t st, const TriplesIO &io);
 
 }  // namespace tb

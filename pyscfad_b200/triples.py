@@ -145,6 +145,70 @@ def energy_vjp(mo_energy, t1, t2, ovoo, ovov, ovvv, fvo, ybar=1.0, precision="fp
     return e, grads
 
 
+def _check_mat(mat, o):
+    if tuple(mat.shape) != (o, o):
+        raise ValueError(f"mat has shape {tuple(mat.shape)}, expected {(o, o)}")
+
+
+def lno_workspace_size(nocc, nvir, packed=True, want_grad=True, precision="fp64") -> int:
+    return int(_lib.load().triples_lno_workspace_size(_lib.PRECISION[precision], nocc, nvir,
+                                                      int(packed), int(want_grad)))
+
+
+def lno_energy(mat, mo_energy, t1, t2, ovoo, ovov, ovvv, fvo, precision="fp64", device=None,
+               stream=None, check=True) -> torch.Tensor:
+    """LNO (T) energy with the occupied projector mat[o,o] (= ulo^T ulo,
+    pyscfad/lno/ccsd_t.py:42); mat = identity gives E(T).  FP64 only."""
+    lib = _lib.load()
+    device = torch.device(device or (t1.device if isinstance(t1, torch.Tensor) and t1.is_cuda else "cuda"))
+    args = [_as_dev(a, device) for a in (mat, mo_energy, t1, t2, ovoo, ovov, ovvv, fvo)]
+    mat, mo_energy, t1, t2, ovoo, ovov, ovvv, fvo = args
+    o, v, packed = _shapes(t1, t2, ovoo, ovov, ovvv, fvo, mo_energy)
+    _check_mat(mat, o)
+    prec = _lib.PRECISION[precision]
+    nbytes = lib.triples_lno_workspace_size(prec, o, v, int(packed), 0)
+    if nbytes == 0:
+        raise _lib.TriplesError(4 if prec != 0 or o > 64 else 1, "triples_lno_workspace_size")
+    ws = _workspace(nbytes, device)
+    e = torch.zeros((), dtype=torch.float64, device=device)
+    st = stream if stream is not None else torch.cuda.current_stream(device)
+    rc = lib.triples_lno_energy(st.cuda_stream, prec, o, v, int(packed),
+                                *[a.data_ptr() for a in args], ws.data_ptr(), ws.numel(), e.data_ptr())
+    _lib.check(rc, "triples_lno_energy")
+    if check:
+        _lib.check(lib.triples_check_device_status(st.cuda_stream, ws.data_ptr()), "triples_lno_energy (device)")
+    return e
+
+
+def lno_energy_vjp(mat, mo_energy, t1, t2, ovoo, ovov, ovvv, fvo, ybar=1.0, precision="fp64",
+                   device=None, stream=None, check=True):
+    """LNO (T) energy and its VJP; the dict holds "mat" next to the seven
+    keys of energy_vjp, each in its input's layout.  Returns (e, dict)."""
+    lib = _lib.load()
+    device = torch.device(device or (t1.device if isinstance(t1, torch.Tensor) and t1.is_cuda else "cuda"))
+    args = [_as_dev(a, device) for a in (mat, mo_energy, t1, t2, ovoo, ovov, ovvv, fvo)]
+    mat, mo_energy, t1, t2, ovoo, ovov, ovvv, fvo = args
+    o, v, packed = _shapes(t1, t2, ovoo, ovov, ovvv, fvo, mo_energy)
+    _check_mat(mat, o)
+    prec = _lib.PRECISION[precision]
+    nbytes = lib.triples_lno_workspace_size(prec, o, v, int(packed), 1)
+    if nbytes == 0:
+        raise _lib.TriplesError(4 if prec != 0 or o > 64 else 1, "triples_lno_workspace_size")
+    ws = _workspace(nbytes, device)
+    e = torch.zeros((), dtype=torch.float64, device=device)
+    keys = ("mat",) + KEYS
+    grads = {k: torch.empty_like(a) for k, a in zip(keys, args)}
+    st = stream if stream is not None else torch.cuda.current_stream(device)
+    rc = lib.triples_lno_energy_vjp(st.cuda_stream, prec, o, v, int(packed),
+                                    *[a.data_ptr() for a in args], float(ybar), ws.data_ptr(), ws.numel(),
+                                    e.data_ptr(), *[grads[k].data_ptr() for k in keys])
+    _lib.check(rc, "triples_lno_energy_vjp")
+    if check:
+        _lib.check(lib.triples_check_device_status(st.cuda_stream, ws.data_ptr()),
+                   "triples_lno_energy_vjp (device)")
+    return e, grads
+
+
 def device_status(device=None, stream=None) -> int:
     """Synchronise and return the device-side status of the last call."""
     device = torch.device(device or "cuda")

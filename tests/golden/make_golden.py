@@ -8,7 +8,12 @@ layouts), E(T), the gradients w.r.t. every input as an independent tensor
 (ovvv unpacked), and the reference's packed-tril ovvv cotangent
 (pyscfad/cc/ccsd_t.py:184-191).
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          # all fixtures
+    python tests/golden/make_golden.py --lno    # the LNO fixtures only
+
+The LNO fixtures hold, in addition, the projector mat and its cotangent,
+from the reference's lnoccsdt_contract / lnoccsdt_energy_vjp
+(pyscfadlib/pyscfadlib/vjp/cc/lno_ccsd_t.c, lno_ccsd_t_vjp.c).
 """
 from __future__ import annotations
 
@@ -37,6 +42,39 @@ CASES = {
 }
 
 
+# LNO fragment cases, name: (nocc, nvir, naux, seed, nlo); the projector is
+# mat = ulo^T ulo for a seeded ulo[nlo, nocc] (pyscfad/lno/ccsd_t.py:42)
+LNO_CASES = {
+    "lno_o3v5": (3, 5, 20, 11, 1),
+    "lno_o4v9": (4, 9, 30, 12, 2),
+    "lno_o5v19": (5, 19, 60, 13, 2),   # three virtual blocks (16, 2, 1): ragged chunks
+    "lno_o6v2": (6, 2, 10, 14, 3),     # nvir < nocc
+}
+
+
+def lno_projector(nocc, nlo, seed):
+    rng = np.random.default_rng(1000 + seed)
+    ulo = np.linalg.qr(rng.normal(size=(nocc, nocc)))[0][:nlo]
+    return ulo.T @ ulo
+
+
+def main_lno():
+    for name, (o, v, naux, seed, nlo) in LNO_CASES.items():
+        inp = make_inputs(o, v, naux, seed=seed, fvo_sigma=1e-3)
+        mat = lno_projector(o, nlo, seed)
+        e, g = O.ref_lno_energy_vjp(inp, mat, ybar=1.0)
+        cot = O.reference_cotangents(g, o, v)
+        out = dict(nocc=o, nvir=v, naux=naux, seed=seed, nlo=nlo, e=e, in_mat=mat, grad_mat=g["mat"])
+        for k in O.GRAD_KEYS:
+            out["in_" + k] = getattr(inp, k)
+            out["grad_" + k] = g[k]
+        out["cot_ovvv_tril"] = cot["ovvv"]
+        out["in_ovvv_tril"] = inp.ovvv_tril()
+        path = os.path.join(HERE, f"{name}.npz")
+        np.savez_compressed(path, **out)
+        print(f"{name}: E = {e:.15g}  -> {os.path.relpath(path, ROOT)}")
+
+
 def main():
     if not O.ref_available():
         O.build()
@@ -57,4 +95,8 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if "--lno" in sys.argv:
+        main_lno()
+    else:
+        main()
+        main_lno()

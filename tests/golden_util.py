@@ -8,14 +8,27 @@ from pyscfad_b200.synthetic import TriplesInputs
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 KEYS = ("mo_energy", "t1", "t2", "ovoo", "ovov", "ovvv", "fvo")
+LNO_PREFIX = "lno_"
+
+
+def _all():
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
 
 
 def names():
-    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
+    """Canonical (T) fixtures."""
+    return [n for n in _all() if not n.startswith(LNO_PREFIX)]
+
+
+def lno_names():
+    """LNO fragment (T) fixtures (projector mat on the first occupied index)."""
+    return [n for n in _all() if n.startswith(LNO_PREFIX)]
 
 
 def load(name):
     z = np.load(os.path.join(GOLDEN, name + ".npz"))
     inp = TriplesInputs(*[np.ascontiguousarray(z["in_" + k]) for k in KEYS])
     grads = {k: z["grad_" + k] for k in KEYS}
+    if name.startswith(LNO_PREFIX):
+        grads["mat"] = z["grad_mat"]
     return inp, float(z["e"]), grads, z

@@ -26,6 +26,7 @@ def test_library_exports_every_declared_symbol():
     lib = _lib.load()
     decl = _declared_functions()
     assert "triples_energy_vjp" in decl and "triples_energy" in decl
+    assert "triples_lno_energy_vjp" in decl and "triples_lno_workspace_size" in decl
     for name in decl:
         assert hasattr(lib, name), name
 
@@ -59,3 +60,23 @@ def test_status_strings():
     assert b"workspace" in lib.triples_status_string(2)
     with pytest.raises(_lib.TriplesError):
         _lib.check(1, "probe")
+
+
+def test_lno_plan_limits():
+    """The LNO path is FP64 with nocc <= 64; other requests are refused on the host."""
+    lib = _lib.load()
+    a = lib.triples_lno_workspace_size(0, 5, 19, 1, 0)
+    b = lib.triples_lno_workspace_size(0, 5, 19, 1, 1)
+    assert 0 < a < b
+    assert b > lib.triples_workspace_size(0, 5, 19, 1, 1)        # whole-chunk work arrays
+    assert lib.triples_lno_workspace_size(1, 5, 19, 1, 1) == 0   # mixed precision
+    assert lib.triples_lno_workspace_size(0, 65, 19, 1, 1) == 0  # nocc > 64
+    null = None
+    rc = lib.triples_lno_energy(null, 1, 5, 19, 1, *([null] * 8), null, 0, null)
+    assert rc == 4   # TRIPLES_ERR_UNSUPPORTED
+    rc = lib.triples_lno_energy(null, 0, 5, 19, 1, *([ctypes.c_void_p(16)] * 8), ctypes.c_void_p(16), 8,
+                                ctypes.c_void_p(16))
+    assert rc == 2   # workspace too small
+    rc = lib.triples_lno_energy(null, 0, 5, 19, 1, null, *([ctypes.c_void_p(16)] * 7), ctypes.c_void_p(16),
+                                1 << 40, ctypes.c_void_p(16))
+    assert rc == 1   # mat missing

@@ -80,3 +80,49 @@ def test_oracle_gradient_central_differences():
             fd = (ep - em) / (2 * h)
             an = g[k].reshape(-1)[idx]
             assert abs(fd - an) <= 1e-6 * max(abs(an), np.abs(g[k]).max() * 1e-3), (k, idx, fd, an)
+
+
+# ---- LNO fragment (T): projector mat on the first occupied index ----
+_LNO_KEYS = ("mat",) + G.KEYS
+
+
+@pytest.mark.parametrize("name", G.lno_names())
+def test_lno_numpy_restatement_matches_reference_golden(name):
+    inp, e_ref, g_ref, z = G.load(name)
+    e, g = O.np_lno_energy_vjp(inp, z["in_mat"], ybar=1.0)
+    assert abs(e - e_ref) <= 1e-12 * max(1e-3, abs(e_ref))
+    for k in _LNO_KEYS:
+        assert _relerr(g[k], g_ref[k]) < 1e-11, k
+    assert np.allclose(O.fold_ovvv_tril(g_ref["ovvv"]), z["cot_ovvv_tril"], rtol=0, atol=1e-15)
+
+
+def test_lno_identity_projector_is_canonical():
+    inp, e_ref, g_ref, _ = G.load("o4v9_fvo")
+    e, g = O.np_lno_energy_vjp(inp, np.eye(inp.nocc), ybar=1.0)
+    assert abs(e - e_ref) <= 1e-12 * abs(e_ref)
+    for k in G.KEYS:
+        assert _relerr(g[k], g_ref[k]) < 1e-11, k
+
+
+def test_lno_reference_library_reproduces_golden():
+    if not O.ref_available():
+        pytest.skip("reference library not built on this machine")
+    inp, e_ref, g_ref, z = G.load("lno_o4v9")
+    e, g = O.ref_lno_energy_vjp(inp, z["in_mat"], ybar=1.0)
+    assert abs(e - e_ref) < 1e-15
+    for k in _LNO_KEYS:
+        assert _relerr(g[k], g_ref[k]) < 1e-13, k
+
+
+def test_lno_projector_gradient_central_differences():
+    """dE/dmat by central differences (E is linear in mat: exact up to rounding)."""
+    inp, _, g_ref, z = G.load("lno_o3v5")
+    mat = z["in_mat"].copy()
+    for (l, i) in [(0, 0), (1, 2), (2, 1)]:
+        h = 1e-3
+        mat[l, i] += h
+        ep, _ = O.np_lno_energy_vjp(inp, mat, want_grad=False)
+        mat[l, i] -= 2 * h
+        em, _ = O.np_lno_energy_vjp(inp, mat, want_grad=False)
+        mat[l, i] += h
+        assert abs((ep - em) / (2 * h) - g_ref["mat"][l, i]) < 1e-12 * max(1.0, abs(g_ref["mat"][l, i]))

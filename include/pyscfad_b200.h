@@ -92,8 +92,10 @@ int triples_energy_vjp(void *stream, int precision, int nocc, int nvir, int ovvv
  * projector mat[o,o] (pyscfad/lno/ccsd_t.py:42, mat = ulo^T ulo):
  *   E = (1/3) sum_{ijk,abc} (sum_l mat[l,i] W[l,j,k]) Z[i,j,k] / D[i,j,k]
  * in the index convention of triples_energy (mat = identity gives E(T)).
- * Only precision TRIPLES_PRECISION_FP64 and nocc <= 64 are supported
- * (TRIPLES_ERR_UNSUPPORTED otherwise).  Other arguments, layouts and
+ * nocc <= 64 (TRIPLES_ERR_UNSUPPORTED otherwise); every precision: the
+ * mixed ones run the W contraction and the adjoint contractions on the tensor
+ * cores as triples_energy does and the projected epilogue in FP64.  Other
+ * arguments, layouts and
  * workspace rules are those of triples_energy / triples_energy_vjp;
  * triples_lno_workspace_size sizes the workspace of these two calls.
  * Replaces lnoccsdt_contract (pyscfadlib/pyscfadlib/vjp/cc/lno_ccsd_t.c:96)

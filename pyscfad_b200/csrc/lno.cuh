@@ -10,38 +10,67 @@
 //   Zbar = Qbar / D,   Dbar = -Qbar Q / D,   Xbar = r3^T(Zbar),
 //   WWbar = P^T(Wtbar) + Xbar,   VVbar = Xbar / 2,
 //   wbar = sum_sigma WWbar(sigma pos),  vbar = sum_sigma VVbar(sigma pos).
-// The projector couples occupied triples that the canonical epilogue keeps
-// apart, so these steps work on whole-chunk FP64 arrays in the staging layout
-// (position = (tau; p, q, y, x, r, z), p outermost) instead of orbit tiles.
-// A chunk is closed under the index permutations involved (simultaneous
-// occupied/virtual permutations, the virtual-only permutations of r3, and
-// any change of p), so every gather stays inside the chunk.
+//
+// The projector couples all values of the first occupied index, which the
+// canonical epilogue's orbit tiles keep apart, so one chunk takes four passes
+// over FP64 work arrays in the staging layout (position = (tau; p, q, y, x,
+// r, z), p outermost, "column" = everything after p):
+//   1. tile forward  (orbit tiles in shared memory): WW -> B0, Q -> B2
+//   2. projection    (streaming over columns, all p of a column in a tile):
+//                    energy; with the adjoint also mat_bar, Dbar -> mo_bar,
+//                    Zbar -> B3 and P^T(Wtbar) -> B1
+//   3. tile adjoint  (orbit tiles): Xbar, WWbar, VVbar, their orbit sums;
+//                    wbar -> FP64 Wbar staging, vbar -> B0
+//   4. V gradients   (streaming over (r, z) rows of vbar)
+// An orbit tile is one occupied representative i >= j >= k with all its
+// permutations, times one triple of virtual sub-blocks with all its
+// orderings: closed under the simultaneous permutations of the orbit sums and
+// the virtual-only permutations of r3, so passes 1 and 3 gather only within
+// shared memory.
 #pragma once
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include "common.cuh"
 
 namespace tb {
 
-constexpr int kLnoMaxO = 64;    // largest nocc of the LNO path (shared-memory tiles)
+constexpr int kLnoMaxO = 64;    // largest nocc of the LNO path (projection tiles)
 constexpr int kLnoMaxTv = 16;   // largest virtual block
 constexpr int kLnoThreads = 256;
-constexpr int kLnoTile = 32;    // columns of a projection tile
+constexpr int kLnoTile = 32;    // columns per projection tile
+constexpr int kLnoSB = 4;       // virtual sub-block edge of an orbit tile
+constexpr int kLnoRegion = kLnoSB * kLnoSB * kLnoSB;
+constexpr int kLnoMaxSub = 64;  // sub-block triples per chunk: (16/4)^3
+constexpr int kLnoWaves = 4;    // waves of the streaming passes
+
+struct LnoSub {
+    int st[3];
+    int len[3];
+};
 
 struct LnoArgs {
     Dims d;
     ChunkDesc ch;
     signed char tau_of[27];                // ordering of (slot x, slot y, slot z); slots 0..2 = A, B, C
-    const double *S;                       // raw w of the chunk (FP64 staging)
+    int nsub;
+    LnoSub sub[kLnoMaxSub];
+    const int *ijk;                        // occupied representatives i >= j >= k
+    const void *S;                         // raw w of the chunk (staging, FP64 or FP32)
     double *B0, *B1, *B2, *B3;             // chunk-shaped work arrays (staging layout)
     const double *mat, *mo_e, *t1, *t2, *ovov, *fvo;
-    double *SW;                            // FP64 Wbar staging [y][p][x][q][rzp] per ordering
+    void *SW;                              // Wbar staging per ordering: FP64 [y][p][x][q][rzp], or
+                                           // 16-bit hi/lo planes [h][y][p][x][q][rzp] at 2 swoff
+    const double *wscale;                  // power-of-two scale of the fp16 split
     double *mat_bar, *mo_bar, *t1_bar, *t2_bar, *ovov_bar, *fvo_bar;
     double ybar;
+    int want_grad;
     double *part;                          // energy partials, gridDim.x * nperm
 };
 
 // r3 on the virtual indices (pyscfad/cc/ccsd_t_slow.py:84-87):
-// Z(j) = sum_s c_s X(i) with i[s[k]] = j[k].
-__constant__ int c_r3_perm[6][3] = {{0, 1, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}, {0, 2, 1}, {1, 0, 2}};
+// Z(j) = sum_s c_s X(i) with i[s[k]] = j[k], s = (0,1,2), (1,2,0), (2,0,1),
+// (2,1,0), (0,2,1), (1,0,2) (the orderings of lno_build_tables).
 __constant__ double c_r3_coef[6] = {4.0, 1.0, 1.0, -2.0, -2.0, -2.0};
 
 __device__ __forceinline__ int lno_slot(const ChunkDesc &ch, int g) {
@@ -50,342 +79,590 @@ __device__ __forceinline__ int lno_slot(const ChunkDesc &ch, int g) {
                                                                : 2;
 }
 
-// staging offset of position (p,q,r; x,y,z), global virtual indices
-__device__ __forceinline__ long long lno_off(const LnoArgs &A, int p, int q, int r, int x, int y, int z) {
-    const int o = A.d.o;
-    const int sx = lno_slot(A.ch, x), sy = lno_slot(A.ch, y), sz = lno_slot(A.ch, z);
-    const PermBlock &pb = A.ch.pb[A.tau_of[(sx * 3 + sy) * 3 + sz]];
-    return pb.soff + ((((long long)p * o + q) * pb.Ty + (y - pb.Y0)) * pb.Tx + (x - pb.X0)) * o * pb.Tz +
-           (long long)r * pb.Tz + (z - pb.Z0);
-}
-
-struct LnoPos {
-    int p, q, r, x, y, z;
-    long long off;
-};
-
-// position idx of ordering pb (staging order p, q, y, x, r, z)
-__device__ __forceinline__ LnoPos lno_decode(const LnoArgs &A, const PermBlock &pb, long long idx) {
-    const int o = A.d.o;
-    LnoPos P;
-    P.off = pb.soff + idx;
-    P.z = (int)(idx % pb.Tz) + pb.Z0;
-    idx /= pb.Tz;
-    P.r = (int)(idx % o);
-    idx /= o;
-    P.x = (int)(idx % pb.Tx) + pb.X0;
-    idx /= pb.Tx;
-    P.y = (int)(idx % pb.Ty) + pb.Y0;
-    idx /= pb.Ty;
-    P.q = (int)(idx % o);
-    P.p = (int)(idx / o);
-    return P;
-}
-
-__device__ __forceinline__ long long lno_npos(const LnoArgs &A, const PermBlock &pb) {
-    const long long o = A.d.o;
-    return o * o * o * pb.Tx * pb.Ty * pb.Tz;
-}
-
-__device__ __forceinline__ double lno_v(const LnoArgs &A, int p, int q, int r, int x, int y, int z) {
-    const int o = A.d.o, v = A.d.v;
-    return A.ovov[(((long long)p * v + x) * o + q) * v + y] * A.t1[(long long)r * v + z] +
-           A.t2[(((long long)q * o + p) * v + y) * v + x] * A.fvo[(long long)z * o + r];
-}
-
-__device__ __forceinline__ double lno_D(const LnoArgs &A, int p, int q, int r, int x, int y, int z) {
-    const int o = A.d.o;
-    return A.mo_e[p] + A.mo_e[q] + A.mo_e[r] - A.mo_e[o + x] - A.mo_e[o + y] - A.mo_e[o + z];
-}
-
 __device__ __forceinline__ double lno_warp_sum(double s) {
     for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
     return s;
 }
 
-// one thread per position of ordering blockIdx.y
-#define LNO_FOR_POSITIONS(A)                                                                                       \
-    const PermBlock &pb = (A).ch.pb[blockIdx.y];                                                                 \
-    const long long npos = lno_npos((A), pb);                                                                    \
-    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < npos;                          \
-         idx += (long long)gridDim.x * blockDim.x)
+// ---------------------------------------------------------------------------
+// orbit tiles
+// ---------------------------------------------------------------------------
+// Candidate region c = 6 pi + rho: occupied triple (ijk[pi0], ijk[pi1], ijk[pi2])
+// and virtual sub-ranges (U[rho0], U[rho1], U[rho2]).  Candidates with the same
+// triple and ranges hold the same positions; the first of them is "primary"
+// and owns a 4x4x4 slab of the shared arrays.  A position is (slab, slot),
+// slot = (4 l0 + l1) 4 + l2 for local virtual indices l.  The gather tables
+// give, per candidate and permutation, the candidate holding the permuted
+// position, and per slot and permutation the permuted slot.
+constexpr int kLnoIt = (36 * kLnoRegion + kLnoThreads - 1) / kLnoThreads;   // positions per thread
 
-// B0 = WW, B1 = X = WW + VV/2
-__global__ void __launch_bounds__(kLnoThreads) k_lno_ww(LnoArgs A) {
-    LNO_FOR_POSITIONS(A) {
-        const LnoPos P = lno_decode(A, pb, idx);
-        const int oc[3] = {P.p, P.q, P.r}, vi[3] = {P.x, P.y, P.z};
+// Gather tables, the same for every tile (built on the host, lno_build_tables):
+// per candidate and permutation the candidate holding the permuted position,
+// per permutation and slot the permuted slot; sigma runs over the six
+// simultaneous permutations, s over the six terms of r3 (0: forward
+// i[m] = j[sinv[m]], 1: adjoint j[k] = i[s[k]]).
+struct alignas(16) LnoTables {
+    unsigned char symsl[6][kLnoRegion];      // 16-byte multiples first: copied as uint4
+    unsigned char r3sl[2][6][kLnoRegion];
+    unsigned char symc[36][6];
+    unsigned char r3c[2][36][6];
+};
+__constant__ LnoTables c_lno_tab;
+
+inline void lno_build_tables(LnoTables &t) {
+    static const int r3p[6][3] = {{0, 1, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}, {0, 2, 1}, {1, 0, 2}};
+    for (int cc = 0; cc < 36; cc++)
+        for (int s = 0; s < 6; s++) {
+            int pp[3], pr[3], ps[3], m[3];
+            perm_of(cc / 6, pp);
+            perm_of(cc % 6, pr);
+            perm_of(s, ps);
+            t.symc[cc][s] = (unsigned char)(6 * perm_index(pp[ps[0]], pp[ps[1]]) + perm_index(pr[ps[0]], pr[ps[1]]));
+            for (int k = 0; k < 3; k++) m[r3p[s][k]] = k;
+            t.r3c[0][cc][s] = (unsigned char)(6 * (cc / 6) + perm_index(pr[m[0]], pr[m[1]]));
+            for (int k = 0; k < 3; k++) m[k] = r3p[s][k];
+            t.r3c[1][cc][s] = (unsigned char)(6 * (cc / 6) + perm_index(pr[m[0]], pr[m[1]]));
+        }
+    for (int s = 0; s < 6; s++)
+        for (int sl = 0; sl < kLnoRegion; sl++) {
+            const int l[3] = {sl / (kLnoSB * kLnoSB), (sl / kLnoSB) % kLnoSB, sl % kLnoSB};
+            int ps[3], m[3];
+            perm_of(s, ps);
+            t.symsl[s][sl] = (unsigned char)((l[ps[0]] * kLnoSB + l[ps[1]]) * kLnoSB + l[ps[2]]);
+            for (int k = 0; k < 3; k++) m[r3p[s][k]] = k;
+            t.r3sl[0][s][sl] = (unsigned char)((l[m[0]] * kLnoSB + l[m[1]]) * kLnoSB + l[m[2]]);
+            for (int k = 0; k < 3; k++) m[k] = r3p[s][k];
+            t.r3sl[1][s][sl] = (unsigned char)((l[m[0]] * kLnoSB + l[m[1]]) * kLnoSB + l[m[2]]);
+        }
+}
+
+// Duplicate candidates depend only on which occupied indices coincide
+// (i == j, j == k) and which virtual sub-ranges coincide (U0 == U1, U1 == U2):
+// 16 patterns, each listing its slabs' candidates and every candidate's slab.
+struct LnoPattern {
+    unsigned char nslab;
+    unsigned char cand[36];
+    unsigned char prim[36];
+};
+__constant__ LnoPattern c_lno_pat[16];
+
+inline void lno_build_patterns(LnoPattern pats[16]) {
+    for (int pid = 0; pid < 16; pid++) {
+        const int eo01 = (pid >> 3) & 1, eo12 = (pid >> 2) & 1, ev01 = (pid >> 1) & 1, ev12 = pid & 1;
+        int occ[3] = {2, 1, 0}, vr[3] = {2, 1, 0};
+        if (eo12) occ[1] = occ[2];
+        if (eo01) occ[0] = occ[1];
+        if (ev12) vr[1] = vr[2];
+        if (ev01) vr[0] = vr[1];
+        int key[36][6], first[36];
+        for (int c = 0; c < 36; c++) {
+            int pp[3], pr[3];
+            perm_of(c / 6, pp);
+            perm_of(c % 6, pr);
+            for (int k = 0; k < 3; k++) {
+                key[c][k] = occ[pp[k]];
+                key[c][3 + k] = vr[pr[k]];
+            }
+            first[c] = c;
+            for (int c2 = 0; c2 < c; c2++) {
+                bool same = true;
+                for (int k = 0; k < 6; k++) same = same && key[c2][k] == key[c][k];
+                if (same) {
+                    first[c] = c2;
+                    break;
+                }
+            }
+        }
+        LnoPattern &P = pats[pid];
+        int n = 0, prim[36];
+        for (int c = 0; c < 36; c++)
+            if (first[c] == c) {
+                prim[c] = n;
+                P.cand[n++] = (unsigned char)c;
+            }
+        for (int c = n; c < 36; c++) P.cand[c] = 0;
+        for (int c = 0; c < 36; c++) P.prim[c] = (unsigned char)prim[first[c]];
+        P.nslab = (unsigned char)n;
+    }
+}
+
+struct LnoTile {
+    int occ[36][3];       // per slab: occupied triple
+    int vst[36][3];       // per slab: virtual range starts (global)
+    int vlen[36][3];      // per slab: range lengths
+    long long soff[36];   // per slab: staging offset of local (0,0,0)
+    long long swoff[36];  // per slab: Wbar staging offset of local (0,0,0)
+    int sx[36], sy[36];   // per slab: staging strides of local x, y
+    long long swx[36], swy[36];
+    long long b_ov[36], b_t2[36];   // per slab: ovov[p,x0,q,y0], t2[q,p,y0,x0] offsets
+    int b_t1[36], b_fv[36];         // per slab: t1[r,z0], fvo[z0,r] offsets
+    long long plane[36];  // per slab: elements of its ordering's Wbar plane (split staging)
+    long long swbase[36]; // per slab: its ordering's Wbar offset (the split planes start at twice it)
+    double eocc[36];      // per slab: e_p + e_q + e_r
+    short symg[36][6];    // per slab and sigma: first position of the target slab
+    short r3g[2][36][6];  // per slab and r3 term
+    alignas(16) unsigned char symsl[6][kLnoRegion];
+    alignas(16) unsigned char r3sl[2][6][kLnoRegion];
+    int nslab;
+};
+
+__device__ void lno_tile_setup(const LnoArgs &A, LnoTile &T) {
+    const int o = A.d.o, v = A.d.v;
+    const int rep = blockIdx.x;
+    const LnoSub &U = A.sub[blockIdx.y];
+    {
+        const uint4 *src = reinterpret_cast<const uint4 *>(&c_lno_tab.symsl[0][0]);
+        uint4 *dst = reinterpret_cast<uint4 *>(&T.symsl[0][0]);
+        for (int e = threadIdx.x; e < 6 * kLnoRegion / 16; e += blockDim.x) dst[e] = src[e];
+        const uint4 *src2 = reinterpret_cast<const uint4 *>(&c_lno_tab.r3sl[0][0][0]);
+        uint4 *dst2 = reinterpret_cast<uint4 *>(&T.r3sl[0][0][0]);
+        for (int e = threadIdx.x; e < 12 * kLnoRegion / 16; e += blockDim.x) dst2[e] = src2[e];
+    }
+    const int ijk[3] = {A.ijk[3 * rep], A.ijk[3 * rep + 1], A.ijk[3 * rep + 2]};
+    const int pid = ((ijk[0] == ijk[1]) << 3) | ((ijk[1] == ijk[2]) << 2) | ((U.st[0] == U.st[1]) << 1) |
+                    (U.st[1] == U.st[2]);
+    const LnoPattern &P = c_lno_pat[pid];
+    const int c = threadIdx.x;
+    if (c == 0) T.nslab = P.nslab;
+    if (c < P.nslab) {
+        const int cc = P.cand[c];
+        int pp[3], pr[3];
+        perm_of(cc / 6, pp);
+        perm_of(cc % 6, pr);
+        for (int k = 0; k < 3; k++) {
+            T.occ[c][k] = ijk[pp[k]];
+            T.vst[c][k] = U.st[pr[k]];
+            T.vlen[c][k] = U.len[pr[k]];
+        }
+        const int x0 = T.vst[c][0], y0 = T.vst[c][1], z0 = T.vst[c][2];
+        const int p = T.occ[c][0], q = T.occ[c][1], r = T.occ[c][2];
+        const int t = A.tau_of[(lno_slot(A.ch, x0) * 3 + lno_slot(A.ch, y0)) * 3 + lno_slot(A.ch, z0)];
+        const PermBlock &pb = A.ch.pb[t];
+        const long long oTz = (long long)o * pb.Tz;
+        T.sx[c] = (int)oTz;
+        T.sy[c] = (int)(pb.Tx * oTz);
+        T.soff[c] = pb.soff + (((long long)p * o + q) * pb.Ty + (y0 - pb.Y0)) * pb.Tx * oTz +
+                    (long long)(x0 - pb.X0) * oTz + (long long)r * pb.Tz + (z0 - pb.Z0);
+        const long long wx = (long long)o * pb.rzp, wy = (long long)o * pb.Tx * wx;
+        T.swx[c] = wx;
+        T.swy[c] = wy;
+        T.swoff[c] = pb.swoff + (long long)(y0 - pb.Y0) * wy + (long long)p * pb.Tx * wx + (long long)(x0 - pb.X0) * wx +
+                     (long long)q * pb.rzp + (long long)r * pb.Tz + (z0 - pb.Z0);
+        T.plane[c] = (long long)pb.Ty * wy;
+        T.swbase[c] = pb.swoff;
+        T.b_ov[c] = (((long long)p * v + x0) * o + q) * v + y0;
+        T.b_t2[c] = (((long long)q * o + p) * v + y0) * v + x0;
+        T.b_t1[c] = r * v + z0;
+        T.b_fv[c] = z0 * o + r;
+        T.eocc[c] = A.mo_e[p] + A.mo_e[q] + A.mo_e[r];
+        for (int s = 0; s < 6; s++) {
+            T.symg[c][s] = (short)(P.prim[c_lno_tab.symc[cc][s]] * kLnoRegion);
+            T.r3g[0][c][s] = (short)(P.prim[c_lno_tab.r3c[0][cc][s]] * kLnoRegion);
+            T.r3g[1][c][s] = (short)(P.prim[c_lno_tab.r3c[1][cc][s]] * kLnoRegion);
+        }
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ int lno_sym_at(const LnoTile &T, int g, int sl, int s) {
+    return T.symg[g][s] + T.symsl[s][sl];
+}
+__device__ __forceinline__ int lno_r3_at(const LnoTile &T, int g, int sl, int s, int adj) {
+    return T.r3g[adj][g][s] + T.r3sl[adj][s][sl];
+}
+
+// it-th position of this thread; fields valid only when in range
+#define LNO_POS(T, it)                                                                                              \
+    const int e = threadIdx.x + (it) * kLnoThreads;                                                               \
+    const bool inr = e < (T).nslab * kLnoRegion;                                                                  \
+    const int g = inr ? e / kLnoRegion : 0, sl = e % kLnoRegion;                                                  \
+    const int l0 = sl / (kLnoSB * kLnoSB), l1 = (sl / kLnoSB) % kLnoSB, l2 = sl % kLnoSB;                         \
+    const bool valid = inr && l0 < (T).vlen[g][0] && l1 < (T).vlen[g][1] && l2 < (T).vlen[g][2];                \
+    const long long goff = (T).soff[g] + (long long)l1 * (T).sy[g] + (long long)l0 * (T).sx[g] + l2
+
+// pass 1: WW -> B0, Q = r3(WW + VV/2) / D -> B2
+template <typename StageT>
+__global__ void __launch_bounds__(kLnoThreads) k_lno_tile_fwd(LnoArgs A) {
+    const StageT *S = reinterpret_cast<const StageT *>(A.S);
+    __shared__ LnoTile T;
+    extern __shared__ double lno_sm[];
+    double *sW = lno_sm, *sV = lno_sm + 36 * kLnoRegion;
+    lno_tile_setup(A, T);
+    const int o = A.d.o;
+#pragma unroll
+    for (int it = 0; it < kLnoIt; it++) {
+        LNO_POS(T, it);
+        if (!inr) break;
+        double w = 0.0, vv = 0.0;
+        if (valid) {
+            // v = ovov[p,x,q,y] t1[r,z] + t2[q,p,y,x] fvo[z,r]
+            const int o_ = A.d.o, v_ = A.d.v;
+            w = (double)S[goff];
+            vv = A.ovov[T.b_ov[g] + (long long)l0 * o_ * v_ + l1] * A.t1[T.b_t1[g] + l2] +
+                 A.t2[T.b_t2[g] + (long long)l1 * v_ + l0] * A.fvo[T.b_fv[g] + l2 * o_];
+        }
+        sW[e] = w;
+        sV[e] = vv;
+    }
+    __syncthreads();
+    double xr[kLnoIt];
+#pragma unroll
+    for (int it = 0; it < kLnoIt; it++) {
+        LNO_POS(T, it);
+        xr[it] = 0.0;
+        if (!valid) continue;
         double ww = 0.0, vv = 0.0;
 #pragma unroll
         for (int s = 0; s < 6; s++) {
-            int ps[3];
-            perm_of(s, ps);
-            const int p = oc[ps[0]], q = oc[ps[1]], r = oc[ps[2]];
-            const int x = vi[ps[0]], y = vi[ps[1]], z = vi[ps[2]];
-            ww += A.S[lno_off(A, p, q, r, x, y, z)];
-            vv += lno_v(A, p, q, r, x, y, z);
+            const int k = lno_sym_at(T, g, sl, s);
+            ww += sW[k];
+            vv += sV[k];
         }
-        A.B0[P.off] = ww;
-        A.B1[P.off] = ww + 0.5 * vv;
+        A.B0[goff] = ww;
+        xr[it] = ww + 0.5 * vv;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < kLnoIt; it++) {
+        LNO_POS(T, it);
+        (void)valid;
+        (void)goff;
+        if (inr) sW[e] = xr[it];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < kLnoIt; it++) {
+        LNO_POS(T, it);
+        if (!valid) continue;
+        double z = 0.0;
+#pragma unroll
+        for (int s = 0; s < 6; s++) z += c_r3_coef[s] * sW[lno_r3_at(T, g, sl, s, 0)];
+        const double D = T.eocc[g] - A.mo_e[o + T.vst[g][0] + l0] - A.mo_e[o + T.vst[g][1] + l1] -
+                         A.mo_e[o + T.vst[g][2] + l2];
+        A.B2[goff] = z / D;
     }
 }
 
-// B2 = Q = r3(X) / D
-__global__ void __launch_bounds__(kLnoThreads) k_lno_q(LnoArgs A) {
-    LNO_FOR_POSITIONS(A) {
-        const LnoPos P = lno_decode(A, pb, idx);
-        const int j[3] = {P.x, P.y, P.z};
-        double zsum = 0.0;
+// pass 3: Xbar = r3^T(Zbar (B3)), WWbar = P^T(Wtbar) (B1) + Xbar, VVbar = Xbar/2;
+// wbar = orbit sum of WWbar -> Wbar staging, vbar = orbit sum of VVbar -> B0.
+// SPLIT 0: FP64 staging; 1: fp16 hi/lo of wbar * wscale (exact power of two);
+// 2: bf16 hi/lo, unscaled -- the operand formats of the adjoint contractions.
+template <int SPLIT>
+__global__ void __launch_bounds__(kLnoThreads) k_lno_tile_adj(LnoArgs A) {
+    __shared__ LnoTile T;
+    extern __shared__ double lno_sm[];
+    double *sZ = lno_sm, *sW = lno_sm + 36 * kLnoRegion;
+    lno_tile_setup(A, T);
+#pragma unroll
+    for (int it = 0; it < kLnoIt; it++) {
+        LNO_POS(T, it);
+        if (!inr) break;
+        sZ[e] = valid ? A.B3[goff] : 0.0;
+        sW[e] = valid ? A.B1[goff] : 0.0;
+    }
+    __syncthreads();
+    double xr[kLnoIt];
+#pragma unroll
+    for (int it = 0; it < kLnoIt; it++) {
+        LNO_POS(T, it);
+        (void)goff;
+        xr[it] = 0.0;
+        if (!valid) continue;
+        double xb = 0.0;
+#pragma unroll
+        for (int s = 0; s < 6; s++) xb += c_r3_coef[s] * sZ[lno_r3_at(T, g, sl, s, 1)];
+        xr[it] = xb;
+        sW[e] += xb;   // only this thread reads sW[e] in this phase
+    }
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < kLnoIt; it++) {
+        LNO_POS(T, it);
+        (void)valid;
+        (void)goff;
+        if (inr) sZ[e] = 0.5 * xr[it];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < kLnoIt; it++) {
+        LNO_POS(T, it);
+        if (!valid) continue;
+        double wb = 0.0, vb = 0.0;
 #pragma unroll
         for (int s = 0; s < 6; s++) {
-            int i[3];
-#pragma unroll
-            for (int k = 0; k < 3; k++) i[c_r3_perm[s][k]] = j[k];
-            zsum += c_r3_coef[s] * A.B1[lno_off(A, P.p, P.q, P.r, i[0], i[1], i[2])];
+            const int k = lno_sym_at(T, g, sl, s);
+            wb += sW[k];
+            vb += sZ[k];
         }
-        A.B2[P.off] = zsum / lno_D(A, P.p, P.q, P.r, P.x, P.y, P.z);
+        const long long wl = T.swoff[g] + (long long)l1 * T.swy[g] + (long long)l0 * T.swx[g] + l2;
+        if (SPLIT == 0) {
+            reinterpret_cast<double *>(A.SW)[wl] = wb;
+        } else if (SPLIT == 1) {
+            const float xs = (float)(wb * *A.wscale);
+            const __half h = __float2half_rn(xs);
+            __half *dst = reinterpret_cast<__half *>(A.SW) + T.swbase[g] + wl;   // 2 swoff + local offset
+            dst[0] = h;
+            dst[T.plane[g]] = __float2half_rn(xs - __half2float(h));
+        } else {
+            const float xs = (float)wb;
+            const __nv_bfloat16 h = __float2bfloat16_rn(xs);
+            __nv_bfloat16 *dst = reinterpret_cast<__nv_bfloat16 *>(A.SW) + T.swbase[g] + wl;
+            dst[0] = h;
+            dst[T.plane[g]] = __float2bfloat16_rn(xs - __bfloat162float(h));
+        }
+        A.B0[goff] = vb;
     }
 }
 
-// Projection along the first occupied index, out[i, rest] = f sum_l M(l,i) in[l, rest]:
-// transpose = 1: M(l,i) = mat[l,i] (Wt from WW); 0: M(l,i) = mat[i,l] (P^T, the adjoint).
-// A block stages in[:, c0:c0+32] in shared memory and writes all o rows of
-// those columns.
-__global__ void __launch_bounds__(kLnoThreads) k_lno_project(LnoArgs A, const double *__restrict__ in,
-                                                             double *__restrict__ out, int transpose, double f) {
-    __shared__ double tile[kLnoMaxO][kLnoTile + 1];
+#undef LNO_POS
+
+// ---------------------------------------------------------------------------
+// pass 2: projection along the first occupied index, streaming over columns
+// ---------------------------------------------------------------------------
+// Column c of ordering pb = (((q Ty + y) Tx + x) o + r) Tz + z (< 2^31); position p c.
+// Per 32-column tile with all o rows of WW (B0) and Q (B2) in shared memory:
+//   Wt[i,c] = sum_l mat[l,i] WW[l,c],  energy += Wt Q;
+//   with the adjoint: Zbar = f Wt / D -> B3, Dbar = -f Wt Q / D -> B2 (over Q),
+//   P^T(Wtbar)[l,c] = f sum_i mat[l,i] Q[i,c] -> B1, Gram WW Q^T -> mat_bar
+//   (f = ybar / 3).
+// Thread (warp w, lane j) owns column j and rows w, w+8, ... (R of them); the
+// Gram products use 4x4 register tiles of (l, i) over a share of the columns.
+constexpr int kLnoTileLd = kLnoTile + 1;
+
+inline size_t lno_proj_smem(int o) {
+    return (size_t)(2 * kLnoMaxO * kLnoTileLd + o * o + kLnoMaxO + kLnoTile) * sizeof(double);
+}
+
+template <int R>
+__global__ void __launch_bounds__(kLnoThreads, 2) k_lno_proj(LnoArgs A) {
+    extern __shared__ double lno_sm[];
+    double *sw = lno_sm, *sq = sw + kLnoMaxO * kLnoTileLd, *sM = sq + kLnoMaxO * kLnoTileLd;
     const int o = A.d.o;
+    double *s_eo = sM + o * o, *s_ecol = s_eo + kLnoMaxO;
+    __shared__ double red[kLnoThreads / 32];
+    const int o4 = (o + 3) & ~3;
     const PermBlock &pb = A.ch.pb[blockIdx.y];
-    const long long stride_p = lno_npos(A, pb) / o;
-    const long long ntile = (stride_p + kLnoTile - 1) / kLnoTile;
-    for (long long tb = blockIdx.x; tb < ntile; tb += gridDim.x) {
-        const long long c0 = tb * kLnoTile;
+    const int stride_p = o * o * pb.Tx * pb.Ty * pb.Tz;
+    const int ntile = (stride_p + kLnoTile - 1) / kLnoTile;
+    const double f = A.ybar / 3.0;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const bool grad = A.want_grad != 0;
+    for (int k = threadIdx.x; k < o * o; k += blockDim.x) sM[k] = A.mat[k];
+    for (int k = threadIdx.x; k < o; k += blockDim.x) s_eo[k] = A.mo_e[k];
+    // Gram register tiles
+    const int nmt = o4 / 4, nm = nmt * nmt;
+    const int cg = nm >= kLnoThreads ? 1 : kLnoThreads / nm;
+    const bool gact = (int)threadIdx.x < nm * cg;
+    const int mt = threadIdx.x % nm, cgi = threadIdx.x / nm;
+    const int lb = (mt / nmt) * 4, ib = (mt % nmt) * 4;
+    double acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
+    double en = 0.0;
+    const double *W = A.B0 + pb.soff, *Qg = A.B2 + pb.soff;
+    for (int tb = blockIdx.x; tb < ntile; tb += gridDim.x) {
+        const int c0 = tb * kLnoTile;
         __syncthreads();
-        for (int e = threadIdx.x; e < o * kLnoTile; e += blockDim.x) {
+        for (int e = threadIdx.x; e < o4 * kLnoTile; e += blockDim.x) {
             const int l = e / kLnoTile, j = e % kLnoTile;
-            tile[l][j] = (c0 + j < stride_p) ? in[pb.soff + l * stride_p + c0 + j] : 0.0;
+            const bool ok = l < o && c0 + j < stride_p;
+            sw[l * kLnoTileLd + j] = ok ? W[(long long)l * stride_p + c0 + j] : 0.0;
+            sq[l * kLnoTileLd + j] = ok ? Qg[(long long)l * stride_p + c0 + j] : 0.0;
+        }
+        if (grad && threadIdx.x < kLnoTile) {
+            int cc = c0 + threadIdx.x;
+            double ec = 0.0;
+            if (cc < stride_p) {
+                const int zl = cc % pb.Tz;
+                cc /= pb.Tz;
+                const int r = cc % o;
+                cc /= o;
+                const int xl = cc % pb.Tx;
+                cc /= pb.Tx;
+                const int yl = cc % pb.Ty;
+                const int q = cc / pb.Ty;
+                ec = A.mo_e[q] + A.mo_e[r] - A.mo_e[o + pb.X0 + xl] - A.mo_e[o + pb.Y0 + yl] -
+                     A.mo_e[o + pb.Z0 + zl];
+            }
+            s_ecol[threadIdx.x] = ec;
         }
         __syncthreads();
-        for (int e = threadIdx.x; e < o * kLnoTile; e += blockDim.x) {
-            const int i = e / kLnoTile, j = e % kLnoTile;
-            if (c0 + j >= stride_p) continue;
-            double s = 0.0;
-            for (int l = 0; l < o; l++)
-                s += (transpose ? __ldg(&A.mat[l * o + i]) : __ldg(&A.mat[i * o + l])) * tile[l][j];
-            out[pb.soff + i * stride_p + c0 + j] = f * s;
+        const int j = lane;
+        const int c = c0 + j;
+        const bool ok = c < stride_p;
+        double wt[R], pq[R];
+#pragma unroll
+        for (int k = 0; k < R; k++) wt[k] = pq[k] = 0.0;
+        for (int l = 0; l < o; l++) {
+            const double a = sw[l * kLnoTileLd + j], b = sq[l * kLnoTileLd + j];
+#pragma unroll
+            for (int k = 0; k < R; k++) {
+                const int i = warp + k * (kLnoThreads / 32);
+                if (i < o) {
+                    wt[k] += sM[l * o + i] * a;
+                    if (grad) pq[k] += sM[i * o + l] * b;
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < R; k++) {
+            const int i = warp + k * (kLnoThreads / 32);
+            if (i < o) {
+                const double qv = sq[i * kLnoTileLd + j];
+                en += wt[k] * qv;
+                if (grad && ok) {
+                    const double D = s_eo[i] + s_ecol[j];
+                    const double qb = f * wt[k];
+                    const long long at = pb.soff + (long long)i * stride_p + c;
+                    A.B3[at] = qb / D;
+                    A.B2[at] = -qb * qv / D;
+                    A.B1[at] = f * pq[k];
+                }
+            }
+        }
+        if (grad && gact) {
+            for (int jj = cgi; jj < kLnoTile; jj += cg) {
+                double a[4], b[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    a[k] = sw[(lb + k) * kLnoTileLd + jj];
+                    b[k] = sq[(ib + k) * kLnoTileLd + jj];
+                }
+#pragma unroll
+                for (int x = 0; x < 4; x++)
+#pragma unroll
+                    for (int y = 0; y < 4; y++) acc[x][y] += a[x] * b[y];
+            }
         }
     }
-}
-
-// energy partials (1/3) sum Wt Q (B3 = Wt, B2 = Q), one per block
-__global__ void __launch_bounds__(kLnoThreads) k_lno_energy(LnoArgs A) {
-    __shared__ double red[kLnoThreads / 32];
-    double e = 0.0;
-    LNO_FOR_POSITIONS(A) e += A.B3[pb.soff + idx] * A.B2[pb.soff + idx];
-    e = lno_warp_sum(e);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = e;
+    en = lno_warp_sum(en);
+    if (lane == 0) red[warp] = en;
     __syncthreads();
     if (threadIdx.x == 0) {
         double s = 0.0;
         for (int w = 0; w < kLnoThreads / 32; w++) s += red[w];
         A.part[blockIdx.y * gridDim.x + blockIdx.x] = s / 3.0;
     }
-}
-
-// mat_bar[l,i] += (ybar/3) sum_rest WW[l, rest] Q[i, rest]
-__global__ void __launch_bounds__(kLnoThreads) k_lno_matbar(LnoArgs A) {
-    __shared__ double sw[kLnoMaxO][kLnoTile + 1], sq[kLnoMaxO][kLnoTile + 1];
-    constexpr int kAcc = kLnoMaxO * kLnoMaxO / kLnoThreads;
-    const int o = A.d.o;
-    const PermBlock &pb = A.ch.pb[blockIdx.y];
-    const long long stride_p = lno_npos(A, pb) / o;
-    const long long ntile = (stride_p + kLnoTile - 1) / kLnoTile;
-    double acc[kAcc];
-#pragma unroll
-    for (int k = 0; k < kAcc; k++) acc[k] = 0.0;
-    for (long long tb = blockIdx.x; tb < ntile; tb += gridDim.x) {
-        const long long c0 = tb * kLnoTile;
-        __syncthreads();
-        for (int e = threadIdx.x; e < o * kLnoTile; e += blockDim.x) {
-            const int l = e / kLnoTile, j = e % kLnoTile;
-            const bool ok = c0 + j < stride_p;
-            sw[l][j] = ok ? A.B0[pb.soff + l * stride_p + c0 + j] : 0.0;
-            sq[l][j] = ok ? A.B2[pb.soff + l * stride_p + c0 + j] : 0.0;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < kAcc; k++) {
-            const int pair = threadIdx.x + k * kLnoThreads;
-            if (pair < o * o) {
-                const int l = pair / o, i = pair % o;
-                double s = 0.0;
-#pragma unroll 8
-                for (int j = 0; j < kLnoTile; j++) s += sw[l][j] * sq[i][j];
-                acc[k] += s;
-            }
-        }
-    }
-#pragma unroll
-    for (int k = 0; k < kAcc; k++) {
-        const int pair = threadIdx.x + k * kLnoThreads;
-        if (pair < o * o && acc[k] != 0.0) atomicAdd(&A.mat_bar[pair], A.ybar / 3.0 * acc[k]);
-    }
-}
-
-// One thread per pair row (p,q,y,x) of ordering blockIdx.y, looping over (r,z);
-// the loop is warp-uniform so that every lane takes part in the shuffles.
-#define LNO_FOR_PAIR_ROWS(A)                                                                                       \
-    const PermBlock &pb = (A).ch.pb[blockIdx.y];                                                                 \
-    const long long npr = (long long)(A).d.o * (A).d.o * pb.Ty * pb.Tx;                                          \
-    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < npr;                 \
-         base += (long long)gridDim.x * blockDim.x)
-
-// B3: Wt -> Zbar = (ybar/3) Wt / D in place; Dbar = -(ybar/3) Wt Q / D into mo_bar
-__global__ void __launch_bounds__(kLnoThreads) k_lno_zbar(LnoArgs A) {
-    __shared__ double s_occ[kLnoMaxO], s_vir[3][kLnoMaxTv];
-    const int o = A.d.o;
-    for (int e = threadIdx.x; e < kLnoMaxO; e += blockDim.x) s_occ[e] = 0.0;
-    for (int e = threadIdx.x; e < 3 * kLnoMaxTv; e += blockDim.x) s_vir[e / kLnoMaxTv][e % kLnoMaxTv] = 0.0;
+    if (!grad) return;
+    // Gram partials: column groups summed in shared memory, then one atomic per entry
+    double *sG = sw;   // o*o <= 2 * kLnoMaxO * kLnoTileLd entries, tiles no longer needed
+    for (int k = threadIdx.x; k < o * o; k += blockDim.x) sG[k] = 0.0;
     __syncthreads();
-    const int lane = threadIdx.x & 31;
-    LNO_FOR_PAIR_ROWS(A) {
-        const long long pr = base + lane;
-        const bool active = pr < npr;
-        const int xl = (int)(pr % pb.Tx), yl = (int)((pr / pb.Tx) % pb.Ty);
-        const int q = (int)((pr / ((long long)pb.Tx * pb.Ty)) % o), p = (int)(pr / ((long long)pb.Tx * pb.Ty * o));
-        const int x = pb.X0 + xl, y = pb.Y0 + yl;
-        double zacc[kLnoMaxTv];
+    if (gact) {
 #pragma unroll
-        for (int z = 0; z < kLnoMaxTv; z++) zacc[z] = 0.0;
-        double dsum = 0.0;
-        for (int r = 0; r < o; r++) {
-            double dr = 0.0;
+        for (int x = 0; x < 4; x++)
 #pragma unroll
-            for (int zl = 0; zl < kLnoMaxTv; zl++) {
-                if (zl < pb.Tz) {
-                    double db = 0.0;
-                    if (active) {
-                        const long long off = pb.soff + (pr * o + r) * pb.Tz + zl;
-                        const double D = lno_D(A, p, q, r, x, y, pb.Z0 + zl);
-                        const double qb = A.ybar / 3.0 * A.B3[off];
-                        db = -qb * A.B2[off] / D;
-                        A.B3[off] = qb / D;
-                    }
-                    dr += db;
-                    zacc[zl] += db;
-                }
-            }
-            dsum += dr;
-            const double wr = lno_warp_sum(dr);   // every lane has the same r
-            if (lane == 0 && wr != 0.0) atomicAdd(&s_occ[r], wr);
-        }
-#pragma unroll
-        for (int zl = 0; zl < kLnoMaxTv; zl++) {
-            if (zl < pb.Tz) {
-                const double wz = lno_warp_sum(zacc[zl]);
-                if (lane == 0 && wz != 0.0) atomicAdd(&s_vir[2][zl], -wz);
-            }
-        }
-        if (active && dsum != 0.0) {
-            atomicAdd(&s_occ[p], dsum);
-            atomicAdd(&s_occ[q], dsum);
-            atomicAdd(&s_vir[0][xl], -dsum);
-            atomicAdd(&s_vir[1][yl], -dsum);
-        }
+            for (int y = 0; y < 4; y++)
+                if (lb + x < o && ib + y < o && acc[x][y] != 0.0) atomicAdd(&sG[(lb + x) * o + ib + y], acc[x][y]);
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < o; e += blockDim.x)
-        if (s_occ[e] != 0.0) atomicAdd(&A.mo_bar[e], s_occ[e]);
-    for (int e = threadIdx.x; e < 3 * kLnoMaxTv; e += blockDim.x) {
-        const int role = e / kLnoMaxTv, k = e % kLnoMaxTv;
-        const int g0 = role == 0 ? pb.X0 : role == 1 ? pb.Y0 : pb.Z0;
-        const int len = role == 0 ? pb.Tx : role == 1 ? pb.Ty : pb.Tz;
-        if (k < len && s_vir[role][k] != 0.0) atomicAdd(&A.mo_bar[o + g0 + k], s_vir[role][k]);
-    }
+    for (int k = threadIdx.x; k < o * o; k += blockDim.x)
+        if (sG[k] != 0.0) atomicAdd(&A.mat_bar[k], f * sG[k]);
 }
 
-// Xbar(i) = sum_s c_s Zbar(j), j[k] = i[s[k]] (the transpose of r3);
-// B0 += Xbar (WWbar), B1 = Xbar / 2 (VVbar)
-__global__ void __launch_bounds__(kLnoThreads) k_lno_xbar(LnoArgs A) {
-    LNO_FOR_POSITIONS(A) {
-        const LnoPos P = lno_decode(A, pb, idx);
-        const int i[3] = {P.x, P.y, P.z};
-        double xb = 0.0;
-#pragma unroll
-        for (int s = 0; s < 6; s++)
-            xb += c_r3_coef[s] *
-                  A.B3[lno_off(A, P.p, P.q, P.r, i[c_r3_perm[s][0]], i[c_r3_perm[s][1]], i[c_r3_perm[s][2]])];
-        A.B0[P.off] += xb;
-        A.B1[P.off] = 0.5 * xb;
-    }
-}
-
-// wbar, vbar: orbit sums of WWbar (B0) and VVbar (B1).  wbar goes to the FP64
-// Wbar staging that the adjoint contractions read; vbar to the V-term gradients
-// of v = ovov[p,x,q,y] t1[r,z] + t2[q,p,y,x] fvo[z,r].
-__global__ void __launch_bounds__(kLnoThreads) k_lno_scatter(LnoArgs A) {
-    __shared__ double s_t1[kLnoMaxO][kLnoMaxTv], s_fv[kLnoMaxO][kLnoMaxTv];
+// ---------------------------------------------------------------------------
+// pass 4: V-term and denominator gradients from vbar (B0) and Dbar (B2), one
+// warp per (p, q, y, x) row of o Tz contiguous (r, z) values:
+//   ovov_bar[p,x,q,y] += sum_rz vbar t1[r,z],   t2_bar[q,p,y,x] += sum_rz vbar fvo[z,r],
+//   t1_bar[r,z] += sum vbar ovov[p,x,q,y],      fvo_bar[z,r] += sum vbar t2[q,p,y,x],
+//   mo_bar[p], [q], [r] += sum Dbar;  mo_bar[o+x], [o+y], [o+z] -= sum Dbar.
+// Lane k of every warp owns elements k, k+32, ... of the row (M per lane) and
+// keeps their sums in registers across rows.
+// ---------------------------------------------------------------------------
+template <int M>
+__global__ void __launch_bounds__(kLnoThreads) k_lno_vgrad(LnoArgs A) {
+    __shared__ double s_t1[kLnoMaxO * kLnoMaxTv], s_fv[kLnoMaxO * kLnoMaxTv], s_rz[kLnoMaxO * kLnoMaxTv];
+    __shared__ double s_occ[kLnoThreads / 32][kLnoMaxO], s_vir[kLnoThreads / 32][2][kLnoMaxTv];
     const int o = A.d.o, v = A.d.v;
-    for (int e = threadIdx.x; e < kLnoMaxO * kLnoMaxTv; e += blockDim.x) {
-        s_t1[e / kLnoMaxTv][e % kLnoMaxTv] = 0.0;
-        s_fv[e / kLnoMaxTv][e % kLnoMaxTv] = 0.0;
-    }
+    const PermBlock &pb = A.ch.pb[blockIdx.y];
+    const int oTz = o * pb.Tz;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int k = threadIdx.x; k < oTz; k += blockDim.x) s_t1[k] = s_fv[k] = s_rz[k] = 0.0;
+    for (int k = lane; k < kLnoMaxO; k += 32) s_occ[warp][k] = 0.0;
+    for (int k = lane; k < 2 * kLnoMaxTv; k += 32) s_vir[warp][k / kLnoMaxTv][k % kLnoMaxTv] = 0.0;
     __syncthreads();
-    const int lane = threadIdx.x & 31;
-    LNO_FOR_PAIR_ROWS(A) {
-        const long long pr = base + lane;
-        const bool active = pr < npr;
-        const int xl = (int)(pr % pb.Tx), yl = (int)((pr / pb.Tx) % pb.Ty);
-        const int q = (int)((pr / ((long long)pb.Tx * pb.Ty)) % o), p = (int)(pr / ((long long)pb.Tx * pb.Ty * o));
+    double a1[M], af[M], ar[M];
+#pragma unroll
+    for (int m = 0; m < M; m++) a1[m] = af[m] = ar[m] = 0.0;
+    const int npr = o * o * pb.Ty * pb.Tx;
+    const int nwarp = gridDim.x * (blockDim.x >> 5);
+    for (int pr = blockIdx.x * (blockDim.x >> 5) + warp; pr < npr; pr += nwarp) {
+        const int xl = pr % pb.Tx, yl = (pr / pb.Tx) % pb.Ty;
+        const int q = (pr / (pb.Tx * pb.Ty)) % o, p = pr / (pb.Tx * pb.Ty * o);
         const int x = pb.X0 + xl, y = pb.Y0 + yl;
         const long long iov = (((long long)p * v + x) * o + q) * v + y;
         const long long it2 = (((long long)q * o + p) * v + y) * v + x;
-        const double ovv = active ? A.ovov[iov] : 0.0, t2v = active ? A.t2[it2] : 0.0;
-        const long long wx = (long long)o * pb.rzp, wy = (long long)o * pb.Tx * wx;
-        const long long swrow = pb.swoff + yl * wy + (long long)p * pb.Tx * wx + xl * wx + (long long)q * pb.rzp;
-        double a_ov = 0.0, a_t2 = 0.0;
-        for (int r = 0; r < o; r++) {
-            for (int zl = 0; zl < pb.Tz; zl++) {
-                const int z = pb.Z0 + zl;
-                double vb = 0.0;
-                if (active) {
-                    const int occ[3] = {p, q, r}, vir[3] = {x, y, z};
-                    double wb = 0.0;
+        const double ovv = A.ovov[iov], t2v = A.t2[it2];
+        const double *rv = A.B0 + pb.soff + (long long)pr * oTz;
+        const double *rd = A.B2 + pb.soff + (long long)pr * oTz;
+        double s_ov = 0.0, s_t2 = 0.0, s_d = 0.0;
 #pragma unroll
-                    for (int s = 0; s < 6; s++) {
-                        int ps[3];
-                        perm_of(s, ps);
-                        const long long off = lno_off(A, occ[ps[0]], occ[ps[1]], occ[ps[2]], vir[ps[0]], vir[ps[1]],
-                                                      vir[ps[2]]);
-                        wb += A.B0[off];
-                        vb += A.B1[off];
-                    }
-                    A.SW[swrow + (long long)r * pb.Tz + zl] = wb;
-                    a_ov += vb * A.t1[(long long)r * v + z];
-                    a_t2 += vb * A.fvo[(long long)z * o + r];
-                }
-                // every lane has the same (r, z)
-                const double w1 = lno_warp_sum(vb * ovv), w2 = lno_warp_sum(vb * t2v);
-                if (lane == 0) {
-                    if (w1 != 0.0) atomicAdd(&s_t1[r][zl], w1);
-                    if (w2 != 0.0) atomicAdd(&s_fv[r][zl], w2);
+        for (int m = 0; m < M; m++) {
+            const int k = lane + 32 * m;
+            if (k < oTz) {
+                const int r = k / pb.Tz, z = pb.Z0 + k % pb.Tz;
+                const double vb = rv[k], db = rd[k];
+                s_ov += vb * __ldg(&A.t1[r * v + z]);
+                s_t2 += vb * __ldg(&A.fvo[z * o + r]);
+                s_d += db;
+                a1[m] += vb * ovv;
+                af[m] += vb * t2v;
+                ar[m] += db;
+            }
+        }
+        s_ov = lno_warp_sum(s_ov);
+        s_t2 = lno_warp_sum(s_t2);
+        s_d = lno_warp_sum(s_d);
+        if (lane == 0) {
+            if (s_ov != 0.0) atomicAdd(&A.ovov_bar[iov], s_ov);
+            if (s_t2 != 0.0) atomicAdd(&A.t2_bar[it2], s_t2);
+            s_occ[warp][p] += s_d;
+            s_occ[warp][q] += s_d;
+            s_vir[warp][0][xl] -= s_d;
+            s_vir[warp][1][yl] -= s_d;
+        }
+    }
+    // combine the warps' register sums (one warp at a time: no atomics)
+    for (int w = 0; w < kLnoThreads / 32; w++) {
+        if (warp == w) {
+#pragma unroll
+            for (int m = 0; m < M; m++) {
+                const int k = lane + 32 * m;
+                if (k < oTz) {
+                    s_t1[k] += a1[m];
+                    s_fv[k] += af[m];
+                    s_rz[k] += ar[m];
                 }
             }
         }
-        if (active) {
-            if (a_ov != 0.0) atomicAdd(&A.ovov_bar[iov], a_ov);
-            if (a_t2 != 0.0) atomicAdd(&A.t2_bar[it2], a_t2);
+        __syncthreads();
+    }
+    for (int k = threadIdx.x; k < oTz; k += blockDim.x) {
+        const int r = k / pb.Tz, z = pb.Z0 + k % pb.Tz;
+        if (s_t1[k] != 0.0) atomicAdd(&A.t1_bar[(long long)r * v + z], s_t1[k]);
+        if (s_fv[k] != 0.0) atomicAdd(&A.fvo_bar[(long long)z * o + r], s_fv[k]);
+        if (s_rz[k] != 0.0) {
+            atomicAdd(&A.mo_bar[r], s_rz[k]);
+            atomicAdd(&A.mo_bar[o + z], -s_rz[k]);
         }
     }
-    __syncthreads();
-    for (int e = threadIdx.x; e < o * pb.Tz; e += blockDim.x) {
-        const int r = e / pb.Tz, zl = e % pb.Tz;
-        if (s_t1[r][zl] != 0.0) atomicAdd(&A.t1_bar[(long long)r * v + pb.Z0 + zl], s_t1[r][zl]);
-        if (s_fv[r][zl] != 0.0) atomicAdd(&A.fvo_bar[(long long)(pb.Z0 + zl) * o + r], s_fv[r][zl]);
+    for (int k = threadIdx.x; k < o; k += blockDim.x) {
+        double t = 0.0;
+        for (int w = 0; w < kLnoThreads / 32; w++) t += s_occ[w][k];
+        if (t != 0.0) atomicAdd(&A.mo_bar[k], t);
+    }
+    for (int k = threadIdx.x; k < 2 * kLnoMaxTv; k += blockDim.x) {
+        const int role = k / kLnoMaxTv, kk = k % kLnoMaxTv;
+        const int len = role == 0 ? pb.Tx : pb.Ty;
+        if (kk >= len) continue;
+        double t = 0.0;
+        for (int w = 0; w < kLnoThreads / 32; w++) t += s_vir[w][role][kk];
+        if (t != 0.0) atomicAdd(&A.mo_bar[o + (role == 0 ? pb.X0 : pb.Y0) + kk], t);
     }
 }
 
-#undef LNO_FOR_POSITIONS
-#undef LNO_FOR_PAIR_ROWS
+inline size_t lno_tile_smem() { return 2 * 36 * kLnoRegion * sizeof(double); }
 
 }  // namespace tb

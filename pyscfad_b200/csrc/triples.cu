@@ -42,10 +42,12 @@ static int g_kseg_f1 = 1;  // same for the W contraction
 // ---------------------------------------------------------------------------
 // optional per-kernel-class timing with CUDA events (on the launch stream)
 // ---------------------------------------------------------------------------
-enum ProfCat { P_PREP = 0, P_F1, P_F2, P_B1A, P_B1B, P_B1C, P_B1D, P_FOLD, P_LNO, P_NCAT };
+enum ProfCat { P_PREP = 0, P_F1, P_F2, P_B1A, P_B1B, P_B1C, P_B1D, P_FOLD, P_LNO, P_LNO_PROJ, P_LNO_ADJ, P_LNO_VG,
+               P_NCAT };
 static const char *kProfNames[P_NCAT] = {"prep", "f1_contract", "f2_epilogue",
                                          "b1a_ovvv_grad", "b1b_t2_grad", "b1c_ovoo_grad",
-                                         "b1d_t2_ooov_grad", "fold", "lno_epilogue"};
+                                         "b1d_t2_ooov_grad", "fold", "lno_tile_fwd", "lno_projection",
+                                         "lno_tile_adj", "lno_vgrad"};
 struct ProfRec {
     int cat;
     cudaEvent_t a, b;
@@ -148,7 +150,7 @@ int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan
     if (nocc < 1 || nvir < 1 || nocc > kMaxCols || nvir > 32767) return TRIPLES_ERR_INVALID_ARGUMENT;
     if (precision < TRIPLES_PRECISION_FP64 || precision > TRIPLES_PRECISION_MIXED_BF16)
         return TRIPLES_ERR_INVALID_ARGUMENT;
-    if (lno && (precision != TRIPLES_PRECISION_FP64 || nocc > kLnoMaxO)) return TRIPLES_ERR_UNSUPPORTED;
+    if (lno && nocc > kLnoMaxO) return TRIPLES_ERR_UNSUPPORTED;
     P = Plan{};
     P.lno = lno ? 1 : 0;
     P.prec = precision;
@@ -347,7 +349,7 @@ __global__ void k_make_scales(Ctrl *ctrl, int scaled) {
 // chunk (|Z| <= 12 max|X|, |X| <= 6 max|w| + 3 max|v|, |R WW| <= 72 max|w|,
 // orbit weight <= 2).  Resets the running max |w| for the next chunk.
 __global__ void k_chunk_scale(Ctrl *ctrl, const double *__restrict__ mo_e, int o, int a0, int na, int b0,
-                              int nb, int c0, int nc, double ybar, int scaled) {
+                              int nb, int c0, int nc, double ybar, int scaled, int lno) {
     __shared__ double s_min[3], s_maxo;
     const double inf = 1e300;
     if (threadIdx.x < 4) {
@@ -368,7 +370,11 @@ __global__ void k_chunk_scale(Ctrl *ctrl, const double *__restrict__ mo_e, int o
         const double mw = (double)__uint_as_float(ctrl->wmax_bits);
         const double mv = __longlong_as_double((long long)ctrl->absmax[3]) * __longlong_as_double((long long)ctrl->absmax[4]) +
                           __longlong_as_double((long long)ctrl->absmax[2]) * __longlong_as_double((long long)ctrl->absmax[5]);
-        double bound = 2.0 * fabs(ybar) * (144.0 * mw + 36.0 * mv) / (dmin > 1e-300 ? dmin : 1e-300);
+        // |wbar| <= 6 |WWbar|; with the LNO projector (row / column abs sums nr, nc)
+        // WWbar = P^T(ybar Q / 3) + r3^T(ybar P(WW) / (3 D)), |Q| <= 12 (6 mw + 3 mv) / dmin;
+        // nr = nc = 1 is the canonical bound
+        const double nr = lno ? ctrl->lno_norm[0] : 1.0, ncl = lno ? ctrl->lno_norm[1] : 1.0;
+        double bound = 2.0 * fabs(ybar) * (72.0 * (nr + ncl) * mw + 36.0 * nr * mv) / (dmin > 1e-300 ? dmin : 1e-300);
         ctrl->wscale = scaled ? pow2_scale(bound) : 1.0;
         ctrl->wmax_bits = 0u;
     }
@@ -388,6 +394,30 @@ __device__ __forceinline__ void split16<__nv_bfloat16>(double xs, __nv_bfloat16 
 }
 
 // A1h[h][y][p][x][f] = split(ovvv[p,x,f,y] * sA), f < Kp8 (zero beyond v)
+// max abs row sum and max abs column sum of the LNO projector mat[o,o]
+__global__ void k_lno_mat_norms(const double *__restrict__ mat, int o, Ctrl *ctrl) {
+    __shared__ double s_r[kLnoMaxO], s_c[kLnoMaxO];
+    for (int i = threadIdx.x; i < o; i += blockDim.x) {
+        double r = 0.0, c = 0.0;
+        for (int k = 0; k < o; k++) {
+            r += fabs(mat[i * o + k]);
+            c += fabs(mat[k * o + i]);
+        }
+        s_r[i] = r;
+        s_c[i] = c;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double mr = 0.0, mc = 0.0;
+        for (int i = 0; i < o; i++) {
+            mr = fmax(mr, s_r[i]);
+            mc = fmax(mc, s_c[i]);
+        }
+        ctrl->lno_norm[0] = mr;
+        ctrl->lno_norm[1] = mc;
+    }
+}
+
 template <typename H>
 __global__ void k_prep_A1h(const double *__restrict__ ovvv, int packed, Dims d, int Kp8,
                            const Ctrl *ctrl, H *__restrict__ out) {
@@ -816,11 +846,40 @@ static int num_sms() {
 
 // LNO chunk epilogue (FP64): energy of the projected amplitudes and, with
 // want_grad, mat_bar, the D and V-term gradients and the FP64 Wbar staging
-// that the adjoint contractions read next.
+// that the adjoint contractions read next (four passes, see lno.cuh).
+template <typename StageT>
 static int lno_chunk(const Plan &P, const ChunkDesc &ch, cudaStream_t st, const TriplesIO &io, char *ws,
-                     Ctrl *ctrl, const double *S, double *SW) {
+                     Ctrl *ctrl, const StageT *S, void *SW, const int *ijk, int split) {
+    {
+        constexpr int kMaxDev = 64;
+        static bool ready[kMaxDev] = {};
+        int dev = 0;
+        TB_CUDA(cudaGetDevice(&dev));
+        if (dev < 0 || dev >= kMaxDev) return TRIPLES_ERR_UNSUPPORTED;
+        if (!ready[dev]) {
+            const int ts = (int)lno_tile_smem();
+            TB_CUDA(cudaFuncSetAttribute(k_lno_tile_fwd<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, ts));
+            TB_CUDA(cudaFuncSetAttribute(k_lno_tile_fwd<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, ts));
+            TB_CUDA(cudaFuncSetAttribute(k_lno_tile_adj<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, ts));
+            TB_CUDA(cudaFuncSetAttribute(k_lno_tile_adj<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, ts));
+            TB_CUDA(cudaFuncSetAttribute(k_lno_tile_adj<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, ts));
+            static LnoTables tabs;
+            lno_build_tables(tabs);
+            TB_CUDA(cudaMemcpyToSymbol(c_lno_tab, &tabs, sizeof(tabs)));
+            static LnoPattern pats[16];
+            lno_build_patterns(pats);
+            TB_CUDA(cudaMemcpyToSymbol(c_lno_pat, pats, sizeof(pats)));
+            const int ps = (int)lno_proj_smem(kLnoMaxO);
+            TB_CUDA(cudaFuncSetAttribute(k_lno_proj<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps));
+            TB_CUDA(cudaFuncSetAttribute(k_lno_proj<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps));
+            TB_CUDA(cudaFuncSetAttribute(k_lno_proj<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps));
+            TB_CUDA(cudaFuncSetAttribute(k_lno_proj<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps));
+            ready[dev] = true;
+        }
+    }
+    const Dims &d = P.d;
     LnoArgs A;
-    A.d = P.d;
+    A.d = d;
     A.ch = ch;
     for (int k = 0; k < 27; k++) A.tau_of[k] = 0;
     for (int sx = 0; sx < 3; sx++)
@@ -829,6 +888,26 @@ static int lno_chunk(const Plan &P, const ChunkDesc &ch, cudaStream_t st, const 
                 for (int t = 0; t < ch.nperm; t++)
                     if (ch.pb[t].bx == ch.blk[sx] && ch.pb[t].by == ch.blk[sy] && ch.pb[t].bz == ch.blk[sz])
                         A.tau_of[(sx * 3 + sy) * 3 + sz] = (signed char)t;
+    // virtual sub-block triples, one per orbit of orderings
+    A.nsub = 0;
+    int nsb[3];
+    for (int t = 0; t < 3; t++) nsb[t] = (ch.nabc[t] + kLnoSB - 1) / kLnoSB;
+    for (int sa = 0; sa < nsb[0]; sa++)
+        for (int sb = 0; sb < nsb[1]; sb++) {
+            if (ch.blk[0] == ch.blk[1] && sb > sa) continue;
+            for (int sc = 0; sc < nsb[2]; sc++) {
+                if (ch.blk[1] == ch.blk[2] && sc > sb) continue;
+                if (A.nsub >= kLnoMaxSub) return TRIPLES_ERR_UNSUPPORTED;
+                LnoSub &u = A.sub[A.nsub++];
+                const int si[3] = {sa, sb, sc};
+                for (int t = 0; t < 3; t++) {
+                    u.st[t] = ch.base[t] + si[t] * kLnoSB;
+                    const int len = ch.nabc[t] - si[t] * kLnoSB;
+                    u.len[t] = len < kLnoSB ? len : kLnoSB;
+                }
+            }
+        }
+    A.ijk = ijk;
     A.S = S;
     A.B0 = (double *)(ws + P.off_L[0]);
     A.B1 = (double *)(ws + P.off_L[1]);
@@ -836,29 +915,66 @@ static int lno_chunk(const Plan &P, const ChunkDesc &ch, cudaStream_t st, const 
     A.B3 = (double *)(ws + P.off_L[3]);
     A.mat = io.mat; A.mo_e = io.mo_energy; A.t1 = io.t1; A.t2 = io.t2; A.ovov = io.ovov; A.fvo = io.fvo;
     A.SW = SW;
+    A.wscale = &ctrl->wscale;
     A.mat_bar = io.mat_bar; A.mo_bar = io.mo_energy_bar; A.t1_bar = io.t1_bar; A.t2_bar = io.t2_bar;
     A.ovov_bar = io.ovov_bar; A.fvo_bar = io.fvo_bar;
     A.ybar = io.ybar;
+    A.want_grad = P.want_grad;
     A.part = (double *)(ws + P.off_lpart);
-    long long maxpos = 0;
+    long long maxcols = 0, maxrows = 0;
     for (int t = 0; t < ch.nperm; t++) {
-        const long long np = (long long)P.d.o * P.d.o * P.d.o * ch.pb[t].Tx * ch.pb[t].Ty * ch.pb[t].Tz;
-        if (np > maxpos) maxpos = np;
+        const long long rows = (long long)d.o * d.o * ch.pb[t].Tx * ch.pb[t].Ty;
+        if (rows * d.o * ch.pb[t].Tz > maxcols) maxcols = rows * d.o * ch.pb[t].Tz;
+        if (rows > maxrows) maxrows = rows;
     }
-    long long gx = (maxpos + kLnoThreads - 1) / kLnoThreads;
-    if (gx > kLnoGrid) gx = kLnoGrid;
-    const dim3 grid((unsigned)gx, (unsigned)ch.nperm);
-    TB_KLAUNCH(P_LNO, k_lno_ww<<<grid, kLnoThreads, 0, st>>>(A));
-    TB_KLAUNCH(P_LNO, k_lno_q<<<grid, kLnoThreads, 0, st>>>(A));
-    TB_KLAUNCH(P_LNO, k_lno_project<<<grid, kLnoThreads, 0, st>>>(A, A.B0, A.B3, 1, 1.0));
-    TB_KLAUNCH(P_LNO, k_lno_energy<<<grid, kLnoThreads, 0, st>>>(A));
-    TB_KLAUNCH(P_LNO, k_f2_energy_sum<<<1, 256, 0, st>>>(A.part, (int)gx * ch.nperm, &ctrl->e_acc));
+    auto clampg = [](long long n) { return (unsigned)(n < kLnoGrid ? (n > 0 ? n : 1) : kLnoGrid); };
+    const dim3 gtile((unsigned)P.n_ijk, (unsigned)A.nsub);
+    // streaming passes: a few full waves of two blocks per SM over the chunk's
+    // orderings (their per-block reductions end in global atomics on a few
+    // hundred entries, so the grid stays small)
+    const long long wave = (long long)kLnoWaves * 2 * num_sms() / ch.nperm;
+    auto clampw = [&](long long n) { return clampg(n < wave ? n : wave); };
+    const dim3 gproj(clampw((maxcols / d.o + kLnoTile - 1) / kLnoTile), (unsigned)ch.nperm);
+    TB_KLAUNCH(P_LNO, k_lno_tile_fwd<StageT><<<gtile, kLnoThreads, lno_tile_smem(), st>>>(A));
+    {
+        const size_t ps = lno_proj_smem(d.o);
+        if (d.o <= 8)
+            TB_KLAUNCH(P_LNO_PROJ, k_lno_proj<1><<<gproj, kLnoThreads, ps, st>>>(A));
+        else if (d.o <= 16)
+            TB_KLAUNCH(P_LNO_PROJ, k_lno_proj<2><<<gproj, kLnoThreads, ps, st>>>(A));
+        else if (d.o <= 32)
+            TB_KLAUNCH(P_LNO_PROJ, k_lno_proj<4><<<gproj, kLnoThreads, ps, st>>>(A));
+        else
+            TB_KLAUNCH(P_LNO_PROJ, k_lno_proj<8><<<gproj, kLnoThreads, ps, st>>>(A));
+    }
+    TB_KLAUNCH(P_LNO_PROJ, k_f2_energy_sum<<<1, 256, 0, st>>>(A.part, (int)(gproj.x * gproj.y), &ctrl->e_acc));
     if (!P.want_grad) return TRIPLES_OK;
-    TB_KLAUNCH(P_LNO, k_lno_matbar<<<grid, kLnoThreads, 0, st>>>(A));
-    TB_KLAUNCH(P_LNO, k_lno_zbar<<<grid, kLnoThreads, 0, st>>>(A));
-    TB_KLAUNCH(P_LNO, k_lno_project<<<grid, kLnoThreads, 0, st>>>(A, A.B2, A.B0, 0, io.ybar / 3.0));
-    TB_KLAUNCH(P_LNO, k_lno_xbar<<<grid, kLnoThreads, 0, st>>>(A));
-    TB_KLAUNCH(P_LNO, k_lno_scatter<<<grid, kLnoThreads, 0, st>>>(A));
+    if (split != 0)   // fp16: power-of-two scale of the split Wbar; bf16: scale 1 (both read by the contractions)
+        TB_KLAUNCH(P_PREP, k_chunk_scale<<<1, 32, 0, st>>>(ctrl, io.mo_energy, d.o, ch.base[0], ch.nabc[0], ch.base[1],
+                                                           ch.nabc[1], ch.base[2], ch.nabc[2], io.ybar,
+                                                           split == 1 ? 1 : 0, 1));
+    if (split == 0)
+        TB_KLAUNCH(P_LNO_ADJ, k_lno_tile_adj<0><<<gtile, kLnoThreads, lno_tile_smem(), st>>>(A));
+    else if (split == 1)
+        TB_KLAUNCH(P_LNO_ADJ, k_lno_tile_adj<1><<<gtile, kLnoThreads, lno_tile_smem(), st>>>(A));
+    else
+        TB_KLAUNCH(P_LNO_ADJ, k_lno_tile_adj<2><<<gtile, kLnoThreads, lno_tile_smem(), st>>>(A));
+    const dim3 gv(clampw((maxrows + kLnoThreads / 32 - 1) / (kLnoThreads / 32)), (unsigned)ch.nperm);
+    int maxTz = 0;
+    for (int t = 0; t < ch.nperm; t++) maxTz = ch.pb[t].Tz > maxTz ? ch.pb[t].Tz : maxTz;
+    const int per_lane = (d.o * maxTz + 31) / 32;
+    if (per_lane <= 2)
+        TB_KLAUNCH(P_LNO_VG, k_lno_vgrad<2><<<gv, kLnoThreads, 0, st>>>(A));
+    else if (per_lane <= 4)
+        TB_KLAUNCH(P_LNO_VG, k_lno_vgrad<4><<<gv, kLnoThreads, 0, st>>>(A));
+    else if (per_lane <= 8)
+        TB_KLAUNCH(P_LNO_VG, k_lno_vgrad<8><<<gv, kLnoThreads, 0, st>>>(A));
+    else if (per_lane <= 12)
+        TB_KLAUNCH(P_LNO_VG, k_lno_vgrad<12><<<gv, kLnoThreads, 0, st>>>(A));
+    else if (per_lane <= 16)
+        TB_KLAUNCH(P_LNO_VG, k_lno_vgrad<16><<<gv, kLnoThreads, 0, st>>>(A));
+    else
+        TB_KLAUNCH(P_LNO_VG, k_lno_vgrad<32><<<gv, kLnoThreads, 0, st>>>(A));
     return TRIPLES_OK;
 }
 
@@ -913,7 +1029,10 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
         TB_CUDA(cudaMemsetAsync(io.t2_bar, 0, o * o * v * v * sizeof(double), st));
         TB_CUDA(cudaMemsetAsync(io.ovov_bar, 0, o * v * o * v * sizeof(double), st));
         TB_CUDA(cudaMemsetAsync(io.fvo_bar, 0, v * o * sizeof(double), st));
-        if (P.lno) TB_CUDA(cudaMemsetAsync(io.mat_bar, 0, o * o * sizeof(double), st));
+        if (P.lno) {
+            TB_CUDA(cudaMemsetAsync(io.mat_bar, 0, o * o * sizeof(double), st));
+            if (mixed) TB_KLAUNCH(P_PREP, k_lno_mat_norms<<<1, 64, 0, st>>>(io.mat, d.o, ctrl));
+        }
     }
 
     // FP64 operand layouts (used by the FP64 contractions only)
@@ -1062,7 +1181,7 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                 }
                 if (P.lno) {
                     // projected energy: whole-chunk epilogue instead of the orbit tiles
-                    const int rc = lno_chunk(P, ch, st, io, ws, ctrl, (const double *)S, (double *)SW);
+                    const int rc = lno_chunk<StageT>(P, ch, st, io, ws, ctrl, S, SW, ijk, mixed ? (bf16 ? 2 : 1) : 0);
                     if (rc != TRIPLES_OK) return rc;
                 } else {
                     // F2: energy (+ adjoint of the raw amplitudes)
@@ -1094,7 +1213,7 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                     if (mixed && P.want_grad)
                         TB_KLAUNCH(P_PREP, k_chunk_scale<<<1, 32, 0, st>>>(ctrl, io.mo_energy, d.o, ch.base[0], ch.nabc[0],
                                                                            ch.base[1], ch.nabc[1], ch.base[2], ch.nabc[2],
-                                                                           io.ybar, bf16 ? 0 : 1));
+                                                                           io.ybar, bf16 ? 0 : 1, 0));
                     F.wscale = &ctrl->wscale;
                     F.ybar = io.ybar;
                     F.want_grad = P.want_grad;

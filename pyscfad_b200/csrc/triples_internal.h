@@ -23,6 +23,7 @@ struct Ctrl {
     double wscale;                // per-chunk power-of-two scale of the split Wbar
     unsigned long long absmax[6]; // bit patterns of max |ovvv|, |ovoo|, |t2|, |ovov|, |t1|, |fvo|
     unsigned wmax_bits;           // bit pattern of max |W| of the current chunk (F1)
+    double lno_norm[2];           // LNO projector: max abs row sum, max abs column sum
 };
 
 static_assert(sizeof(Ctrl) <= kCtrlBytes, "control block too large");
@@ -30,7 +31,7 @@ static_assert(sizeof(Ctrl) <= kCtrlBytes, "control block too large");
 struct Plan {
     Dims d;
     int prec, want_grad, packed;
-    int lno;         // projected (LNO) energy: FP64 only, chunk work arrays off_L
+    int lno;         // projected (LNO) energy: whole-chunk work arrays off_L
     int nb;          // number of virtual blocks
     int n_ijk;       // occupied triplet representatives i >= j >= k
     int max_items;   // largest |A||B||C| over chunks

@@ -158,7 +158,7 @@ def lno_workspace_size(nocc, nvir, packed=True, want_grad=True, precision="fp64"
 def lno_energy(mat, mo_energy, t1, t2, ovoo, ovov, ovvv, fvo, precision="fp64", device=None,
                stream=None, check=True) -> torch.Tensor:
     """LNO (T) energy with the occupied projector mat[o,o] (= ulo^T ulo,
-    pyscfad/lno/ccsd_t.py:42); mat = identity gives E(T).  FP64 only."""
+    pyscfad/lno/ccsd_t.py:42); mat = identity gives E(T).  nocc <= 64."""
     lib = _lib.load()
     device = torch.device(device or (t1.device if isinstance(t1, torch.Tensor) and t1.is_cuda else "cuda"))
     args = [_as_dev(a, device) for a in (mat, mo_energy, t1, t2, ovoo, ovov, ovvv, fvo)]
@@ -168,7 +168,7 @@ def lno_energy(mat, mo_energy, t1, t2, ovoo, ovov, ovvv, fvo, precision="fp64", 
     prec = _lib.PRECISION[precision]
     nbytes = lib.triples_lno_workspace_size(prec, o, v, int(packed), 0)
     if nbytes == 0:
-        raise _lib.TriplesError(4 if prec != 0 or o > 64 else 1, "triples_lno_workspace_size")
+        raise _lib.TriplesError(4 if o > 64 else 1, "triples_lno_workspace_size")
     ws = _workspace(nbytes, device)
     e = torch.zeros((), dtype=torch.float64, device=device)
     st = stream if stream is not None else torch.cuda.current_stream(device)
@@ -193,7 +193,7 @@ def lno_energy_vjp(mat, mo_energy, t1, t2, ovoo, ovov, ovvv, fvo, ybar=1.0, prec
     prec = _lib.PRECISION[precision]
     nbytes = lib.triples_lno_workspace_size(prec, o, v, int(packed), 1)
     if nbytes == 0:
-        raise _lib.TriplesError(4 if prec != 0 or o > 64 else 1, "triples_lno_workspace_size")
+        raise _lib.TriplesError(4 if o > 64 else 1, "triples_lno_workspace_size")
     ws = _workspace(nbytes, device)
     e = torch.zeros((), dtype=torch.float64, device=device)
     keys = ("mat",) + KEYS

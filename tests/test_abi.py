@@ -63,16 +63,16 @@ def test_status_strings():
 
 
 def test_lno_plan_limits():
-    """The LNO path is FP64 with nocc <= 64; other requests are refused on the host."""
+    """The LNO path takes nocc <= 64 in every precision; larger problems are refused on the host."""
     lib = _lib.load()
     a = lib.triples_lno_workspace_size(0, 5, 19, 1, 0)
     b = lib.triples_lno_workspace_size(0, 5, 19, 1, 1)
     assert 0 < a < b
     assert b > lib.triples_workspace_size(0, 5, 19, 1, 1)        # whole-chunk work arrays
-    assert lib.triples_lno_workspace_size(1, 5, 19, 1, 1) == 0   # mixed precision
+    assert lib.triples_lno_workspace_size(1, 5, 19, 1, 1) > 0    # mixed precision
     assert lib.triples_lno_workspace_size(0, 65, 19, 1, 1) == 0  # nocc > 64
     null = None
-    rc = lib.triples_lno_energy(null, 1, 5, 19, 1, *([null] * 8), null, 0, null)
+    rc = lib.triples_lno_energy(null, 0, 65, 19, 1, *([null] * 8), null, 0, null)
     assert rc == 4   # TRIPLES_ERR_UNSUPPORTED
     rc = lib.triples_lno_energy(null, 0, 5, 19, 1, *([ctypes.c_void_p(16)] * 8), ctypes.c_void_p(16), 8,
                                 ctypes.c_void_p(16))

@@ -24,10 +24,10 @@ def _relerr(a, b):
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-7))
 
 
-def _run(inp, mat, packed=True, ybar=1.0):
+def _run(inp, mat, packed=True, ybar=1.0, precision="fp64"):
     ovvv = inp.ovvv_tril() if packed else inp.ovvv
     e, g = triples.lno_energy_vjp(mat, inp.mo_energy, inp.t1, inp.t2, inp.ovoo, inp.ovov, ovvv, inp.fvo,
-                                  ybar=ybar, device="cuda")
+                                  ybar=ybar, precision=precision, device="cuda")
     torch.cuda.synchronize()
     return float(e), {k: v.cpu().numpy() for k, v in g.items()}
 
@@ -47,6 +47,37 @@ def test_lno_matches_reference_golden(name, packed):
     for k in KEYS:
         ref = z["cot_ovvv_tril"] if (k == "ovvv" and packed) else g_ref[k]
         assert _relerr(g[k], ref) < G_RTOL, k
+
+
+# tensor-core contractions on 16-bit hi/lo splits, FP64 epilogue: the
+# tolerances of the canonical mixed path
+MIXED_TOL = {"mixed": (1e-6, 1e-5), "mixed_bf16": (1e-4, 1e-3)}
+
+
+@pytest.mark.parametrize("name", ["lno_o4v9", "lno_o5v19"])
+@pytest.mark.parametrize("precision", ["mixed", "mixed_bf16"])
+def test_lno_mixed_matches_reference_golden(name, precision):
+    inp, e_ref, g_ref, z = G.load(name)
+    te, tg = MIXED_TOL[precision]
+    e, g = _run(inp, z["in_mat"], packed=True, precision=precision)
+    assert abs(e - e_ref) <= te * abs(e_ref), (e, e_ref)
+    for k in KEYS:
+        ref = z["cot_ovvv_tril"] if k == "ovvv" else g_ref[k]
+        assert _relerr(g[k], ref) < tg, k
+
+
+def test_lno_mixed_full_projector():
+    """Mixed path with a full non-symmetric projector (scale bound with row/column sums != 1)."""
+    inp = make_inputs(7, 24, 40, seed=3, fvo_sigma=1e-3)
+    mat = np.random.default_rng(7).normal(size=(7, 7)) * 0.8
+    e_ref, g_ref = _run(inp, mat, packed=False)
+    e, g = _run(inp, mat, packed=False, precision="mixed")
+    assert abs(e - e_ref) <= 1e-6 * abs(e_ref)
+    for k in KEYS:
+        assert _relerr(g[k], g_ref[k]) < 1e-5, k
+    e0 = triples.lno_energy(mat, inp.mo_energy, inp.t1, inp.t2, inp.ovoo, inp.ovov, inp.ovvv, inp.fvo,
+                            precision="mixed", device="cuda")
+    assert abs(float(e0) - e) <= 1e-12 * abs(e)
 
 
 def test_lno_energy_only_matches_vjp_energy():
@@ -103,7 +134,7 @@ def test_lno_mirror_kernel_autograd():
     mo, fvo, ovoo, ovov, ovvv = t(inp.mo_energy), t(inp.fvo), t(inp.ovoo), t(inp.ovov), t(inp.ovvv_tril())
     e = L._ccsd_t_energy(mat, t1T, t2T, mo, fvo, ovoo, ovov, ovvv, 4000)
     (2.0 * e).backward()
-    assert abs(float(e) - e_ref) <= E_RTOL * abs(e_ref)
+    assert abs(float(e.detach()) - e_ref) <= E_RTOL * abs(e_ref)
     assert _relerr(mat.grad.cpu().numpy(), 2 * g_ref["mat"]) < G_RTOL
     assert _relerr(t1T.grad.cpu().numpy(), 2 * g_ref["t1"].T) < G_RTOL
     assert _relerr(t2T.grad.cpu().numpy(), 2 * g_ref["t2"].transpose(2, 3, 1, 0)) < G_RTOL

@@ -325,6 +325,152 @@ def run_accuracy(args, o, v, naux):
     print(json.dumps(out))
 
 
+# ---------------------------------------------------------------------------
+# LNO fragment (T): projector on the first occupied index
+# ---------------------------------------------------------------------------
+LNO_METRIC = "LNO (T) E+VJP TFLOP/s (projected first occupied index), B200 vs reference CPU kernels"
+# algorithmic bytes per raw amplitude position of each LNO epilogue pass
+# (sz = staging element size: 8 FP64, 4 mixed): tile forward reads w, writes
+# WW and Q; the projection reads WW, Q and writes Zbar, Dbar, P^T(Wtbar);
+# tile adjoint reads Zbar, P^T(Wtbar), writes vbar and the Wbar operand
+# (FP64, or two 16-bit halves); V gradients read vbar, Dbar.
+def lno_pass_bytes(sz):
+    return {"lno_tile_fwd": sz + 16, "lno_projection": 40, "lno_tile_adj": 16 + 8 + (8 if sz == 8 else 4),
+            "lno_vgrad": 16}
+
+
+def run_lno(args, o, v, naux):
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    from pyscfad_b200 import _lib, triples
+    from pyscfad_b200.synthetic import make_inputs_torch
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    lib = _lib.load()
+    inp = make_inputs_torch(o, v, naux, seed=args.seed, device=dev)
+    il, jl = torch.tril_indices(v, v, device=dev)
+    inp["ovvv"] = inp["ovvv"][:, :, il, jl].contiguous()
+    # projector of a fragment with half the occupied orbitals: mat = ulo^T ulo
+    rng = np.random.default_rng(1000 + args.seed)
+    ulo = np.linalg.qr(rng.normal(size=(o, o)))[0][: max(1, o // 2)]
+    mat = torch.tensor(ulo.T @ ulo, dtype=torch.float64, device=dev)
+    dev_args = [mat] + [inp[k] for k in triples.KEYS]
+
+    def step(a):
+        return triples.lno_energy_vjp(*a, ybar=1.0, precision=args.precision, device=dev, check=False)
+
+    for _ in range(args.warmup):
+        e, g = step(dev_args)
+    torch.cuda.synchronize()
+    _lib.check(triples.device_status(dev), "warm-up")
+    e_val = float(e)
+    del g
+    clocks = ClockSampler(0)
+    torch.cuda.synchronize()
+    clocks.start()
+    lib.triples_profile_enable(1)
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record()
+    for _ in range(args.steps):
+        e, g = step(dev_args)
+    s1.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ncat = 16
+    ms, cnt = (ctypes.c_double * ncat)(), (ctypes.c_int * ncat)()
+    ncat = lib.triples_profile_read(ncat, ms, cnt)
+    lib.triples_profile_enable(0)
+    prof = {lib.triples_profile_name(i).decode(): (ms[i], cnt[i]) for i in range(ncat)}
+    t_dev = s0.elapsed_time(s1) / 1e3
+    _lib.check(triples.device_status(dev), "timed steps")
+    del g
+    flops = algorithmic_flops(o, v)["step"]
+    value = args.steps * flops / t_dev / 1e12
+
+    host_in = [a.cpu().pin_memory() for a in dev_args]
+    h2d = sum(a.numel() * a.element_size() for a in host_in)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    grads_host, d2h = None, 0
+    for _ in range(args.steps):
+        dev_in = [a.to(dev, non_blocking=True) for a in host_in]
+        ee, gg = step(dev_in)
+        if grads_host is None:
+            grads_host = {k: torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for k, t in gg.items()}
+            e_host = torch.empty((), dtype=torch.float64, pin_memory=True)
+        e_host.copy_(ee, non_blocking=True)
+        for k, t in gg.items():
+            grads_host[k].copy_(t, non_blocking=True)
+        d2h = 8 + sum(t.numel() * t.element_size() for t in gg.values())
+        del dev_in, gg
+    e1.record()
+    torch.cuda.synchronize()
+    t_e2e = e0.elapsed_time(e1) / 1e3
+
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except (OSError, ValueError):
+        pass
+    hpeak, hnote = (float(peaks["hbm_gbs"]), "of measured (copy)") if "hbm_gbs" in peaks else (6650.0, "of fallback")
+    positions = float(o) ** 3 * float(v) ** 3
+    pbytes = lno_pass_bytes(8 if args.precision == "fp64" else 4)
+    total_ms = sum(m for m, _ in prof.values()) or 1.0
+    classes = {}
+    for k, b in pbytes.items():
+        m, c = prof.get(k, (0.0, 0))
+        if c <= 0 or m <= 0:
+            continue
+        ach = b * positions * args.steps / (m / 1e3) / 1e9
+        classes[k] = {"bound": "hbm", "achieved": ach, "peak": hpeak, "unit": "GB/s", "frac": ach / hpeak,
+                      "kernel": k, "launches": c, "avg_launch_ms": m / c, "share": m / total_ms,
+                      "bytes_per_position": b}
+    roof = None
+    if classes:
+        dom = max(classes, key=lambda k: prof[k][0])
+        roof = dict(classes[dom])
+        roof["traffic"] = load_traffic("lno_" + args.workload, args.precision).get(dom)
+        roof["peak_note"] = hnote
+        roof["classes"] = {k: {kk: (round(vv, 4) if isinstance(vv, float) else vv) for kk, vv in c.items()
+                               if kk in ("achieved", "frac", "share")} for k, c in classes.items()}
+    line = {
+        "metric": LNO_METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_dev / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else (
+            "fp16x3-split f32acc, f64 LNO epilogue" if args.precision == "mixed" else "bf16x3-split f32acc, f64 LNO epilogue"),
+        "data": DATA + "; projector mat = ulo^T ulo, ulo = o/2 orthonormal rows (seeded)",
+        "config": {"workload": "lno_" + args.workload, "nocc": o, "nvir": v, "naux": naux,
+                   "precision": args.precision, "nlo": max(1, o // 2), "l2": "chunk work arrays larger than L2",
+                   "e_t": e_val},
+        "e2e": {"value": args.steps * flops / t_e2e / 1e12, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(sum(c for _, c in prof.values())),
+        "kernel_ms": {k: round(m, 3) for k, (m, _) in prof.items()},
+        "roofline": roof,
+        "clocks": clk,
+    }
+    if not args.no_cpu_baseline:
+        cores = os.cpu_count() or 1
+        env = dict(os.environ, OMP_NUM_THREADS=str(cores), OPENBLAS_NUM_THREADS="1")
+        try:
+            out = subprocess.run([sys.executable, os.path.join(ROOT, "oracle", "cpu_baseline.py"), str(o), str(v),
+                                  "--target", str(args.cpu_target), "--lno"], env=env, capture_output=True,
+                                 text=True, timeout=900, check=True)
+            res = json.loads(out.stdout.strip().splitlines()[-1])
+            line["cpu_baseline"] = {"value": res["tflops"], "unit": "TFLOP/s", "cores": res["cores"],
+                                    "kind": "reference", "sample": res["sample"], "t_full_s": res["t_full_s"]}
+        except Exception as exc:  # noqa: BLE001
+            line["cpu_baseline"] = {"value": None, "unit": "TFLOP/s", "error": f"{exc}"[:300]}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -332,7 +478,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "mixed_bf16", "fp64"])
-    ap.add_argument("--workload", default="large_o40v360", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default=None, choices=sorted(WORKLOADS),
+                    help="default large_o40v360 (medium_o20v180 with --lno)")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--cpu-target", type=float, default=8.0, help="seconds per CPU backward sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -346,10 +493,15 @@ def main():
                     help="instead of the headline: 256 uneven problems (nocc 4-12, nvir 20-80, naux 4(o+v)) "
                          "as one CUDA-graph launch vs one call per problem; one JSON line")
     ap.add_argument("--instances", type=int, default=256)
+    ap.add_argument("--lno", action="store_true",
+                    help="instead of the headline: the LNO fragment (T) (projector on the first occupied "
+                         "index, pyscfad/lno/ccsd_t.py) E+VJP on --workload (default medium_o20v180)")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="scale of the Cholesky-like factors (a small value gives a physically sized E(T))")
     args = ap.parse_args()
 
+    if args.workload is None:
+        args.workload = "medium_o20v180" if args.lno else "large_o40v360"
     world = _env_int("WORLD_SIZE", 1)
     rank = _env_int("RANK", 0)
     local_rank = _env_int("LOCAL_RANK", 0)
@@ -363,6 +515,10 @@ def main():
         return
     if args.batched:
         run_batched(args)
+        return
+    if args.lno:
+        if rank == 0:
+            run_lno(args, o, v, naux)
         return
 
     import torch

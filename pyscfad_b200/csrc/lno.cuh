@@ -41,6 +41,10 @@ constexpr int kLnoThreads = 256;
 constexpr int kLnoTile = 32;    // columns per projection tile
 constexpr int kLnoSB = 4;       // virtual sub-block edge of an orbit tile
 constexpr int kLnoRegion = kLnoSB * kLnoSB * kLnoSB;
+// slab layout in shared memory: slot s at s + 3 (s / 16) (fewer bank conflicts
+// on the permuted gathers), 73 doubles per slab
+constexpr int kLnoSlab = kLnoRegion + 3 * (kLnoRegion / 16 - 1) + 1;
+__host__ __device__ constexpr int lno_pad(int slot) { return slot + 3 * (slot >> 4); }
 constexpr int kLnoMaxSub = 64;  // sub-block triples per chunk: (16/4)^3
 constexpr int kLnoWaves = 4;    // waves of the streaming passes
 
@@ -128,11 +132,11 @@ inline void lno_build_tables(LnoTables &t) {
             const int l[3] = {sl / (kLnoSB * kLnoSB), (sl / kLnoSB) % kLnoSB, sl % kLnoSB};
             int ps[3], m[3];
             perm_of(s, ps);
-            t.symsl[s][sl] = (unsigned char)((l[ps[0]] * kLnoSB + l[ps[1]]) * kLnoSB + l[ps[2]]);
+            t.symsl[s][sl] = (unsigned char)lno_pad((l[ps[0]] * kLnoSB + l[ps[1]]) * kLnoSB + l[ps[2]]);
             for (int k = 0; k < 3; k++) m[r3p[s][k]] = k;
-            t.r3sl[0][s][sl] = (unsigned char)((l[m[0]] * kLnoSB + l[m[1]]) * kLnoSB + l[m[2]]);
+            t.r3sl[0][s][sl] = (unsigned char)lno_pad((l[m[0]] * kLnoSB + l[m[1]]) * kLnoSB + l[m[2]]);
             for (int k = 0; k < 3; k++) m[k] = r3p[s][k];
-            t.r3sl[1][s][sl] = (unsigned char)((l[m[0]] * kLnoSB + l[m[1]]) * kLnoSB + l[m[2]]);
+            t.r3sl[1][s][sl] = (unsigned char)lno_pad((l[m[0]] * kLnoSB + l[m[1]]) * kLnoSB + l[m[2]]);
         }
 }
 
@@ -208,8 +212,8 @@ struct LnoTile {
 
 __device__ void lno_tile_setup(const LnoArgs &A, LnoTile &T) {
     const int o = A.d.o, v = A.d.v;
-    const int rep = blockIdx.x;
-    const LnoSub &U = A.sub[blockIdx.y];
+    const int rep = blockIdx.y;               // sub-block triples vary fastest: neighbours in memory
+    const LnoSub &U = A.sub[blockIdx.x];
     {
         const uint4 *src = reinterpret_cast<const uint4 *>(&c_lno_tab.symsl[0][0]);
         uint4 *dst = reinterpret_cast<uint4 *>(&T.symsl[0][0]);
@@ -256,9 +260,9 @@ __device__ void lno_tile_setup(const LnoArgs &A, LnoTile &T) {
         T.b_fv[c] = z0 * o + r;
         T.eocc[c] = A.mo_e[p] + A.mo_e[q] + A.mo_e[r];
         for (int s = 0; s < 6; s++) {
-            T.symg[c][s] = (short)(P.prim[c_lno_tab.symc[cc][s]] * kLnoRegion);
-            T.r3g[0][c][s] = (short)(P.prim[c_lno_tab.r3c[0][cc][s]] * kLnoRegion);
-            T.r3g[1][c][s] = (short)(P.prim[c_lno_tab.r3c[1][cc][s]] * kLnoRegion);
+            T.symg[c][s] = (short)(P.prim[c_lno_tab.symc[cc][s]] * kLnoSlab);
+            T.r3g[0][c][s] = (short)(P.prim[c_lno_tab.r3c[0][cc][s]] * kLnoSlab);
+            T.r3g[1][c][s] = (short)(P.prim[c_lno_tab.r3c[1][cc][s]] * kLnoSlab);
         }
     }
     __syncthreads();
@@ -276,6 +280,7 @@ __device__ __forceinline__ int lno_r3_at(const LnoTile &T, int g, int sl, int s,
     const int e = threadIdx.x + (it) * kLnoThreads;                                                               \
     const bool inr = e < (T).nslab * kLnoRegion;                                                                  \
     const int g = inr ? e / kLnoRegion : 0, sl = e % kLnoRegion;                                                  \
+    const int si = g * kLnoSlab + lno_pad(sl);                                                                    \
     const int l0 = sl / (kLnoSB * kLnoSB), l1 = (sl / kLnoSB) % kLnoSB, l2 = sl % kLnoSB;                         \
     const bool valid = inr && l0 < (T).vlen[g][0] && l1 < (T).vlen[g][1] && l2 < (T).vlen[g][2];                \
     const long long goff = (T).soff[g] + (long long)l1 * (T).sy[g] + (long long)l0 * (T).sx[g] + l2
@@ -286,7 +291,7 @@ __global__ void __launch_bounds__(kLnoThreads) k_lno_tile_fwd(LnoArgs A) {
     const StageT *S = reinterpret_cast<const StageT *>(A.S);
     __shared__ LnoTile T;
     extern __shared__ double lno_sm[];
-    double *sW = lno_sm, *sV = lno_sm + 36 * kLnoRegion;
+    double *sW = lno_sm, *sV = lno_sm + 36 * kLnoSlab;
     lno_tile_setup(A, T);
     const int o = A.d.o;
 #pragma unroll
@@ -301,8 +306,8 @@ __global__ void __launch_bounds__(kLnoThreads) k_lno_tile_fwd(LnoArgs A) {
             vv = A.ovov[T.b_ov[g] + (long long)l0 * o_ * v_ + l1] * A.t1[T.b_t1[g] + l2] +
                  A.t2[T.b_t2[g] + (long long)l1 * v_ + l0] * A.fvo[T.b_fv[g] + l2 * o_];
         }
-        sW[e] = w;
-        sV[e] = vv;
+        sW[si] = w;
+        sV[si] = vv;
     }
     __syncthreads();
     double xr[kLnoIt];
@@ -327,7 +332,7 @@ __global__ void __launch_bounds__(kLnoThreads) k_lno_tile_fwd(LnoArgs A) {
         LNO_POS(T, it);
         (void)valid;
         (void)goff;
-        if (inr) sW[e] = xr[it];
+        if (inr) sW[si] = xr[it];
     }
     __syncthreads();
 #pragma unroll
@@ -351,14 +356,14 @@ template <int SPLIT>
 __global__ void __launch_bounds__(kLnoThreads) k_lno_tile_adj(LnoArgs A) {
     __shared__ LnoTile T;
     extern __shared__ double lno_sm[];
-    double *sZ = lno_sm, *sW = lno_sm + 36 * kLnoRegion;
+    double *sZ = lno_sm, *sW = lno_sm + 36 * kLnoSlab;
     lno_tile_setup(A, T);
 #pragma unroll
     for (int it = 0; it < kLnoIt; it++) {
         LNO_POS(T, it);
         if (!inr) break;
-        sZ[e] = valid ? A.B3[goff] : 0.0;
-        sW[e] = valid ? A.B1[goff] : 0.0;
+        sZ[si] = valid ? A.B3[goff] : 0.0;
+        sW[si] = valid ? A.B1[goff] : 0.0;
     }
     __syncthreads();
     double xr[kLnoIt];
@@ -372,7 +377,7 @@ __global__ void __launch_bounds__(kLnoThreads) k_lno_tile_adj(LnoArgs A) {
 #pragma unroll
         for (int s = 0; s < 6; s++) xb += c_r3_coef[s] * sZ[lno_r3_at(T, g, sl, s, 1)];
         xr[it] = xb;
-        sW[e] += xb;   // only this thread reads sW[e] in this phase
+        sW[si] += xb;   // only this thread reads sW[si] in this phase
     }
     __syncthreads();
 #pragma unroll
@@ -380,7 +385,7 @@ __global__ void __launch_bounds__(kLnoThreads) k_lno_tile_adj(LnoArgs A) {
         LNO_POS(T, it);
         (void)valid;
         (void)goff;
-        if (inr) sZ[e] = 0.5 * xr[it];
+        if (inr) sZ[si] = 0.5 * xr[it];
     }
     __syncthreads();
 #pragma unroll
@@ -425,52 +430,65 @@ __global__ void __launch_bounds__(kLnoThreads) k_lno_tile_adj(LnoArgs A) {
 //   with the adjoint: Zbar = f Wt / D -> B3, Dbar = -f Wt Q / D -> B2 (over Q),
 //   P^T(Wtbar)[l,c] = f sum_i mat[l,i] Q[i,c] -> B1, Gram WW Q^T -> mat_bar
 //   (f = ybar / 3).
-// Thread (warp w, lane j) owns column j and rows w, w+8, ... (R of them); the
-// Gram products use 4x4 register tiles of (l, i) over a share of the columns.
-constexpr int kLnoTileLd = kLnoTile + 1;
+// The three products run on the FP64 tensor cores (mma.sync m8n8k4, FP64 in
+// and out): per 8x8 output tile a thread holds D[g][2t], D[g][2t+1]
+// (g = lane / 4, t = lane % 4), A[g][t] and B[t][g] of each k-step.
+constexpr int kLnoLd = 36;   // row stride of the shared tiles (conflict-free fragment loads)
 
 inline size_t lno_proj_smem(int o) {
-    return (size_t)(2 * kLnoMaxO * kLnoTileLd + o * o + kLnoMaxO + kLnoTile) * sizeof(double);
+    return (size_t)(4 * kLnoMaxO * kLnoLd + o * o + kLnoMaxO + 2 * kLnoTile) * sizeof(double);
 }
 
-template <int R>
+// 8-byte global -> shared copy that bypasses registers; ok = false writes zero
+__device__ __forceinline__ void lno_cp_async8(double *dst, const double *src, bool ok) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(ok ? 8 : 0) : "memory");
+}
+__device__ __forceinline__ void lno_cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void lno_cp_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+__device__ __forceinline__ void lno_dmma(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
 __global__ void __launch_bounds__(kLnoThreads, 2) k_lno_proj(LnoArgs A) {
     extern __shared__ double lno_sm[];
-    double *sw = lno_sm, *sq = sw + kLnoMaxO * kLnoTileLd, *sM = sq + kLnoMaxO * kLnoTileLd;
+    // two buffers of the WW / Q tiles: the next tile streams in while this one is used
+    double *sw_b = lno_sm, *sq_b = sw_b + 2 * kLnoMaxO * kLnoLd, *sM = sq_b + 2 * kLnoMaxO * kLnoLd;
     const int o = A.d.o;
-    double *s_eo = sM + o * o, *s_ecol = s_eo + kLnoMaxO;
+    double *s_eo = sM + o * o, *s_ecol_b = s_eo + kLnoMaxO;
     __shared__ double red[kLnoThreads / 32];
-    const int o4 = (o + 3) & ~3;
+    const int o4 = (o + 3) & ~3, o8 = (o + 7) / 8, rows = 8 * o8;
     const PermBlock &pb = A.ch.pb[blockIdx.y];
     const int stride_p = o * o * pb.Tx * pb.Ty * pb.Tz;
     const int ntile = (stride_p + kLnoTile - 1) / kLnoTile;
     const double f = A.ybar / 3.0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int fg = lane >> 2, ft = lane & 3;   // fragment row group / thread in group
     const bool grad = A.want_grad != 0;
     for (int k = threadIdx.x; k < o * o; k += blockDim.x) sM[k] = A.mat[k];
     for (int k = threadIdx.x; k < o; k += blockDim.x) s_eo[k] = A.mo_e[k];
-    // Gram register tiles
-    const int nmt = o4 / 4, nm = nmt * nmt;
-    const int cg = nm >= kLnoThreads ? 1 : kLnoThreads / nm;
-    const bool gact = (int)threadIdx.x < nm * cg;
-    const int mt = threadIdx.x % nm, cgi = threadIdx.x / nm;
-    const int lb = (mt / nmt) * 4, ib = (mt % nmt) * 4;
-    double acc[4][4];
+    constexpr int kG = (kLnoMaxO / 8) * (kLnoMaxO / 8) / (kLnoThreads / 32);   // Gram tiles per warp
+    const int ngram = o8 * o8;
+    double acc[kG][2];
 #pragma unroll
-    for (int a = 0; a < 4; a++)
-#pragma unroll
-        for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
+    for (int k = 0; k < kG; k++) acc[k][0] = acc[k][1] = 0.0;
     double en = 0.0;
     const double *W = A.B0 + pb.soff, *Qg = A.B2 + pb.soff;
-    for (int tb = blockIdx.x; tb < ntile; tb += gridDim.x) {
+    // issue the copies of tile tb into buffer b (and its column energies)
+    auto issue = [&](int tb, int b) {
         const int c0 = tb * kLnoTile;
-        __syncthreads();
-        for (int e = threadIdx.x; e < o4 * kLnoTile; e += blockDim.x) {
+        double *sw = sw_b + b * kLnoMaxO * kLnoLd, *sq = sq_b + b * kLnoMaxO * kLnoLd;
+        for (int e = threadIdx.x; e < rows * kLnoTile; e += blockDim.x) {
             const int l = e / kLnoTile, j = e % kLnoTile;
             const bool ok = l < o && c0 + j < stride_p;
-            sw[l * kLnoTileLd + j] = ok ? W[(long long)l * stride_p + c0 + j] : 0.0;
-            sq[l * kLnoTileLd + j] = ok ? Qg[(long long)l * stride_p + c0 + j] : 0.0;
+            const long long at = ok ? (long long)l * stride_p + c0 + j : 0;
+            lno_cp_async8(sw + l * kLnoLd + j, W + at, ok);
+            lno_cp_async8(sq + l * kLnoLd + j, Qg + at, ok);
         }
+        lno_cp_commit();
         if (grad && threadIdx.x < kLnoTile) {
             int cc = c0 + threadIdx.x;
             double ec = 0.0;
@@ -486,56 +504,65 @@ __global__ void __launch_bounds__(kLnoThreads, 2) k_lno_proj(LnoArgs A) {
                 ec = A.mo_e[q] + A.mo_e[r] - A.mo_e[o + pb.X0 + xl] - A.mo_e[o + pb.Y0 + yl] -
                      A.mo_e[o + pb.Z0 + zl];
             }
-            s_ecol[threadIdx.x] = ec;
+            s_ecol_b[b * kLnoTile + threadIdx.x] = ec;
         }
-        __syncthreads();
-        const int j = lane;
-        const int c = c0 + j;
-        const bool ok = c < stride_p;
-        double wt[R], pq[R];
-#pragma unroll
-        for (int k = 0; k < R; k++) wt[k] = pq[k] = 0.0;
-        for (int l = 0; l < o; l++) {
-            const double a = sw[l * kLnoTileLd + j], b = sq[l * kLnoTileLd + j];
-#pragma unroll
-            for (int k = 0; k < R; k++) {
-                const int i = warp + k * (kLnoThreads / 32);
-                if (i < o) {
-                    wt[k] += sM[l * o + i] * a;
-                    if (grad) pq[k] += sM[i * o + l] * b;
-                }
+    };
+    int buf = 0;
+    if ((int)blockIdx.x < ntile) issue(blockIdx.x, 0);
+    for (int tb = blockIdx.x; tb < ntile; tb += gridDim.x) {
+        const int c0 = tb * kLnoTile;
+        if (tb + (int)gridDim.x < ntile)
+            issue(tb + gridDim.x, buf ^ 1);
+        else
+            lno_cp_commit();   // empty group: keeps the wait count uniform
+        lno_cp_wait1();        // this thread's copies of tile tb have landed
+        __syncthreads();       // ... and everyone's
+        const double *sw = sw_b + buf * kLnoMaxO * kLnoLd, *sq = sq_b + buf * kLnoMaxO * kLnoLd;
+        const double *s_ecol = s_ecol_b + buf * kLnoTile;
+        // Wt and P^T(Q) tiles (rows i / l in 8-blocks, columns in 8-blocks) and their epilogue
+        for (int tile = warp; tile < o8 * (kLnoTile / 8); tile += kLnoThreads / 32) {
+            const int mt = tile / (kLnoTile / 8), nt = tile % (kLnoTile / 8);
+            const int i = mt * 8 + fg;
+            double w0 = 0.0, w1 = 0.0, p0 = 0.0, p1 = 0.0;
+            for (int k0 = 0; k0 < o4; k0 += 4) {
+                const int l = k0 + ft;
+                const bool in = i < o && l < o;
+                lno_dmma(w0, w1, in ? sM[l * o + i] : 0.0, sw[l * kLnoLd + nt * 8 + fg]);
+                if (grad) lno_dmma(p0, p1, in ? sM[i * o + l] : 0.0, sq[l * kLnoLd + nt * 8 + fg]);
             }
-        }
 #pragma unroll
-        for (int k = 0; k < R; k++) {
-            const int i = warp + k * (kLnoThreads / 32);
-            if (i < o) {
-                const double qv = sq[i * kLnoTileLd + j];
-                en += wt[k] * qv;
-                if (grad && ok) {
-                    const double D = s_eo[i] + s_ecol[j];
-                    const double qb = f * wt[k];
+            for (int h = 0; h < 2; h++) {
+                const int cl = nt * 8 + 2 * ft + h;
+                const double wt = h ? w1 : w0;
+                const double qv = sq[i * kLnoLd + cl];
+                en += wt * qv;
+                const int c = c0 + cl;
+                if (grad && i < o && c < stride_p) {
+                    const double D = s_eo[i] + s_ecol[cl];
+                    const double qb = f * wt;
                     const long long at = pb.soff + (long long)i * stride_p + c;
                     A.B3[at] = qb / D;
                     A.B2[at] = -qb * qv / D;
-                    A.B1[at] = f * pq[k];
+                    A.B1[at] = f * (h ? p1 : p0);
                 }
             }
         }
-        if (grad && gact) {
-            for (int jj = cgi; jj < kLnoTile; jj += cg) {
-                double a[4], b[4];
+        if (grad) {
+            // Gram[l, i] += sum_c WW[l, c] Q[i, c]: warp-owned 8x8 tiles, k over the 32 columns
 #pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    a[k] = sw[(lb + k) * kLnoTileLd + jj];
-                    b[k] = sq[(ib + k) * kLnoTileLd + jj];
+            for (int k = 0; k < kG; k++) {
+                const int gt = warp + k * (kLnoThreads / 32);
+                if (gt < ngram) {
+                    const int mt = gt / o8, nt = gt % o8;
+#pragma unroll
+                    for (int k0 = 0; k0 < kLnoTile; k0 += 4)
+                        lno_dmma(acc[k][0], acc[k][1], sw[(mt * 8 + fg) * kLnoLd + k0 + ft],
+                                 sq[(nt * 8 + fg) * kLnoLd + k0 + ft]);
                 }
-#pragma unroll
-                for (int x = 0; x < 4; x++)
-#pragma unroll
-                    for (int y = 0; y < 4; y++) acc[x][y] += a[x] * b[y];
             }
         }
+        __syncthreads();   // buffer buf is refilled two tiles from now
+        buf ^= 1;
     }
     en = lno_warp_sum(en);
     if (lane == 0) red[warp] = en;
@@ -546,20 +573,19 @@ __global__ void __launch_bounds__(kLnoThreads, 2) k_lno_proj(LnoArgs A) {
         A.part[blockIdx.y * gridDim.x + blockIdx.x] = s / 3.0;
     }
     if (!grad) return;
-    // Gram partials: column groups summed in shared memory, then one atomic per entry
-    double *sG = sw;   // o*o <= 2 * kLnoMaxO * kLnoTileLd entries, tiles no longer needed
-    for (int k = threadIdx.x; k < o * o; k += blockDim.x) sG[k] = 0.0;
-    __syncthreads();
-    if (gact) {
 #pragma unroll
-        for (int x = 0; x < 4; x++)
+    for (int k = 0; k < kG; k++) {
+        const int gt = warp + k * (kLnoThreads / 32);
+        if (gt < ngram) {
+            const int l = (gt / o8) * 8 + fg;
 #pragma unroll
-            for (int y = 0; y < 4; y++)
-                if (lb + x < o && ib + y < o && acc[x][y] != 0.0) atomicAdd(&sG[(lb + x) * o + ib + y], acc[x][y]);
+            for (int h = 0; h < 2; h++) {
+                const int i = (gt % o8) * 8 + 2 * ft + h;
+                const double gv = h ? acc[k][1] : acc[k][0];
+                if (l < o && i < o && gv != 0.0) atomicAdd(&A.mat_bar[l * o + i], f * gv);
+            }
+        }
     }
-    __syncthreads();
-    for (int k = threadIdx.x; k < o * o; k += blockDim.x)
-        if (sG[k] != 0.0) atomicAdd(&A.mat_bar[k], f * sG[k]);
 }
 
 // ---------------------------------------------------------------------------
@@ -663,6 +689,6 @@ __global__ void __launch_bounds__(kLnoThreads) k_lno_vgrad(LnoArgs A) {
     }
 }
 
-inline size_t lno_tile_smem() { return 2 * 36 * kLnoRegion * sizeof(double); }
+inline size_t lno_tile_smem() { return 2 * 36 * kLnoSlab * sizeof(double); }
 
 }  // namespace tb

@@ -870,10 +870,7 @@ static int lno_chunk(const Plan &P, const ChunkDesc &ch, cudaStream_t st, const 
             lno_build_patterns(pats);
             TB_CUDA(cudaMemcpyToSymbol(c_lno_pat, pats, sizeof(pats)));
             const int ps = (int)lno_proj_smem(kLnoMaxO);
-            TB_CUDA(cudaFuncSetAttribute(k_lno_proj<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps));
-            TB_CUDA(cudaFuncSetAttribute(k_lno_proj<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps));
-            TB_CUDA(cudaFuncSetAttribute(k_lno_proj<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps));
-            TB_CUDA(cudaFuncSetAttribute(k_lno_proj<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps));
+            TB_CUDA(cudaFuncSetAttribute(k_lno_proj, cudaFuncAttributeMaxDynamicSharedMemorySize, ps));
             ready[dev] = true;
         }
     }
@@ -928,7 +925,7 @@ static int lno_chunk(const Plan &P, const ChunkDesc &ch, cudaStream_t st, const 
         if (rows > maxrows) maxrows = rows;
     }
     auto clampg = [](long long n) { return (unsigned)(n < kLnoGrid ? (n > 0 ? n : 1) : kLnoGrid); };
-    const dim3 gtile((unsigned)P.n_ijk, (unsigned)A.nsub);
+    const dim3 gtile((unsigned)A.nsub, (unsigned)P.n_ijk);
     // streaming passes: a few full waves of two blocks per SM over the chunk's
     // orderings (their per-block reductions end in global atomics on a few
     // hundred entries, so the grid stays small)
@@ -936,17 +933,7 @@ static int lno_chunk(const Plan &P, const ChunkDesc &ch, cudaStream_t st, const 
     auto clampw = [&](long long n) { return clampg(n < wave ? n : wave); };
     const dim3 gproj(clampw((maxcols / d.o + kLnoTile - 1) / kLnoTile), (unsigned)ch.nperm);
     TB_KLAUNCH(P_LNO, k_lno_tile_fwd<StageT><<<gtile, kLnoThreads, lno_tile_smem(), st>>>(A));
-    {
-        const size_t ps = lno_proj_smem(d.o);
-        if (d.o <= 8)
-            TB_KLAUNCH(P_LNO_PROJ, k_lno_proj<1><<<gproj, kLnoThreads, ps, st>>>(A));
-        else if (d.o <= 16)
-            TB_KLAUNCH(P_LNO_PROJ, k_lno_proj<2><<<gproj, kLnoThreads, ps, st>>>(A));
-        else if (d.o <= 32)
-            TB_KLAUNCH(P_LNO_PROJ, k_lno_proj<4><<<gproj, kLnoThreads, ps, st>>>(A));
-        else
-            TB_KLAUNCH(P_LNO_PROJ, k_lno_proj<8><<<gproj, kLnoThreads, ps, st>>>(A));
-    }
+    TB_KLAUNCH(P_LNO_PROJ, k_lno_proj<<<gproj, kLnoThreads, lno_proj_smem(d.o), st>>>(A));
     TB_KLAUNCH(P_LNO_PROJ, k_f2_energy_sum<<<1, 256, 0, st>>>(A.part, (int)(gproj.x * gproj.y), &ctrl->e_acc));
     if (!P.want_grad) return TRIPLES_OK;
     if (split != 0)   // fp16: power-of-two scale of the split Wbar; bf16: scale 1 (both read by the contractions)

@@ -70,6 +70,7 @@ struct LnoArgs {
     double ybar;
     int want_grad;
     double *part;                          // energy partials, gridDim.x * nperm
+    int n_ijk;                             // occupied representatives
 };
 
 // r3 on the virtual indices (pyscfad/cc/ccsd_t_slow.py:84-87):
@@ -111,7 +112,8 @@ struct alignas(16) LnoTables {
     unsigned char symc[36][6];
     unsigned char r3c[2][36][6];
 };
-__constant__ LnoTables c_lno_tab;
+// global (not constant) memory: threads read different entries at once
+__device__ LnoTables c_lno_tab;
 
 inline void lno_build_tables(LnoTables &t) {
     static const int r3p[6][3] = {{0, 1, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}, {0, 2, 1}, {1, 0, 2}};
@@ -148,7 +150,7 @@ struct LnoPattern {
     unsigned char cand[36];
     unsigned char prim[36];
 };
-__constant__ LnoPattern c_lno_pat[16];
+__device__ LnoPattern c_lno_pat[16];
 
 inline void lno_build_patterns(LnoPattern pats[16]) {
     for (int pid = 0; pid < 16; pid++) {
@@ -190,100 +192,165 @@ inline void lno_build_patterns(LnoPattern pats[16]) {
     }
 }
 
+// A block handles one virtual sub-block triple and kLnoReps consecutive
+// occupied representatives.  What depends only on the virtual side (per
+// candidate ordering: staging bases and strides, validity, energies) is set
+// up once per block; per representative only the occupied offsets of the
+// slabs are recomputed (ALU and shared memory only).
+constexpr int kLnoReps = 16;
+
 struct LnoTile {
-    int occ[36][3];       // per slab: occupied triple
-    int vst[36][3];       // per slab: virtual range starts (global)
-    int vlen[36][3];      // per slab: range lengths
-    long long soff[36];   // per slab: staging offset of local (0,0,0)
-    long long swoff[36];  // per slab: Wbar staging offset of local (0,0,0)
-    int sx[36], sy[36];   // per slab: staging strides of local x, y
-    long long swx[36], swy[36];
-    long long b_ov[36], b_t2[36];   // per slab: ovov[p,x0,q,y0], t2[q,p,y0,x0] offsets
-    int b_t1[36], b_fv[36];         // per slab: t1[r,z0], fvo[z0,r] offsets
-    long long plane[36];  // per slab: elements of its ordering's Wbar plane (split staging)
-    long long swbase[36]; // per slab: its ordering's Wbar offset (the split planes start at twice it)
-    double eocc[36];      // per slab: e_p + e_q + e_r
-    short symg[36][6];    // per slab and sigma: first position of the target slab
-    short r3g[2][36][6];  // per slab and r3 term
-    alignas(16) unsigned char symsl[6][kLnoRegion];
-    alignas(16) unsigned char r3sl[2][6][kLnoRegion];
-    int nslab;
+    // per candidate (virtual side)
+    long long soff_v[36], swoff_v[36], swbase_c[36], plane_c[36];
+    int strP[36], strQ[36], swP[36], rzp[36], tz[36];
+    long long bov_v[36];
+    int bt2_v[36], bt1_v[36], bfv_v[36];
+    int roff[36][kLnoSB * kLnoSB];  // staging offset of local (l0, l1, 0)
+    int swro[36][kLnoSB * kLnoSB];  // Wbar staging offset of local (l0, l1, 0)
+    unsigned long long vmask_c[36]; // slots inside the ranges
+    unsigned char cpr[36][3];       // which sub-range fills each virtual slot
+    double ev_r[3][kLnoSB];         // virtual orbital energies of the three sub-ranges
+    double s_eo[kLnoMaxO];
+    unsigned char symc[36][6], r3c[2][36][6];
+    LnoPattern pat[16];
+    int ijk[kLnoReps][3];
+    // per slab (current representative)
+    long long soff[36], swoff[36], b_ov[36], b_t2[36];
+    int b_t1[36], b_fv[36], cand[36];
+    double eocc[36];
+    short symg[36][6], r3g[2][36][6];
+    int nslab, nrep;
 };
 
-__device__ void lno_tile_setup(const LnoArgs &A, LnoTile &T) {
+// once per block: the virtual side of all 36 candidates
+__device__ void lno_tile_setup_block(const LnoArgs &A, LnoTile &T) {
     const int o = A.d.o, v = A.d.v;
-    const int rep = blockIdx.y;               // sub-block triples vary fastest: neighbours in memory
     const LnoSub &U = A.sub[blockIdx.x];
-    {
-        const uint4 *src = reinterpret_cast<const uint4 *>(&c_lno_tab.symsl[0][0]);
-        uint4 *dst = reinterpret_cast<uint4 *>(&T.symsl[0][0]);
-        for (int e = threadIdx.x; e < 6 * kLnoRegion / 16; e += blockDim.x) dst[e] = src[e];
-        const uint4 *src2 = reinterpret_cast<const uint4 *>(&c_lno_tab.r3sl[0][0][0]);
-        uint4 *dst2 = reinterpret_cast<uint4 *>(&T.r3sl[0][0][0]);
-        for (int e = threadIdx.x; e < 12 * kLnoRegion / 16; e += blockDim.x) dst2[e] = src2[e];
+    const int r0 = blockIdx.y * kLnoReps;
+    if (threadIdx.x == 0) T.nrep = min(kLnoReps, A.n_ijk - r0);
+    for (int e = threadIdx.x; e < kLnoReps * 3; e += blockDim.x)
+        T.ijk[e / 3][e % 3] = r0 + e / 3 < A.n_ijk ? A.ijk[3 * r0 + e] : 0;
+    for (int e = threadIdx.x; e < o; e += blockDim.x) T.s_eo[e] = A.mo_e[e];
+    for (int e = threadIdx.x; e < 36; e += blockDim.x) T.cand[e] = 0;
+    for (int e = threadIdx.x; e < 3 * kLnoSB; e += blockDim.x) {
+        const int k = e / kLnoSB, l = e % kLnoSB;
+        T.ev_r[k][l] = l < U.len[k] ? A.mo_e[o + U.st[k] + l] : 0.0;
     }
-    const int ijk[3] = {A.ijk[3 * rep], A.ijk[3 * rep + 1], A.ijk[3 * rep + 2]};
+    for (int e = threadIdx.x; e < 36 * 6; e += blockDim.x) {
+        T.symc[e / 6][e % 6] = c_lno_tab.symc[e / 6][e % 6];
+        T.r3c[0][e / 6][e % 6] = c_lno_tab.r3c[0][e / 6][e % 6];
+        T.r3c[1][e / 6][e % 6] = c_lno_tab.r3c[1][e / 6][e % 6];
+    }
+    for (int e = threadIdx.x; e < (int)sizeof(T.pat); e += blockDim.x)
+        reinterpret_cast<unsigned char *>(T.pat)[e] = reinterpret_cast<const unsigned char *>(c_lno_pat)[e];
+    const int cc = threadIdx.x;
+    if (cc < 36) {
+        int pr[3], vst[3], vl[3];
+        perm_of(cc % 6, pr);
+        for (int k = 0; k < 3; k++) {
+            vst[k] = U.st[pr[k]];
+            vl[k] = U.len[pr[k]];
+            T.cpr[cc][k] = (unsigned char)pr[k];
+        }
+        const int x0 = vst[0], y0 = vst[1], z0 = vst[2];
+        const int t = A.tau_of[(lno_slot(A.ch, x0) * 3 + lno_slot(A.ch, y0)) * 3 + lno_slot(A.ch, z0)];
+        const PermBlock &pb = A.ch.pb[t];
+        const int oTz = o * pb.Tz;
+        const int sx = oTz, sy = pb.Tx * oTz;
+        T.strQ[cc] = pb.Ty * sy;
+        T.strP[cc] = o * pb.Ty * sy;
+        T.tz[cc] = pb.Tz;
+        T.soff_v[cc] = pb.soff + (long long)(y0 - pb.Y0) * sy + (long long)(x0 - pb.X0) * sx + (z0 - pb.Z0);
+        const int wx = o * pb.rzp, wy = o * pb.Tx * wx;
+        T.swP[cc] = pb.Tx * wx;
+        T.rzp[cc] = pb.rzp;
+        T.swoff_v[cc] = pb.swoff + (long long)(y0 - pb.Y0) * wy + (long long)(x0 - pb.X0) * wx + (z0 - pb.Z0);
+        T.plane_c[cc] = (long long)pb.Ty * wy;
+        T.swbase_c[cc] = pb.swoff;
+        T.bov_v[cc] = (long long)x0 * o * v + y0;
+        T.bt2_v[cc] = y0 * v + x0;
+        T.bt1_v[cc] = z0;
+        T.bfv_v[cc] = z0 * o;
+        for (int l01 = 0; l01 < kLnoSB * kLnoSB; l01++) {
+            const int l0 = l01 / kLnoSB, l1 = l01 % kLnoSB;
+            T.roff[cc][l01] = l1 * sy + l0 * sx;
+            T.swro[cc][l01] = l1 * wy + l0 * wx;
+        }
+        unsigned long long m = 0ull;
+        for (int sl = 0; sl < kLnoRegion; sl++) {
+            const int l0 = sl / (kLnoSB * kLnoSB), l1 = (sl / kLnoSB) % kLnoSB, l2 = sl % kLnoSB;
+            if (l0 < vl[0] && l1 < vl[1] && l2 < vl[2]) m |= 1ull << sl;
+        }
+        T.vmask_c[cc] = m;
+    }
+    __syncthreads();
+}
+
+// per representative n: the occupied side of its slabs
+__device__ void lno_tile_setup_rep(const LnoArgs &A, LnoTile &T, int n) {
+    const int o = A.d.o, v = A.d.v;
+    const LnoSub &U = A.sub[blockIdx.x];
+    const int ijk[3] = {T.ijk[n][0], T.ijk[n][1], T.ijk[n][2]};
     const int pid = ((ijk[0] == ijk[1]) << 3) | ((ijk[1] == ijk[2]) << 2) | ((U.st[0] == U.st[1]) << 1) |
                     (U.st[1] == U.st[2]);
-    const LnoPattern &P = c_lno_pat[pid];
+    const LnoPattern &P = T.pat[pid];
     const int c = threadIdx.x;
     if (c == 0) T.nslab = P.nslab;
     if (c < P.nslab) {
         const int cc = P.cand[c];
-        int pp[3], pr[3];
+        int pp[3];
         perm_of(cc / 6, pp);
-        perm_of(cc % 6, pr);
-        for (int k = 0; k < 3; k++) {
-            T.occ[c][k] = ijk[pp[k]];
-            T.vst[c][k] = U.st[pr[k]];
-            T.vlen[c][k] = U.len[pr[k]];
-        }
-        const int x0 = T.vst[c][0], y0 = T.vst[c][1], z0 = T.vst[c][2];
-        const int p = T.occ[c][0], q = T.occ[c][1], r = T.occ[c][2];
-        const int t = A.tau_of[(lno_slot(A.ch, x0) * 3 + lno_slot(A.ch, y0)) * 3 + lno_slot(A.ch, z0)];
-        const PermBlock &pb = A.ch.pb[t];
-        const long long oTz = (long long)o * pb.Tz;
-        T.sx[c] = (int)oTz;
-        T.sy[c] = (int)(pb.Tx * oTz);
-        T.soff[c] = pb.soff + (((long long)p * o + q) * pb.Ty + (y0 - pb.Y0)) * pb.Tx * oTz +
-                    (long long)(x0 - pb.X0) * oTz + (long long)r * pb.Tz + (z0 - pb.Z0);
-        const long long wx = (long long)o * pb.rzp, wy = (long long)o * pb.Tx * wx;
-        T.swx[c] = wx;
-        T.swy[c] = wy;
-        T.swoff[c] = pb.swoff + (long long)(y0 - pb.Y0) * wy + (long long)p * pb.Tx * wx + (long long)(x0 - pb.X0) * wx +
-                     (long long)q * pb.rzp + (long long)r * pb.Tz + (z0 - pb.Z0);
-        T.plane[c] = (long long)pb.Ty * wy;
-        T.swbase[c] = pb.swoff;
-        T.b_ov[c] = (((long long)p * v + x0) * o + q) * v + y0;
-        T.b_t2[c] = (((long long)q * o + p) * v + y0) * v + x0;
-        T.b_t1[c] = r * v + z0;
-        T.b_fv[c] = z0 * o + r;
-        T.eocc[c] = A.mo_e[p] + A.mo_e[q] + A.mo_e[r];
+        const int p = ijk[pp[0]], q = ijk[pp[1]], r = ijk[pp[2]];
+        T.cand[c] = cc;
+        T.soff[c] = T.soff_v[cc] + (long long)p * T.strP[cc] + (long long)q * T.strQ[cc] + r * T.tz[cc];
+        T.swoff[c] = T.swoff_v[cc] + (long long)p * T.swP[cc] + (long long)q * T.rzp[cc] + r * T.tz[cc];
+        T.b_ov[c] = ((long long)p * v * o + q) * v + T.bov_v[cc];
+        T.b_t2[c] = ((long long)q * o + p) * v * v + T.bt2_v[cc];
+        T.b_t1[c] = r * v + T.bt1_v[cc];
+        T.b_fv[c] = T.bfv_v[cc] + r;
+        T.eocc[c] = T.s_eo[p] + T.s_eo[q] + T.s_eo[r];
         for (int s = 0; s < 6; s++) {
-            T.symg[c][s] = (short)(P.prim[c_lno_tab.symc[cc][s]] * kLnoSlab);
-            T.r3g[0][c][s] = (short)(P.prim[c_lno_tab.r3c[0][cc][s]] * kLnoSlab);
-            T.r3g[1][c][s] = (short)(P.prim[c_lno_tab.r3c[1][cc][s]] * kLnoSlab);
+            T.symg[c][s] = (short)(P.prim[T.symc[cc][s]] * kLnoSlab);
+            T.r3g[0][c][s] = (short)(P.prim[T.r3c[0][cc][s]] * kLnoSlab);
+            T.r3g[1][c][s] = (short)(P.prim[T.r3c[1][cc][s]] * kLnoSlab);
         }
     }
     __syncthreads();
 }
 
-__device__ __forceinline__ int lno_sym_at(const LnoTile &T, int g, int sl, int s) {
-    return T.symg[g][s] + T.symsl[s][sl];
-}
-__device__ __forceinline__ int lno_r3_at(const LnoTile &T, int g, int sl, int s, int adj) {
-    return T.r3g[adj][g][s] + T.r3sl[adj][s][sl];
-}
+// Per-thread constants: a thread's slot in its slabs is the same at every
+// iteration (kLnoThreads is a multiple of the slab size), so its local
+// indices and the permuted slots of its gathers are loaded once.
+struct LnoLane {
+    int sl, l0, l1, l2, l01, psl;
+    unsigned sym[2], r3[2][2];   // 8-bit permuted padded slots, four per word (six used)
 
-// it-th position of this thread; fields valid only when in range
-#define LNO_POS(T, it)                                                                                              \
-    const int e = threadIdx.x + (it) * kLnoThreads;                                                               \
-    const bool inr = e < (T).nslab * kLnoRegion;                                                                  \
-    const int g = inr ? e / kLnoRegion : 0, sl = e % kLnoRegion;                                                  \
-    const int si = g * kLnoSlab + lno_pad(sl);                                                                    \
-    const int l0 = sl / (kLnoSB * kLnoSB), l1 = (sl / kLnoSB) % kLnoSB, l2 = sl % kLnoSB;                         \
-    const bool valid = inr && l0 < (T).vlen[g][0] && l1 < (T).vlen[g][1] && l2 < (T).vlen[g][2];                \
-    const long long goff = (T).soff[g] + (long long)l1 * (T).sy[g] + (long long)l0 * (T).sx[g] + l2
+    __device__ __forceinline__ void init() {
+        sl = threadIdx.x % kLnoRegion;
+        l0 = sl / (kLnoSB * kLnoSB);
+        l1 = (sl / kLnoSB) % kLnoSB;
+        l2 = sl % kLnoSB;
+        l01 = l0 * kLnoSB + l1;
+        psl = lno_pad(sl);
+        sym[0] = sym[1] = r3[0][0] = r3[0][1] = r3[1][0] = r3[1][1] = 0u;
+        for (int s = 0; s < 6; s++) {
+            sym[s >> 2] |= (unsigned)c_lno_tab.symsl[s][sl] << (8 * (s & 3));
+            r3[0][s >> 2] |= (unsigned)c_lno_tab.r3sl[0][s][sl] << (8 * (s & 3));
+            r3[1][s >> 2] |= (unsigned)c_lno_tab.r3sl[1][s][sl] << (8 * (s & 3));
+        }
+    }
+    __device__ __forceinline__ int symsl(int s) const { return (sym[s >> 2] >> (8 * (s & 3))) & 0xff; }
+    __device__ __forceinline__ int r3sl(int a, int s) const { return (r3[a][s >> 2] >> (8 * (s & 3))) & 0xff; }
+};
+
+// it-th position of this thread: slab g (candidate cg), shared index si, staging offset goff
+#define LNO_POS(T, L, it)                                                                                           \
+    const int g = (int)(threadIdx.x / kLnoRegion) + (it) * (kLnoThreads / kLnoRegion);                            \
+    const bool inr = g < (T).nslab;                                                                               \
+    const int cg = inr ? (T).cand[g] : 0;                                                                         \
+    const int si = g * kLnoSlab + (L).psl;                                                                        \
+    const bool valid = inr && (((T).vmask_c[cg] >> (L).sl) & 1ull);                                                \
+    const long long goff = (T).soff[g] + (T).roff[cg][(L).l01] + (L).l2
 
 // pass 1: WW -> B0, Q = r3(WW + VV/2) / D -> B2
 template <typename StageT>
@@ -292,19 +359,22 @@ __global__ void __launch_bounds__(kLnoThreads) k_lno_tile_fwd(LnoArgs A) {
     __shared__ LnoTile T;
     extern __shared__ double lno_sm[];
     double *sW = lno_sm, *sV = lno_sm + 36 * kLnoSlab;
-    lno_tile_setup(A, T);
-    const int o = A.d.o;
+    LnoLane L;
+    L.init();
+    lno_tile_setup_block(A, T);
+    const int o = A.d.o, v = A.d.v;
+    const int ovl = L.l0 * o * v + L.l1, t2l = L.l1 * v + L.l0, fvl = L.l2 * o;
+    for (int n = 0; n < T.nrep; n++) {
+    lno_tile_setup_rep(A, T, n);
 #pragma unroll
     for (int it = 0; it < kLnoIt; it++) {
-        LNO_POS(T, it);
+        LNO_POS(T, L, it);
         if (!inr) break;
         double w = 0.0, vv = 0.0;
         if (valid) {
             // v = ovov[p,x,q,y] t1[r,z] + t2[q,p,y,x] fvo[z,r]
-            const int o_ = A.d.o, v_ = A.d.v;
             w = (double)S[goff];
-            vv = A.ovov[T.b_ov[g] + (long long)l0 * o_ * v_ + l1] * A.t1[T.b_t1[g] + l2] +
-                 A.t2[T.b_t2[g] + (long long)l1 * v_ + l0] * A.fvo[T.b_fv[g] + l2 * o_];
+            vv = A.ovov[T.b_ov[g] + ovl] * A.t1[T.b_t1[g] + L.l2] + A.t2[T.b_t2[g] + t2l] * A.fvo[T.b_fv[g] + fvl];
         }
         sW[si] = w;
         sV[si] = vv;
@@ -313,13 +383,14 @@ __global__ void __launch_bounds__(kLnoThreads) k_lno_tile_fwd(LnoArgs A) {
     double xr[kLnoIt];
 #pragma unroll
     for (int it = 0; it < kLnoIt; it++) {
-        LNO_POS(T, it);
+        LNO_POS(T, L, it);
+        (void)si;
         xr[it] = 0.0;
         if (!valid) continue;
         double ww = 0.0, vv = 0.0;
 #pragma unroll
         for (int s = 0; s < 6; s++) {
-            const int k = lno_sym_at(T, g, sl, s);
+            const int k = T.symg[g][s] + L.symsl(s);
             ww += sW[k];
             vv += sV[k];
         }
@@ -329,7 +400,7 @@ __global__ void __launch_bounds__(kLnoThreads) k_lno_tile_fwd(LnoArgs A) {
     __syncthreads();
 #pragma unroll
     for (int it = 0; it < kLnoIt; it++) {
-        LNO_POS(T, it);
+        LNO_POS(T, L, it);
         (void)valid;
         (void)goff;
         if (inr) sW[si] = xr[it];
@@ -337,14 +408,17 @@ __global__ void __launch_bounds__(kLnoThreads) k_lno_tile_fwd(LnoArgs A) {
     __syncthreads();
 #pragma unroll
     for (int it = 0; it < kLnoIt; it++) {
-        LNO_POS(T, it);
+        LNO_POS(T, L, it);
+        (void)si;
         if (!valid) continue;
         double z = 0.0;
 #pragma unroll
-        for (int s = 0; s < 6; s++) z += c_r3_coef[s] * sW[lno_r3_at(T, g, sl, s, 0)];
-        const double D = T.eocc[g] - A.mo_e[o + T.vst[g][0] + l0] - A.mo_e[o + T.vst[g][1] + l1] -
-                         A.mo_e[o + T.vst[g][2] + l2];
+        for (int s = 0; s < 6; s++) z += c_r3_coef[s] * sW[T.r3g[0][g][s] + L.r3sl(0, s)];
+        const double D = T.eocc[g] - T.ev_r[T.cpr[cg][0]][L.l0] - T.ev_r[T.cpr[cg][1]][L.l1] -
+                         T.ev_r[T.cpr[cg][2]][L.l2];
         A.B2[goff] = z / D;
+    }
+    __syncthreads();   // slab data and shared arrays are reused by the next representative
     }
 }
 
@@ -357,10 +431,15 @@ __global__ void __launch_bounds__(kLnoThreads) k_lno_tile_adj(LnoArgs A) {
     __shared__ LnoTile T;
     extern __shared__ double lno_sm[];
     double *sZ = lno_sm, *sW = lno_sm + 36 * kLnoSlab;
-    lno_tile_setup(A, T);
+    LnoLane L;
+    L.init();
+    lno_tile_setup_block(A, T);
+    const float wsc = SPLIT == 1 ? (float)*A.wscale : 1.0f;
+    for (int n = 0; n < T.nrep; n++) {
+    lno_tile_setup_rep(A, T, n);
 #pragma unroll
     for (int it = 0; it < kLnoIt; it++) {
-        LNO_POS(T, it);
+        LNO_POS(T, L, it);
         if (!inr) break;
         sZ[si] = valid ? A.B3[goff] : 0.0;
         sW[si] = valid ? A.B1[goff] : 0.0;
@@ -369,20 +448,20 @@ __global__ void __launch_bounds__(kLnoThreads) k_lno_tile_adj(LnoArgs A) {
     double xr[kLnoIt];
 #pragma unroll
     for (int it = 0; it < kLnoIt; it++) {
-        LNO_POS(T, it);
+        LNO_POS(T, L, it);
         (void)goff;
         xr[it] = 0.0;
         if (!valid) continue;
         double xb = 0.0;
 #pragma unroll
-        for (int s = 0; s < 6; s++) xb += c_r3_coef[s] * sZ[lno_r3_at(T, g, sl, s, 1)];
+        for (int s = 0; s < 6; s++) xb += c_r3_coef[s] * sZ[T.r3g[1][g][s] + L.r3sl(1, s)];
         xr[it] = xb;
         sW[si] += xb;   // only this thread reads sW[si] in this phase
     }
     __syncthreads();
 #pragma unroll
     for (int it = 0; it < kLnoIt; it++) {
-        LNO_POS(T, it);
+        LNO_POS(T, L, it);
         (void)valid;
         (void)goff;
         if (inr) sZ[si] = 0.5 * xr[it];
@@ -390,32 +469,35 @@ __global__ void __launch_bounds__(kLnoThreads) k_lno_tile_adj(LnoArgs A) {
     __syncthreads();
 #pragma unroll
     for (int it = 0; it < kLnoIt; it++) {
-        LNO_POS(T, it);
+        LNO_POS(T, L, it);
+        (void)si;
         if (!valid) continue;
         double wb = 0.0, vb = 0.0;
 #pragma unroll
         for (int s = 0; s < 6; s++) {
-            const int k = lno_sym_at(T, g, sl, s);
+            const int k = T.symg[g][s] + L.symsl(s);
             wb += sW[k];
             vb += sZ[k];
         }
-        const long long wl = T.swoff[g] + (long long)l1 * T.swy[g] + (long long)l0 * T.swx[g] + l2;
+        const long long wl = T.swoff[g] + T.swro[cg][L.l01] + L.l2;
         if (SPLIT == 0) {
             reinterpret_cast<double *>(A.SW)[wl] = wb;
         } else if (SPLIT == 1) {
-            const float xs = (float)(wb * *A.wscale);
+            const float xs = (float)wb * wsc;
             const __half h = __float2half_rn(xs);
-            __half *dst = reinterpret_cast<__half *>(A.SW) + T.swbase[g] + wl;   // 2 swoff + local offset
+            __half *dst = reinterpret_cast<__half *>(A.SW) + T.swbase_c[cg] + wl;   // 2 swoff + local offset
             dst[0] = h;
-            dst[T.plane[g]] = __float2half_rn(xs - __half2float(h));
+            dst[T.plane_c[cg]] = __float2half_rn(xs - __half2float(h));
         } else {
             const float xs = (float)wb;
             const __nv_bfloat16 h = __float2bfloat16_rn(xs);
-            __nv_bfloat16 *dst = reinterpret_cast<__nv_bfloat16 *>(A.SW) + T.swbase[g] + wl;
+            __nv_bfloat16 *dst = reinterpret_cast<__nv_bfloat16 *>(A.SW) + T.swbase_c[cg] + wl;
             dst[0] = h;
-            dst[T.plane[g]] = __float2bfloat16_rn(xs - __bfloat162float(h));
+            dst[T.plane_c[cg]] = __float2bfloat16_rn(xs - __bfloat162float(h));
         }
         A.B0[goff] = vb;
+    }
+    __syncthreads();   // slab data and shared arrays are reused by the next representative
     }
 }
 

@@ -925,7 +925,8 @@ static int lno_chunk(const Plan &P, const ChunkDesc &ch, cudaStream_t st, const 
         if (rows > maxrows) maxrows = rows;
     }
     auto clampg = [](long long n) { return (unsigned)(n < kLnoGrid ? (n > 0 ? n : 1) : kLnoGrid); };
-    const dim3 gtile((unsigned)A.nsub, (unsigned)P.n_ijk);
+    A.n_ijk = P.n_ijk;
+    const dim3 gtile((unsigned)A.nsub, (unsigned)((P.n_ijk + kLnoReps - 1) / kLnoReps));
     // streaming passes: a few full waves of two blocks per SM over the chunk's
     // orderings (their per-block reductions end in global atomics on a few
     // hundred entries, so the grid stays small)

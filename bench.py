@@ -34,6 +34,7 @@ sys.path.insert(0, ROOT)
 METRIC = "(T) E+VJP TFLOP/s (o=40,v=360): mixed-prec vs FP64 on B200 at |dE|<=1e-7 Eh"
 WORKLOADS = {
     "water_ccpvdz_o5v19": (5, 19, 80),
+    "small_o14v96": (14, 96, 400),
     "medium_o20v180": (20, 180, 600),
     "large_o40v360": (40, 360, 1200),
     "huge_o50v450": (50, 450, 1500),

@@ -935,7 +935,7 @@ static int lno_chunk(const Plan &P, const ChunkDesc &ch, cudaStream_t st, const 
     const dim3 gproj(clampw((maxcols / d.o + kLnoTile - 1) / kLnoTile), (unsigned)ch.nperm);
     TB_KLAUNCH(P_LNO, k_lno_tile_fwd<StageT><<<gtile, kLnoThreads, lno_tile_smem(), st>>>(A));
     TB_KLAUNCH(P_LNO_PROJ, k_lno_proj<<<gproj, kLnoThreads, lno_proj_smem(d.o), st>>>(A));
-    TB_KLAUNCH(P_LNO_PROJ, k_f2_energy_sum<<<1, 256, 0, st>>>(A.part, (int)(gproj.x * gproj.y), &ctrl->e_acc));
+    TB_KLAUNCH(P_PREP, k_f2_energy_sum<<<1, 256, 0, st>>>(A.part, (int)(gproj.x * gproj.y), &ctrl->e_acc));
     if (!P.want_grad) return TRIPLES_OK;
     if (split != 0)   // fp16: power-of-two scale of the split Wbar; bf16: scale 1 (both read by the contractions)
         TB_KLAUNCH(P_PREP, k_chunk_scale<<<1, 32, 0, st>>>(ctrl, io.mo_energy, d.o, ch.base[0], ch.nabc[0], ch.base[1],

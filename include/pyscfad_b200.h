@@ -121,6 +121,34 @@ int triples_lno_energy_vjp(void *stream, int precision, int nocc, int nvir, int 
                            double *ovoo_bar, double *ovov_bar, double *ovvv_bar,
                            double *fvo_bar);
 
+/* Density-fitted inputs: the ovvv operand comes from the DF factors as the
+ * reference's DF ERIs build it (pyscfad/cc/dfccsd.py:77-88):
+ *   Lov[naux, o*v]          = Lpq[:, :o, o:]
+ *   Lvv[naux, v(v+1)/2]     = pack_tril(Lpq[:, o:, o:])   (pair f >= y at f(f+1)/2 + y)
+ *   ovvv[o*v, v(v+1)/2]     = Lov^T Lvv
+ * built on the device, so the caller never holds or transfers the
+ * o*v*v(v+1)/2 ovvv array.  Gradients are returned for the factors instead of
+ * ovvv: Lov_bar[naux, o*v], Lvv_bar[naux, v(v+1)/2] (the packed convention of
+ * Lvv: one entry per pair).  Everything else is exactly triples_energy[_vjp]
+ * with ovvv_packed = 1 (the three factor products are FP64 GEMMs in the
+ * library). */
+size_t triples_df_workspace_size(int precision, int nocc, int nvir, int naux, int want_grad);
+
+int triples_energy_df(void *stream, int precision, int nocc, int nvir, int naux,
+                      const double *mo_energy, const double *t1, const double *t2,
+                      const double *ovoo, const double *ovov,
+                      const double *Lov, const double *Lvv, const double *fvo,
+                      void *workspace, size_t workspace_bytes, double *e_out);
+
+int triples_energy_vjp_df(void *stream, int precision, int nocc, int nvir, int naux,
+                          const double *mo_energy, const double *t1, const double *t2,
+                          const double *ovoo, const double *ovov,
+                          const double *Lov, const double *Lvv, const double *fvo, double ybar,
+                          void *workspace, size_t workspace_bytes, double *e_out,
+                          double *mo_energy_bar, double *t1_bar, double *t2_bar,
+                          double *ovoo_bar, double *ovov_bar,
+                          double *Lov_bar, double *Lvv_bar, double *fvo_bar);
+
 /* Size of the fixed device scratch behind triples_energy_vjp_static. */
 #define TRIPLES_STATIC_SCRATCH_BYTES ((size_t)64 << 20)
 

@@ -369,3 +369,15 @@ def np_lno_energy_vjp(inp, mat, ybar=1.0, want_grad=True):
     g["ovvv"] = np.einsum('pqrxyz,rqzf->pxfy', wbar, inp.t2)
     g["ovoo"] = -np.einsum('pqrxyz,rmzy->pxmq', wbar, inp.t2)
     return e, g
+
+
+# --------------------------------------------------------------------------
+# DF factors (pyscfad/cc/dfccsd.py:77-88): ovvv_tril = Lov^T Lvv_tril, so the
+# packed ovvv cotangent of pyscfad/cc/ccsd_t.py:184-191 maps to the factors
+# by the chain rule.
+# --------------------------------------------------------------------------
+def df_factor_grads(ovvv_tril_bar, Lov, Lvv_tril):
+    """(Lov_bar[naux, o*v], Lvv_bar[naux, v(v+1)/2]) from the packed ovvv
+    cotangent [o, v, v(v+1)/2]."""
+    G = ovvv_tril_bar.reshape(Lov.shape[1], Lvv_tril.shape[1])
+    return Lvv_tril @ G.T, Lov @ G

@@ -54,6 +54,13 @@ def load():
     lib.triples_lno_energy_vjp.restype = _c_int
     lib.triples_lno_energy_vjp.argtypes = ([_vp, _c_int, _c_int, _c_int, _c_int] + [_vp] * 8 +
                                            [_c_double, _vp, _c_size, _vp] + [_vp] * 8)
+    lib.triples_df_workspace_size.restype = _c_size
+    lib.triples_df_workspace_size.argtypes = [_c_int] * 5
+    lib.triples_energy_df.restype = _c_int
+    lib.triples_energy_df.argtypes = [_vp] + [_c_int] * 4 + [_vp] * 8 + [_vp, _c_size, _vp]
+    lib.triples_energy_vjp_df.restype = _c_int
+    lib.triples_energy_vjp_df.argtypes = ([_vp] + [_c_int] * 4 + [_vp] * 8 + [_c_double, _vp, _c_size, _vp] +
+                                          [_vp] * 8)
     lib.triples_status_string.restype = ctypes.c_char_p
     lib.triples_status_string.argtypes = [_c_int]
     lib.triples_last_cuda_error.restype = _c_int

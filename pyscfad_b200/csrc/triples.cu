@@ -768,6 +768,38 @@ __global__ void k_fold_ovoo(const double *__restrict__ GA2, Dims d, double *__re
 
 __global__ void k_copy_scalar(const double *src, double *dst) { dst[0] = src[0]; }
 
+// plain FP64 GEMM through the multi-index tile (DF factor products)
+__global__ void __launch_bounds__(256) k_gemm_plain(GemmArgs g) {
+    __shared__ GemmSmem sm;
+    const int m0 = blockIdx.x * kGBM, n0 = blockIdx.y * kGBN;
+    if (m0 >= g.M || n0 >= g.N) return;
+    gemm_fp64_tile(g, m0, n0, sm);
+}
+
+// C[m*cms + n*cns] = sum_k A[m*ams + k*aks] B[n*bms + k*bks]
+int gemm_plain(cudaStream_t st, int M, int N, int K, const double *A, long long ams, long long aks,
+               const double *B, long long bms, long long bks, double *C, long long cms, long long cns) {
+    GemmArgs g;
+    g.M = M;
+    g.N = N;
+    g.K = K;
+    g.K2 = 0;
+    g.A = GOp{A, map1(ams), map1(aks), aks == 1 ? 1 : 0};
+    g.B = GOp{B, map1(bms), map1(bks), bks == 1 ? 1 : 0};
+    g.A2 = g.A;
+    g.B2 = g.B;
+    g.C = C;
+    g.cm = map1(cms);
+    g.cn = map1(cns);
+    g.alpha = 1.0;
+    g.alpha2 = 0.0;
+    g.accumulate = 0;
+    const dim3 grid((unsigned)((M + kGBM - 1) / kGBM), (unsigned)((N + kGBN - 1) / kGBN));
+    if (grid.y > 65535) return TRIPLES_ERR_UNSUPPORTED;
+    TB_KLAUNCH(P_PREP, k_gemm_plain<<<grid, 256, 0, st>>>(g));
+    return TRIPLES_OK;
+}
+
 // ---------------------------------------------------------------------------
 // driver
 // ---------------------------------------------------------------------------
@@ -1467,6 +1499,95 @@ int triples_lno_energy_vjp(void *stream, int precision, int nocc, int nvir, int 
     io.mo_energy_bar = mo_energy_bar; io.t1_bar = t1_bar; io.t2_bar = t2_bar; io.ovoo_bar = ovoo_bar;
     io.ovov_bar = ovov_bar; io.ovvv_bar = ovvv_bar; io.fvo_bar = fvo_bar;
     return triples_lno_call(stream, precision, nocc, nvir, ovvv_packed, 1, io, workspace_bytes);
+}
+
+// ---- density-fitted ERI producer ----
+// ovvv[(p,x), pair] = sum_P Lov[P,(p,x)] Lvv[P,pair]  (pyscfad/cc/dfccsd.py:77-88), packed
+// pairs f >= y at f(f+1)/2 + y, built on the device by one FP64 GEMM; the (T)
+// path then runs on it with packed ovvv, and the packed ovvv cotangent maps
+// back to
+//   Lov_bar[P,(p,x)] = sum_pair ovvv_bar[(p,x),pair] Lvv[P,pair]
+//   Lvv_bar[P,pair]  = sum_(p,x) ovvv_bar[(p,x),pair] Lov[P,(p,x)]
+// (two more GEMMs, the same FP64 tile as the FP64 contractions).
+struct DfLayout {
+    tb::Plan P;
+    size_t off_ovvv, off_gvvv, total;
+};
+
+static int df_layout(int precision, int nocc, int nvir, int naux, int want_grad, DfLayout &L) {
+    if (naux < 1) return TRIPLES_ERR_INVALID_ARGUMENT;
+    int rc = tb::make_plan(precision, nocc, nvir, 1, want_grad, L.P);
+    if (rc != TRIPLES_OK) return rc;
+    const size_t nov = (size_t)nocc * nvir, npair = (size_t)nvir * (nvir + 1) / 2;
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    size_t off = al(L.P.total);
+    L.off_ovvv = off;
+    off = al(off + nov * npair * sizeof(double));
+    L.off_gvvv = off;
+    if (want_grad) off = al(off + nov * npair * sizeof(double));
+    L.total = off;
+    return TRIPLES_OK;
+}
+
+size_t triples_df_workspace_size(int precision, int nocc, int nvir, int naux, int want_grad) {
+    DfLayout L;
+    if (df_layout(precision, nocc, nvir, naux, want_grad, L) != TRIPLES_OK) return 0;
+    return L.total;
+}
+
+static int triples_df_call(void *stream, int precision, int nocc, int nvir, int naux, int want_grad,
+                           const double *Lov, const double *Lvv, tb::TriplesIO io, size_t workspace_bytes,
+                           double *Lov_bar, double *Lvv_bar) {
+    DfLayout L;
+    int rc = df_layout(precision, nocc, nvir, naux, want_grad, L);
+    if (rc != TRIPLES_OK) return rc;
+    if (!io.workspace || workspace_bytes < L.total) return TRIPLES_ERR_WORKSPACE;
+    if (!Lov || !Lvv || !io.mo_energy || !io.t1 || !io.t2 || !io.ovoo || !io.ovov || !io.fvo || !io.e_out)
+        return TRIPLES_ERR_INVALID_ARGUMENT;
+    if (want_grad && (!Lov_bar || !Lvv_bar || !io.mo_energy_bar || !io.t1_bar || !io.t2_bar || !io.ovoo_bar ||
+                      !io.ovov_bar || !io.fvo_bar))
+        return TRIPLES_ERR_INVALID_ARGUMENT;
+    cudaStream_t st = (cudaStream_t)stream;
+    char *ws = (char *)io.workspace;
+    double *ovvv = (double *)(ws + L.off_ovvv), *gvvv = (double *)(ws + L.off_gvvv);
+    const long long nov = (long long)nocc * nvir, npair = (long long)nvir * (nvir + 1) / 2;
+    // ovvv[px][pair] = sum_P Lov[P][px] Lvv[P][pair]
+    if ((rc = tb::gemm_plain(st, (int)nov, (int)npair, naux, Lov, 1, nov, Lvv, 1, npair, ovvv, npair, 1)) !=
+        TRIPLES_OK)
+        return rc;
+    io.ovvv = ovvv;
+    io.ovvv_bar = want_grad ? gvvv : nullptr;
+    if ((rc = tb::run_triples(L.P, st, io)) != TRIPLES_OK) return rc;
+    if (!want_grad) return TRIPLES_OK;
+    // Lov_bar[P][px] = sum_pair G[px][pair] Lvv[P][pair]
+    if ((rc = tb::gemm_plain(st, (int)nov, naux, (int)npair, gvvv, npair, 1, Lvv, npair, 1, Lov_bar, 1, nov)) !=
+        TRIPLES_OK)
+        return rc;
+    // Lvv_bar[P][pair] = sum_px G[px][pair] Lov[P][px]
+    return tb::gemm_plain(st, (int)npair, naux, (int)nov, gvvv, 1, npair, Lov, nov, 1, Lvv_bar, 1, npair);
+}
+
+int triples_energy_df(void *stream, int precision, int nocc, int nvir, int naux, const double *mo_energy,
+                      const double *t1, const double *t2, const double *ovoo, const double *ovov, const double *Lov,
+                      const double *Lvv, const double *fvo, void *workspace, size_t workspace_bytes, double *e_out) {
+    tb::TriplesIO io{};
+    io.mo_energy = mo_energy; io.t1 = t1; io.t2 = t2; io.ovoo = ovoo; io.ovov = ovov;
+    io.fvo = fvo; io.ybar = 1.0; io.workspace = workspace; io.e_out = e_out;
+    return triples_df_call(stream, precision, nocc, nvir, naux, 0, Lov, Lvv, io, workspace_bytes, nullptr, nullptr);
+}
+
+int triples_energy_vjp_df(void *stream, int precision, int nocc, int nvir, int naux, const double *mo_energy,
+                          const double *t1, const double *t2, const double *ovoo, const double *ovov,
+                          const double *Lov, const double *Lvv, const double *fvo, double ybar, void *workspace,
+                          size_t workspace_bytes, double *e_out, double *mo_energy_bar, double *t1_bar,
+                          double *t2_bar, double *ovoo_bar, double *ovov_bar, double *Lov_bar, double *Lvv_bar,
+                          double *fvo_bar) {
+    tb::TriplesIO io{};
+    io.mo_energy = mo_energy; io.t1 = t1; io.t2 = t2; io.ovoo = ovoo; io.ovov = ovov;
+    io.fvo = fvo; io.ybar = ybar; io.workspace = workspace; io.e_out = e_out;
+    io.mo_energy_bar = mo_energy_bar; io.t1_bar = t1_bar; io.t2_bar = t2_bar; io.ovoo_bar = ovoo_bar;
+    io.ovov_bar = ovov_bar; io.fvo_bar = fvo_bar;
+    return triples_df_call(stream, precision, nocc, nvir, naux, 1, Lov, Lvv, io, workspace_bytes, Lov_bar, Lvv_bar);
 }
 
 // Fixed scratch for callers that may not allocate device memory themselves

@@ -59,5 +59,7 @@ struct TriplesIO {
 
 int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan &P, int lno = 0);
 int run_triples(const Plan &P, cudaStream_t st, const TriplesIO &io);
+int gemm_plain(cudaStream_t st, int M, int N, int K, const double *A, long long ams, long long aks,
+               const double *B, long long bms, long long bks, double *C, long long cms, long long cns);
 
 }  // namespace tb

@@ -56,6 +56,21 @@ class TriplesInputs:
 
 def make_inputs(nocc: int, nvir: int, naux: int, seed: int = 0,
                 fvo_sigma: float = 0.0, scale: float = 1.0) -> TriplesInputs:
+    return _make(nocc, nvir, naux, seed, fvo_sigma, scale)[0]
+
+
+def make_df_inputs(nocc: int, nvir: int, naux: int, seed: int = 0, fvo_sigma: float = 0.0,
+                   scale: float = 1.0):
+    """make_inputs plus the DF factors its ERIs come from, in the layouts of
+    pyscfad's DF ERIs (dfccsd.py:77-78): Lov[naux, o*v] and the packed
+    Lvv[naux, v(v+1)/2] (pair f >= y at f(f+1)/2 + y).  Returns (inputs, Lov, Lvv)."""
+    inp, Lov, Lvv = _make(nocc, nvir, naux, seed, fvo_sigma, scale)
+    il, jl = np.tril_indices(nvir)
+    Lvv_tril = np.ascontiguousarray(Lvv.reshape(naux, nvir, nvir)[:, il, jl])
+    return inp, np.ascontiguousarray(Lov), Lvv_tril
+
+
+def _make(nocc, nvir, naux, seed, fvo_sigma, scale):
     rng = np.random.default_rng(seed)
     o, v = nocc, nvir
     n = o + v
@@ -77,8 +92,9 @@ def make_inputs(nocc: int, nvir: int, naux: int, seed: int = 0,
         fvo = rng.normal(0.0, fvo_sigma, (v, o))
     else:
         fvo = np.zeros((v, o))
-    return TriplesInputs(mo_energy, t1, t2, np.ascontiguousarray(ovoo),
-                         np.ascontiguousarray(ovov), np.ascontiguousarray(ovvv), fvo)
+    inp = TriplesInputs(mo_energy, t1, t2, np.ascontiguousarray(ovoo),
+                        np.ascontiguousarray(ovov), np.ascontiguousarray(ovvv), fvo)
+    return inp, Lov, Lvv
 
 
 def make_inputs_torch(nocc: int, nvir: int, naux: int, seed: int = 0,

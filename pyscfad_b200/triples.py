@@ -209,6 +209,66 @@ def lno_energy_vjp(mat, mo_energy, t1, t2, ovoo, ovov, ovvv, fvo, ybar=1.0, prec
     return e, grads
 
 
+DF_KEYS = ("mo_energy", "t1", "t2", "ovoo", "ovov", "Lov", "Lvv", "fvo")
+
+
+def _df_args(mo_energy, t1, t2, ovoo, ovov, Lov, Lvv, fvo, device):
+    args = [_as_dev(a, device) for a in (mo_energy, t1, t2, ovoo, ovov, Lov, Lvv, fvo)]
+    o, v = args[1].shape
+    naux = args[5].shape[0]
+    if args[5].numel() != naux * o * v:
+        raise ValueError(f"Lov has shape {tuple(args[5].shape)}, expected ({naux}, {o * v})")
+    if tuple(args[6].shape) != (naux, v * (v + 1) // 2):
+        raise ValueError(f"Lvv has shape {tuple(args[6].shape)}, expected ({naux}, {v * (v + 1) // 2})")
+    return args, o, v, naux
+
+
+def energy_df(mo_energy, t1, t2, ovoo, ovov, Lov, Lvv, fvo, precision="fp64", device=None, stream=None,
+              check=True) -> torch.Tensor:
+    """E(T) with ovvv built on the device from the DF factors as pyscfad's DF
+    ERIs build it (dfccsd.py:77-88): Lov[naux, o*v], Lvv[naux, v(v+1)/2] packed."""
+    lib = _lib.load()
+    device = torch.device(device or (t1.device if isinstance(t1, torch.Tensor) and t1.is_cuda else "cuda"))
+    args, o, v, naux = _df_args(mo_energy, t1, t2, ovoo, ovov, Lov, Lvv, fvo, device)
+    prec = _lib.PRECISION[precision]
+    nbytes = lib.triples_df_workspace_size(prec, o, v, naux, 0)
+    if nbytes == 0:
+        raise _lib.TriplesError(1, "triples_df_workspace_size")
+    ws = _workspace(nbytes, device)
+    e = torch.zeros((), dtype=torch.float64, device=device)
+    st = stream if stream is not None else torch.cuda.current_stream(device)
+    rc = lib.triples_energy_df(st.cuda_stream, prec, o, v, naux, *[a.data_ptr() for a in args], ws.data_ptr(),
+                               ws.numel(), e.data_ptr())
+    _lib.check(rc, "triples_energy_df")
+    if check:
+        _lib.check(lib.triples_check_device_status(st.cuda_stream, ws.data_ptr()), "triples_energy_df (device)")
+    return e
+
+
+def energy_vjp_df(mo_energy, t1, t2, ovoo, ovov, Lov, Lvv, fvo, ybar=1.0, precision="fp64", device=None,
+                  stream=None, check=True):
+    """E(T) and its VJP with respect to the DF factors instead of ovvv: the
+    dict holds "Lov" [naux, o*v] and "Lvv" [naux, v(v+1)/2] (one entry per
+    packed pair) next to the other inputs' cotangents."""
+    lib = _lib.load()
+    device = torch.device(device or (t1.device if isinstance(t1, torch.Tensor) and t1.is_cuda else "cuda"))
+    args, o, v, naux = _df_args(mo_energy, t1, t2, ovoo, ovov, Lov, Lvv, fvo, device)
+    prec = _lib.PRECISION[precision]
+    nbytes = lib.triples_df_workspace_size(prec, o, v, naux, 1)
+    if nbytes == 0:
+        raise _lib.TriplesError(1, "triples_df_workspace_size")
+    ws = _workspace(nbytes, device)
+    e = torch.zeros((), dtype=torch.float64, device=device)
+    grads = {k: torch.empty_like(a) for k, a in zip(DF_KEYS, args)}
+    st = stream if stream is not None else torch.cuda.current_stream(device)
+    rc = lib.triples_energy_vjp_df(st.cuda_stream, prec, o, v, naux, *[a.data_ptr() for a in args], float(ybar),
+                                   ws.data_ptr(), ws.numel(), e.data_ptr(), *[grads[k].data_ptr() for k in DF_KEYS])
+    _lib.check(rc, "triples_energy_vjp_df")
+    if check:
+        _lib.check(lib.triples_check_device_status(st.cuda_stream, ws.data_ptr()), "triples_energy_vjp_df (device)")
+    return e, grads
+
+
 def device_status(device=None, stream=None) -> int:
     """Synchronise and return the device-side status of the last call."""
     device = torch.device(device or "cuda")

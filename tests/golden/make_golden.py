@@ -10,6 +10,7 @@ layouts), E(T), the gradients w.r.t. every input as an independent tensor
 
     python tests/golden/make_golden.py          # all fixtures
     python tests/golden/make_golden.py --lno    # the LNO fixtures only
+    python tests/golden/make_golden.py --df     # the DF-factor fixtures only
 
 The LNO fixtures hold, in addition, the projector mat and its cotangent,
 from the reference's lnoccsdt_contract / lnoccsdt_energy_vjp
@@ -75,6 +76,33 @@ def main_lno():
         print(f"{name}: E = {e:.15g}  -> {os.path.relpath(path, ROOT)}")
 
 
+# DF cases, name: (nocc, nvir, naux, seed): inputs given as the DF factors
+DF_CASES = {
+    "df_o4v9": (4, 9, 30, 21),
+    "df_o5v19": (5, 19, 60, 22),
+}
+
+
+def main_df():
+    from pyscfad_b200.synthetic import make_df_inputs
+    for name, (o, v, naux, seed) in DF_CASES.items():
+        inp, Lov, Lvv = make_df_inputs(o, v, naux, seed=seed, fvo_sigma=1e-3)
+        e, g = O.ref_energy_vjp(inp, ybar=1.0)
+        cot = O.reference_cotangents(g, o, v)
+        Lov_bar, Lvv_bar = O.df_factor_grads(cot["ovvv"], Lov, Lvv)
+        out = dict(nocc=o, nvir=v, naux=naux, seed=seed, e=e, in_Lov=Lov, in_Lvv=Lvv, grad_Lov=Lov_bar,
+                   grad_Lvv=Lvv_bar, cot_ovvv_tril=cot["ovvv"], in_ovvv_tril=inp.ovvv_tril())
+        for k in O.GRAD_KEYS:
+            if k != "ovvv":
+                out["in_" + k] = getattr(inp, k)
+                out["grad_" + k] = g[k]
+        out["in_ovvv"] = inp.ovvv
+        out["grad_ovvv"] = g["ovvv"]
+        path = os.path.join(HERE, f"{name}.npz")
+        np.savez_compressed(path, **out)
+        print(f"{name}: E = {e:.15g}  -> {os.path.relpath(path, ROOT)}")
+
+
 def main():
     if not O.ref_available():
         O.build()
@@ -97,6 +125,9 @@ def main():
 if __name__ == "__main__":
     if "--lno" in sys.argv:
         main_lno()
+    elif "--df" in sys.argv:
+        main_df()
     else:
         main()
         main_lno()
+        main_df()

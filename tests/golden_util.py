@@ -9,6 +9,7 @@ from pyscfad_b200.synthetic import TriplesInputs
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 KEYS = ("mo_energy", "t1", "t2", "ovoo", "ovov", "ovvv", "fvo")
 LNO_PREFIX = "lno_"
+DF_PREFIX = "df_"
 
 
 def _all():
@@ -17,7 +18,12 @@ def _all():
 
 def names():
     """Canonical (T) fixtures."""
-    return [n for n in _all() if not n.startswith(LNO_PREFIX)]
+    return [n for n in _all() if not n.startswith((LNO_PREFIX, DF_PREFIX))]
+
+
+def df_names():
+    """Canonical (T) fixtures whose inputs are given as DF factors (Lov, packed Lvv)."""
+    return [n for n in _all() if n.startswith(DF_PREFIX)]
 
 
 def lno_names():

@@ -80,3 +80,18 @@ def test_lno_plan_limits():
     rc = lib.triples_lno_energy(null, 0, 5, 19, 1, null, *([ctypes.c_void_p(16)] * 7), ctypes.c_void_p(16),
                                 1 << 40, ctypes.c_void_p(16))
     assert rc == 1   # mat missing
+
+
+def test_df_plan():
+    """DF-factor entry points: workspace holds the packed ovvv (and its cotangent); naux >= 1."""
+    lib = _lib.load()
+    a = lib.triples_df_workspace_size(0, 5, 19, 60, 0)
+    b = lib.triples_df_workspace_size(0, 5, 19, 60, 1)
+    assert lib.triples_workspace_size(0, 5, 19, 1, 1) < b and 0 < a < b
+    assert lib.triples_df_workspace_size(0, 5, 19, 0, 1) == 0    # naux < 1
+    null = None
+    rc = lib.triples_energy_df(null, 0, 5, 19, 60, *([null] * 8), null, 0, null)
+    assert rc == 2   # workspace check comes first on null workspace
+    rc = lib.triples_energy_df(null, 0, 5, 19, 60, *([null] * 8), ctypes.c_void_p(256), 1 << 40,
+                               ctypes.c_void_p(16))
+    assert rc == 1   # inputs missing

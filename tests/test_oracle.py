@@ -126,3 +126,49 @@ def test_lno_projector_gradient_central_differences():
         em, _ = O.np_lno_energy_vjp(inp, mat, want_grad=False)
         mat[l, i] += h
         assert abs((ep - em) / (2 * h) - g_ref["mat"][l, i]) < 1e-12 * max(1.0, abs(g_ref["mat"][l, i]))
+
+
+# ---- DF factors: ovvv_tril = Lov^T Lvv_tril (dfccsd.py:77-88) ----
+@pytest.mark.parametrize("name", ["df_o4v9"])
+def test_df_factor_gradients_match_finite_differences(name):
+    """Chain rule of the DF producer: central differences of E(T) (oracle) in a
+    few Lov and packed-Lvv entries against the fixture's factor gradients."""
+    from pyscfad_b200.synthetic import TriplesInputs
+    _, e_ref, g_ref, z = G.load(name)
+    Lov, Lvv = z["in_Lov"].copy(), z["in_Lvv"].copy()
+    o, v = int(z["nocc"]), int(z["nvir"])
+    il, jl = np.tril_indices(v)
+
+    def energy(Lov_, Lvv_):
+        tril = (Lov_.T @ Lvv_).reshape(o, v, -1)
+        full = np.zeros((o, v, v, v))
+        full[:, :, il, jl] = tril
+        full[:, :, jl, il] = tril
+        inp = TriplesInputs(z["in_mo_energy"], z["in_t1"], z["in_t2"], z["in_ovoo"], z["in_ovov"], full, z["in_fvo"])
+        return O.oracle_energy_vjp(inp, want_grad=False)[0]
+
+    assert abs(energy(Lov, Lvv) - e_ref) <= 1e-12 * abs(e_ref)
+    rng = np.random.default_rng(3)
+    for arr, gkey in ((Lov, "grad_Lov"), (Lvv, "grad_Lvv")):
+        flat = arr.reshape(-1)
+        for idx in rng.choice(flat.size, size=3, replace=False):
+            x0 = flat[idx]
+            h = 1e-4 * max(abs(x0), 1e-2)
+            flat[idx] = x0 + h
+            ep = energy(Lov, Lvv)
+            flat[idx] = x0 - h
+            em = energy(Lov, Lvv)
+            flat[idx] = x0
+            fd = (ep - em) / (2 * h)
+            ref = z[gkey].reshape(-1)[idx]
+            assert abs(fd - ref) <= 1e-6 * max(abs(ref), 1e-3 * np.abs(z[gkey]).max()), (gkey, idx, fd, ref)
+
+
+@pytest.mark.parametrize("name", ["df_o4v9", "df_o5v19"])
+def test_df_fixture_is_the_factor_chain_of_the_packed_cotangent(name):
+    _, _, _, z = G.load(name)
+    lb, vb = O.df_factor_grads(z["cot_ovvv_tril"], z["in_Lov"], z["in_Lvv"])
+    assert np.allclose(lb, z["grad_Lov"], rtol=0, atol=1e-14 * np.abs(lb).max())
+    assert np.allclose(vb, z["grad_Lvv"], rtol=0, atol=1e-14 * np.abs(vb).max())
+    o, v = int(z["nocc"]), int(z["nvir"])
+    assert np.allclose((z["in_Lov"].T @ z["in_Lvv"]).reshape(o, v, -1), z["in_ovvv_tril"], rtol=0, atol=1e-14)

@@ -57,3 +57,17 @@ def test_df_equals_ovvv_input_path():
     assert _relerr(g_d["Lvv"], Lov @ G_) < 1e-10
     e0 = triples.energy_df(inp.mo_energy, inp.t1, inp.t2, inp.ovoo, inp.ovov, Lov, Lvv, inp.fvo, device="cuda")
     assert abs(float(e0) - e_d) <= 1e-12 * abs(e_d)
+
+
+def test_df_single_auxiliary_function():
+    """naux = 1: ovvv of rank one; the factor gradients are still the chain rule."""
+    inp, Lov, Lvv = make_df_inputs(3, 7, 1, seed=4, fvo_sigma=1e-3)
+    z = {"in_mo_energy": inp.mo_energy, "in_t1": inp.t1, "in_t2": inp.t2, "in_ovoo": inp.ovoo,
+         "in_ovov": inp.ovov, "in_Lov": Lov, "in_Lvv": Lvv, "in_fvo": inp.fvo}
+    e_d, g_d = _run_df(z, "fp64")
+    e_o, g_o = triples.energy_vjp(inp.mo_energy, inp.t1, inp.t2, inp.ovoo, inp.ovov, inp.ovvv_tril(), inp.fvo,
+                                  device="cuda")
+    G_ = g_o["ovvv"].cpu().numpy().reshape(Lov.shape[1], Lvv.shape[1])
+    assert abs(e_d - float(e_o)) <= 1e-12 * max(abs(float(e_o)), 1e-12)
+    assert _relerr(g_d["Lov"], Lvv @ G_.T) < 1e-10
+    assert _relerr(g_d["Lvv"], Lov @ G_) < 1e-10

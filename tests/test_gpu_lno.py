@@ -160,3 +160,45 @@ def test_lno_mirror_kernel_autograd():
     w, U = np.linalg.eigh(z["in_mat"])
     ulo = (U[:, w > 0.5]).T
     assert abs(L.kernel(_CC(), eris, ulo) - e_ref) <= 1e-11 * abs(e_ref)
+
+
+@pytest.mark.parametrize("o,v", [(1, 1), (1, 6), (3, 1), (2, 2)])
+def test_lno_smallest_shapes(o, v):
+    """Degenerate sizes: one occupied or one virtual orbital (E vanishes
+    analytically for nocc = 1 and the gradients are rounding noise there)."""
+    inp = make_inputs(o, v, 8, seed=o * 10 + v, fvo_sigma=1e-3)
+    mat = np.random.default_rng(o + v).normal(size=(o, o))
+    e_ref, g_ref = O.np_lno_energy_vjp(inp, mat, ybar=1.3)
+    e, g = _run(inp, mat, packed=True, ybar=1.3)
+    assert abs(e - e_ref) <= 1e-12 * max(1e-3, abs(e_ref))
+    scale = max(np.abs(g_ref["t2"]).max(), 1e-7)
+    for k in KEYS:
+        ref = O.fold_ovvv_tril(g_ref[k]) if k == "ovvv" else g_ref[k]
+        assert np.abs(g[k] - ref).max() <= 1e-10 * max(np.abs(ref).max(), scale), k
+
+
+def test_lno_zero_projector_and_zero_seed():
+    """mat = 0: E = 0 and only mat_bar survives; ybar = 0: every gradient is zero."""
+    inp, e_ref, g_ref, z = G.load("lno_o4v9")
+    o = inp.nocc
+    e, g = _run(inp, np.zeros((o, o)))
+    assert e == 0.0
+    _, g_np = O.np_lno_energy_vjp(inp, np.zeros((o, o)), ybar=1.0)
+    assert _relerr(g["mat"], g_np["mat"]) < G_RTOL
+    for k in G.KEYS:
+        assert np.abs(g[k]).max() == 0.0, k
+    e, g = _run(inp, z["in_mat"], ybar=0.0)
+    assert abs(e - e_ref) <= E_RTOL * abs(e_ref)
+    for k in KEYS:
+        assert np.abs(g[k]).max() == 0.0, k
+
+
+def test_lno_bf16_rank_one_projector():
+    inp = make_inputs(5, 19, 40, seed=17, fvo_sigma=1e-3)
+    u = np.random.default_rng(5).normal(size=5)
+    mat = np.outer(u, u) / (u @ u)
+    e_ref, g_ref = _run(inp, mat, packed=True)
+    e, g = _run(inp, mat, packed=True, precision="mixed_bf16")
+    assert abs(e - e_ref) <= 1e-4 * abs(e_ref)
+    for k in KEYS:
+        assert _relerr(g[k], g_ref[k]) < 1e-3, k

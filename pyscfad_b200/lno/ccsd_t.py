@@ -29,20 +29,20 @@ def _canonical(t1T, t2T):
 
 class _LnoTriplesEnergy(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, mat, t1T, t2T, mo_energy, fvo, ovoo, ovov, ovvv):
+    def forward(ctx, precision, mat, t1T, t2T, mo_energy, fvo, ovoo, ovov, ovvv):
         t1, t2 = _canonical(t1T, t2T)
-        if any(ctx.needs_input_grad):
-            e, g = triples.lno_energy_vjp(mat, mo_energy, t1, t2, ovoo, ovov, ovvv, fvo, 1.0)
+        if any(ctx.needs_input_grad[1:]):
+            e, g = triples.lno_energy_vjp(mat, mo_energy, t1, t2, ovoo, ovov, ovvv, fvo, 1.0, precision=precision)
             ctx.grads = g
         else:
-            e = triples.lno_energy(mat, mo_energy, t1, t2, ovoo, ovov, ovvv, fvo)
+            e = triples.lno_energy(mat, mo_energy, t1, t2, ovoo, ovov, ovvv, fvo, precision=precision)
         return e
 
     @staticmethod
     def backward(ctx, ybar):
         g = ctx.grads
         s = ybar.to(torch.float64)
-        return (g["mat"] * s, g["t1"].transpose(0, 1) * s, g["t2"].permute(2, 3, 1, 0) * s,
+        return (None, g["mat"] * s, g["t1"].transpose(0, 1) * s, g["t2"].permute(2, 3, 1, 0) * s,
                 g["mo_energy"] * s, g["fvo"] * s, g["ovoo"] * s, g["ovov"] * s, g["ovvv"] * s)
 
 
@@ -53,11 +53,11 @@ def _device_of(*xs):
     return torch.device("cuda")
 
 
-def _check_memory(nocc, nvir, packed, want_grad):
+def _check_memory(nocc, nvir, packed, want_grad, precision="fp64"):
     """Error behaviour of the reference's memory checks
     (pyscfad/lno/ccsd_t.py:101-103 and 185-192): RuntimeError when the device
     cannot hold the workspace."""
-    need = triples.lno_workspace_size(nocc, nvir, packed, want_grad)
+    need = triples.lno_workspace_size(nocc, nvir, packed, want_grad, precision)
     if torch.cuda.is_available():
         free, _ = torch.cuda.mem_get_info()
         if need > free:
@@ -65,15 +65,16 @@ def _check_memory(nocc, nvir, packed, want_grad):
                                f"({free / 1e6:.0f} MB of device memory free).")
 
 
-def _ccsd_t_energy(mat, t1T, t2T, mo_energy, fvo, ovoo, ovov, ovvv, max_memory=None):
+def _ccsd_t_energy(mat, t1T, t2T, mo_energy, fvo, ovoo, ovov, ovvv, max_memory=None, *, precision="fp64"):
     """Fragment (T) energy (pyscfad/lno/ccsd_t.py:71-112), differentiable
     through autograd in every argument but max_memory (kept for the
-    signature; the device workspace is sized exactly)."""
+    signature; the device workspace is sized exactly).  ``precision`` (not in
+    the reference) selects "fp64", "mixed" or "mixed_bf16" contractions."""
     dev = _device_of(mat, t1T, t2T, mo_energy, fvo, ovoo, ovov, ovvv)
     ts = [torch.as_tensor(x).to(dev) for x in (mat, t1T, t2T, mo_energy, fvo, ovoo, ovov, ovvv)]
     nvir, nocc = ts[1].shape
-    _check_memory(nocc, nvir, ts[7].dim() == 3, any(t.requires_grad for t in ts))
-    return _LnoTriplesEnergy.apply(*ts)
+    _check_memory(nocc, nvir, ts[7].dim() == 3, any(t.requires_grad for t in ts), precision)
+    return _LnoTriplesEnergy.apply(precision, *ts)
 
 
 def _ccsd_t_energy_bwd(max_memory, res, et_bar):
@@ -90,7 +91,7 @@ def _ccsd_t_energy_bwd(max_memory, res, et_bar):
             c["ovoo"], c["ovov"], c["ovvv"])
 
 
-def kernel(mycc, eris, ulo, t1=None, t2=None, verbose=None):
+def kernel(mycc, eris, ulo, t1=None, t2=None, verbose=None, precision="fp64"):
     """Fragment (T) energy for the projector ulo (pyscfad/lno/ccsd_t.py:35-69).
     Host (numpy) inputs return a Python float, as the reference does; torch
     tensors return a 0-dim tensor that carries gradients."""
@@ -111,5 +112,5 @@ def kernel(mycc, eris, ulo, t1=None, t2=None, verbose=None):
     fock = torch.as_tensor(eris.fock).to(dev)
     fvo = fock[nocc:, :nocc].contiguous()
     et = _ccsd_t_energy(mat, t1_t.transpose(0, 1), t2_t.permute(2, 3, 1, 0), eris.mo_energy, fvo,
-                        eris.ovoo, eris.ovov, eris.ovvv, getattr(mycc, "max_memory", None))
+                        eris.ovoo, eris.ovov, eris.ovvv, getattr(mycc, "max_memory", None), precision=precision)
     return float(et) if host else et

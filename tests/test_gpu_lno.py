@@ -202,3 +202,35 @@ def test_lno_bf16_rank_one_projector():
     assert abs(e - e_ref) <= 1e-4 * abs(e_ref)
     for k in KEYS:
         assert _relerr(g[k], g_ref[k]) < 1e-3, k
+
+
+def test_lno_linear_in_projector_at_larger_size():
+    """Size-independent checks where the oracle is too slow (o=12, v=64, several
+    chunks per block edge): E is linear in mat, so E(a M1 + b M2) =
+    a E(M1) + b E(M2) and mat_bar does not depend on mat; mat = I gives the
+    canonical path's energy and gradients."""
+    inp = make_inputs(12, 64, 120, seed=31, fvo_sigma=1e-3)
+    rng = np.random.default_rng(12)
+    m1, m2 = rng.normal(size=(12, 12)), rng.normal(size=(12, 12))
+    e1, g1 = _run(inp, m1)
+    e2, g2 = _run(inp, m2)
+    e3, g3 = _run(inp, 0.5 * m1 - 2.0 * m2)
+    assert abs(e3 - (0.5 * e1 - 2.0 * e2)) <= 1e-11 * (abs(e1) + 4 * abs(e2))
+    assert _relerr(g3["mat"], g1["mat"]) < 1e-10 and _relerr(g2["mat"], g1["mat"]) < 1e-10
+    for k in G.KEYS:
+        assert _relerr(g3[k], 0.5 * g1[k] - 2.0 * g2[k]) < 1e-9, k
+    e_i, g_i = _run(inp, np.eye(12))
+    e_c, g_c = triples.energy_vjp(inp.mo_energy, inp.t1, inp.t2, inp.ovoo, inp.ovov, inp.ovvv_tril(), inp.fvo,
+                                  device="cuda")
+    assert abs(e_i - float(e_c)) <= 1e-12 * abs(float(e_c))
+    for k in G.KEYS:
+        assert _relerr(g_i[k], g_c[k].cpu().numpy()) < 1e-10, k
+
+
+def test_lno_mirror_mixed_precision_keyword():
+    from pyscfad_b200.lno import ccsd_t as L
+
+    inp, e_ref, _, z = G.load("lno_o5v19")
+    e = L._ccsd_t_energy(z["in_mat"], inp.t1.T, inp.t2.transpose(2, 3, 1, 0), inp.mo_energy, inp.fvo, inp.ovoo,
+                         inp.ovov, inp.ovvv_tril(), None, precision="mixed")
+    assert abs(float(e) - e_ref) <= 1e-6 * abs(e_ref)

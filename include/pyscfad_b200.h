@@ -121,6 +121,14 @@ int triples_lno_energy_vjp(void *stream, int precision, int nocc, int nvir, int 
                            double *ovoo_bar, double *ovov_bar, double *ovvv_bar,
                            double *fvo_bar);
 
+/* Introspection (host only, no GPU): the gather tables and de-duplication
+ * patterns of the LNO orbit tiles, as the library builds them, copied into
+ * `out` when `bytes` suffices; returns the size needed.  Layout: six
+ * sigma-permuted slot maps [6][64], two r3 slot maps [2][6][64] (slots padded
+ * as s + 3 (s / 16)), candidate maps [36][6] and [2][36][6] (a 16-byte aligned
+ * block of 1808 bytes), then 16 patterns of {nslab, cand[36], prim[36]}. */
+size_t triples_lno_tables(void *out, size_t bytes);
+
 /* Density-fitted inputs: the ovvv operand comes from the DF factors as the
  * reference's DF ERIs build it (pyscfad/cc/dfccsd.py:77-88):
  *   Lov[naux, o*v]          = Lpq[:, :o, o:]

@@ -1501,6 +1501,20 @@ int triples_lno_energy_vjp(void *stream, int precision, int nocc, int nvir, int 
     return triples_lno_call(stream, precision, nocc, nvir, ovvv_packed, 1, io, workspace_bytes);
 }
 
+// ---- LNO host tables (introspection) ----
+size_t triples_lno_tables(void *out, size_t bytes) {
+    const size_t need = sizeof(tb::LnoTables) + 16 * sizeof(tb::LnoPattern);
+    if (out && bytes >= need) {
+        tb::LnoTables t;
+        tb::LnoPattern pats[16];
+        tb::lno_build_tables(t);
+        tb::lno_build_patterns(pats);
+        std::memcpy(out, &t, sizeof(t));
+        std::memcpy((char *)out + sizeof(t), pats, sizeof(pats));
+    }
+    return need;
+}
+
 // ---- density-fitted ERI producer ----
 // ovvv[(p,x), pair] = sum_P Lov[P,(p,x)] Lvv[P,pair]  (pyscfad/cc/dfccsd.py:77-88), packed
 // pairs f >= y at f(f+1)/2 + y, built on the device by one FP64 GEMM; the (T)

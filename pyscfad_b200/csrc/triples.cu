@@ -161,6 +161,12 @@ int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan
     d.v = nvir;
     d.n = nocc + nvir;
     d.Tv = choose_tv(nocc, nvir);
+    if (lno) {
+        // the projected epilogue keeps whole-chunk FP64 work arrays (6 o^3 Tv^3
+        // values each at most): halve the block until they fit the budget
+        const double o3 = (double)nocc * nocc * nocc;
+        while (d.Tv > 4 && kLnoArrays * 6.0 * o3 * d.Tv * d.Tv * d.Tv * sizeof(double) > kLnoBudgetBytes) d.Tv >>= 1;
+    }
     d.Kp = nvir;
     P.Kp8 = (nvir + 7) / 8 * 8;
     P.Op8 = (nocc + 7) / 8 * 8;
@@ -219,8 +225,17 @@ int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan
     P.off_ijk = take((size_t)P.n_ijk * 3 * sizeof(int));
     P.off_epart = take((size_t)P.n_ijk * P.f2_gy * el);
     if (P.lno) {
-        // WW / Wbar-of-WW, X / VVbar, Q, Wt / Zbar: whole-chunk FP64 arrays
-        for (int k = 0; k < 4; k++) P.off_L[k] = take(P.stage_elems * el);
+        // whole-chunk FP64 arrays: WW / P^T(Wtbar) / vbar (0), Pt(Q) (1), Q / Dbar (2),
+        // Zbar (3); the energy alone needs only 0 and 2
+        P.off_L[0] = take(P.stage_elems * el);
+        P.off_L[2] = take(P.stage_elems * el);
+        if (want_grad) {
+            P.off_L[1] = take(P.stage_elems * el);
+            P.off_L[3] = take(P.stage_elems * el);
+        } else {
+            P.off_L[1] = P.off_L[0];
+            P.off_L[3] = P.off_L[2];
+        }
         P.off_lpart = take((size_t)6 * kLnoGrid * el);
     }
     P.total = off;

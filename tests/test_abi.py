@@ -95,3 +95,15 @@ def test_df_plan():
     rc = lib.triples_energy_df(null, 0, 5, 19, 60, *([null] * 8), ctypes.c_void_p(256), 1 << 40,
                                ctypes.c_void_p(16))
     assert rc == 1   # inputs missing
+
+
+def test_lno_workspace_fits_one_b200_at_the_largest_fragments():
+    """The projected epilogue's whole-chunk arrays grow as nocc^3 Tv^3: the
+    plan halves the virtual block for large nocc so that the workspace stays
+    well inside 180 GB, and energy-only calls keep two of the four arrays."""
+    lib = _lib.load()
+    for prec in (0, 1):
+        for o, v in ((40, 360), (48, 200), (64, 400)):
+            grad = lib.triples_lno_workspace_size(prec, o, v, 1, 1)
+            energy = lib.triples_lno_workspace_size(prec, o, v, 1, 0)
+            assert 0 < energy < grad < 150e9, (prec, o, v, grad)

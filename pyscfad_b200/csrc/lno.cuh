@@ -17,11 +17,12 @@
 // r, z), p outermost, "column" = everything after p):
 //   1. tile forward  (orbit tiles in shared memory): WW -> B0, Q -> B2
 //   2. projection    (streaming over columns, all p of a column in a tile):
-//                    energy; with the adjoint also mat_bar, Dbar -> mo_bar,
+//                    energy; with the adjoint also mat_bar, Dbar -> B2 (over Q),
 //                    Zbar -> B3 and P^T(Wtbar) -> B1
 //   3. tile adjoint  (orbit tiles): Xbar, WWbar, VVbar, their orbit sums;
-//                    wbar -> FP64 Wbar staging, vbar -> B0
-//   4. V gradients   (streaming over (r, z) rows of vbar)
+//                    wbar -> Wbar staging of the adjoint contractions, vbar -> B0
+//   4. V gradients   (streaming over (r, z) rows of vbar and Dbar): the V-term
+//                    gradients and the Dbar reduction into mo_energy_bar
 // An orbit tile is one occupied representative i >= j >= k with all its
 // permutations, times one triple of virtual sub-blocks with all its
 // orderings: closed under the simultaneous permutations of the orbit sums and

@@ -11,7 +11,7 @@ constexpr int kF2Threads = 256;   // chunk-epilogue block size
 constexpr int kMaxTv = 16;        // largest virtual block
 constexpr int kMaxCols = 1024;    // largest nocc * Tv (one staged (r, z) row)
 constexpr int kCtrlBytes = 256;   // control block at workspace offset 0
-constexpr int kLnoGrid = 1184;    // LNO kernels: blocks per ordering (8 per SM)
+constexpr int kLnoGrid = 1184;    // LNO streaming kernels: most blocks per ordering (energy partials)
 constexpr int kLnoArrays = 4;     // LNO whole-chunk FP64 work arrays (with the adjoint)
 constexpr double kLnoBudgetBytes = 96e9;   // their largest total before the block size is halved
 

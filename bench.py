@@ -67,6 +67,31 @@ def job_throughput(world, steps, flops_per_step, t_max):
     return world * steps * flops_per_step / t_max / 1e12
 
 
+# Wall-clock plan of one bench run.  A headline step (E+VJP at o=40, v=360)
+# takes tens of seconds, so the requested --steps/--warmup may not fit the
+# run's wall-clock budget; the plan keeps at least MIN_WARMUP warm-up steps
+# (the first one carries the library's one-time set-up) and times as many of
+# the requested steps as the budget allows, reporting the count it timed.
+MIN_WARMUP = 3
+
+
+def plan_steps(step_s, elapsed_s, steps, warmup, budget_s, reserve_s, e2e_max=2):
+    """(warm-up steps in total, timed steps, e2e steps) for a step of step_s
+    seconds, elapsed_s seconds already spent (one warm-up step included),
+    `steps`/`warmup` requested, budget_s for the whole run and reserve_s kept
+    for the CPU leg and the output.  Never fewer than one timed and one e2e
+    step; warm-up min(warmup, MIN_WARMUP) when warmup >= 1."""
+    step_s = max(float(step_s), 1e-6)
+    warm = max(1, min(int(warmup), MIN_WARMUP)) if warmup >= 1 else 1
+    left = budget_s - elapsed_s - reserve_s - (warm - 1) * step_s
+    e2e = max(1, min(e2e_max, int(steps)))
+    timed = int(max(0.0, left - e2e * step_s * 1.1) // step_s)
+    timed = max(1, min(int(steps), timed))
+    if timed < e2e:
+        e2e = timed
+    return warm, timed, e2e
+
+
 def algorithmic_flops(o, v):
     """Per step and per kernel class (the tensor contractions only)."""
     main = 2.0 * o ** 3 * v ** 4
@@ -158,31 +183,36 @@ def cpu_reference_measure(o, v, target_s=8.0):
 
 
 def run_reference(args, o, v, rank):
+    """The reference's CPU kernels on the host cores, measured ONCE: a full
+    step at o=40, v=360 would take hours on the CPU, so the step time is
+    extrapolated from one bounded job sample (forward slice + backward slice,
+    both the reference's own C code).  Repeating an extrapolation adds
+    nothing, so --steps/--warmup do not repeat it; the line says so."""
     if rank != 0:
         return
-    res = None
-    times = []
-    for i in range(args.warmup + args.steps):
-        res = cpu_reference_measure(o, v, args.cpu_target)
-        if "error" in res:
-            print(json.dumps({"impl": "reference", "unavailable": res["error"]}))
-            return
-        if i >= args.warmup:
-            times.append(res["t_full_s"])
-    t = max(times)
+    t_start = time.perf_counter()
+    res = cpu_reference_measure(o, v, args.cpu_target)
+    if "error" in res:
+        print(json.dumps({"impl": "reference", "unavailable": res["error"]}))
+        return
+    t = res["t_full_s"]
     flops = algorithmic_flops(o, v)["step"]
     val = flops / t / 1e12
     line = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": "TFLOP/s", "n_gpus": 0,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+        "steps": 1, "warmup": 0, "steps_requested": args.steps, "warmup_requested": args.warmup,
+        "ms_per_step": t * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA,
         "config": {"workload": args.workload, "nocc": o, "nvir": v, "naux": WORKLOADS[args.workload][2],
-                   "path": "reference CPU C kernels (ccsd_t_energy_vjp + LNO forward with mat=I)"},
+                   "path": "reference CPU C kernels (ccsd_t_energy_vjp + LNO forward with mat=I)",
+                   "timing": ("one bounded job sample extrapolated to the full step (measured once; "
+                              "warm-up does not apply to an extrapolation)"),
+                   "sample_wall_s": round(time.perf_counter() - t_start, 1)},
         "cpu_baseline": {"value": val, "unit": "TFLOP/s", "cores": res["cores"], "kind": "reference",
                          "sample": res["sample"]},
         "e2e": {"value": val, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    print(json.dumps(line))
+    print(json.dumps(line), flush=True)
 
 
 # ---------------------------------------------------------------------------
@@ -473,6 +503,7 @@ def run_lno(args, o, v, naux):
 
 
 def main():
+    t_start = time.perf_counter()
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=1)
@@ -481,9 +512,16 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "mixed_bf16", "fp64"])
     ap.add_argument("--workload", default=None, choices=sorted(WORKLOADS),
                     help="default large_o40v360 (medium_o20v180 with --lno)")
+    ap.add_argument("--shape", type=int, nargs=3, metavar=("NOCC", "NVIR", "NAUX"), default=None,
+                    help="a custom (nocc, nvir, naux) instead of --workload (small cases for profiler captures)")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--cpu-target", type=float, default=8.0, help="seconds per CPU backward sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--budget", type=float, default=1450.0,
+                    help="wall-clock seconds the whole run may take; timed steps beyond it are not run "
+                         "(the line reports the count timed)")
+    ap.add_argument("--cpu-reserve", type=float, default=150.0,
+                    help="seconds of the budget kept for the CPU-baseline leg")
     ap.add_argument("--accuracy", action="store_true",
                     help="instead of timing: mixed modes vs FP64 on the same inputs (|dE|, relative "
                          "errors, FP64 summation-order noise floor), one JSON line")
@@ -506,6 +544,10 @@ def main():
     world = _env_int("WORLD_SIZE", 1)
     rank = _env_int("RANK", 0)
     local_rank = _env_int("LOCAL_RANK", 0)
+    if args.shape:
+        o, v, naux = args.shape
+        args.workload = "shape_o%dv%d" % (o, v)
+        WORKLOADS[args.workload] = (o, v, naux)
     o, v, naux = WORKLOADS[args.workload]
 
     if args.impl == "reference":
@@ -550,15 +592,22 @@ def main():
         e, g = triples.energy_vjp(*dev_args, ybar=1.0, precision=args.precision, device=dev, check=False)
         return e, g
 
-    # warm-up
-    for _ in range(args.warmup):
-        e, g = step()
+    # first warm-up step (one-time set-up included) sizes the plan; every rank
+    # takes the same plan (the slowest rank's step time)
+    w0 = time.perf_counter()
+    e, g = step()
     torch.cuda.synchronize()
-    st = _lib.load().triples_check_device_status(torch.cuda.current_stream(dev).cuda_stream,
-                                                 triples._workspaces[(dev.type, dev.index)].data_ptr())
-    _lib.check(st, "warm-up")
-    e_val = float(e)
+    step_s = max_over_ranks(time.perf_counter() - w0, dev)
     del g
+    reserve = 0.0 if (args.no_cpu_baseline or world > 1) else args.cpu_reserve
+    n_warm, n_steps, n_e2e = plan_steps(step_s, time.perf_counter() - t_start, args.steps, args.warmup,
+                                        args.budget, reserve)
+    for _ in range(n_warm - 1):
+        e, g = step()
+        del g
+    torch.cuda.synchronize()
+    _lib.check(triples.device_status(dev), "warm-up")
+    e_val = float(e)
 
     # timed region: inputs resident in HBM
     clocks = ClockSampler(local_rank)
@@ -570,8 +619,9 @@ def main():
     s1 = torch.cuda.Event(enable_timing=True)
     s0.record()
     torch.cuda.nvtx.range_push("timed_steps")   # lets a profiler select exactly the timed launches
-    for _ in range(args.steps):
+    for _ in range(n_steps):
         e, g = step()
+        del g
     torch.cuda.nvtx.range_pop()
     s1.record()
     torch.cuda.synchronize()
@@ -587,38 +637,36 @@ def main():
     t_dev = s0.elapsed_time(s1) / 1e3
     t_dev = max_over_ranks(t_dev, dev)
     _lib.check(triples.device_status(dev), "timed steps")
-    del g
 
     flops = algorithmic_flops(o, v)
-    value = job_throughput(world, args.steps, flops["step"], t_dev)
+    value = job_throughput(world, n_steps, flops["step"], t_dev)
 
-    # end-to-end through the public API with host buffers
+    # end-to-end through the public API with host buffers: pinned host inputs
+    # copied in and E plus every gradient copied out, inside the timed region
     host_in = [a.cpu().pin_memory() for a in dev_args]
     h2d = sum(a.numel() * a.element_size() for a in host_in)
-    grads_host = None
+    grads_host = {k: torch.empty(a.shape, dtype=a.dtype, pin_memory=True) for k, a in zip(keys, dev_args)}
+    e_host = torch.empty((), dtype=torch.float64, pin_memory=True)
+    d2h = 8 + sum(t.numel() * t.element_size() for t in grads_host.values())
     barrier()
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record()
-    d2h = 0
-    for _ in range(args.steps):
+    for _ in range(n_e2e):
         dev_in = [a.to(dev, non_blocking=True) for a in host_in]
         ee, gg = triples.energy_vjp(*dev_in, ybar=1.0, precision=args.precision, device=dev, check=False)
-        if grads_host is None:
-            grads_host = {k: torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for k, t in gg.items()}
-            e_host = torch.empty((), dtype=torch.float64, pin_memory=True)
         e_host.copy_(ee, non_blocking=True)
         for k in keys:
             grads_host[k].copy_(gg[k], non_blocking=True)
-        d2h = 8 + sum(t.numel() * t.element_size() for t in gg.values())
         del dev_in, gg
     e1.record()
     torch.cuda.synchronize()
     barrier()
     t_e2e = e0.elapsed_time(e1) / 1e3
     t_e2e = max_over_ranks(t_e2e, dev)
-    e2e_value = job_throughput(world, args.steps, flops["step"], t_e2e)
+    e2e_value = job_throughput(world, n_e2e, flops["step"], t_e2e)
+    del host_in
 
     # roofline of the dominant kernel class
     peaks = {}
@@ -652,12 +700,12 @@ def main():
             continue
         avg_s = ms / 1e3 / cnt
         if k in flops and k != "step":
-            ach = flops[k] * args.steps / cnt / avg_s / 1e12
+            ach = flops[k] * n_steps / cnt / avg_s / 1e12
             ent = {"bound": "tensor", "achieved": ach, "peak": tpeak, "unit": "TFLOP/s", "frac": ach / tpeak}
             if args.precision != "fp64":
                 ent["frac_emulated"] = ach / (tpeak / 3)   # 3 split products per FP32-level product
         elif k in algo_bytes:
-            ach = algo_bytes[k] * args.steps / cnt / avg_s / 1e9
+            ach = algo_bytes[k] * n_steps / cnt / avg_s / 1e9
             ent = {"bound": "hbm", "achieved": ach, "peak": hpeak, "unit": "GB/s", "frac": ach / hpeak}
         else:
             continue
@@ -674,8 +722,9 @@ def main():
                            for k, c in classes.items()}
 
     line = {
-        "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": t_dev / args.steps * 1e3, "higher_is_better": True,
+        "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": n_steps,
+        "warmup": n_warm, "steps_requested": args.steps, "warmup_requested": args.warmup,
+        "ms_per_step": t_dev / n_steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else (
             "fp16x3-split f32acc, f64 epilogue" if args.precision == "mixed" else "bf16x3-split f32acc, f64 epilogue"),
@@ -683,10 +732,14 @@ def main():
         "config": {"workload": args.workload, "nocc": o, "nvir": v, "naux": naux, "precision": args.precision,
                    "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (packed ovvv %.1f GB)" % (inp["ovvv"].numel() * 8 / 1e9),
-                   "e_t": e_val},
-        "e2e": {"value": e2e_value, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                   "e_t": e_val,
+                   "step_plan": ("warm-up %d, timed %d of %d requested, e2e %d: the steps that fit a %d s "
+                                 "wall-clock budget at %.1f s per step" % (n_warm, n_steps, args.steps, n_e2e,
+                                                                           args.budget, step_s))},
+        "e2e": {"value": e2e_value, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "steps": n_e2e},
         "gpu_launches": int(sum(c for _, c in prof.values())),
-        "triplets_per_s": world * args.steps * (o * (o + 1) * (o + 2) // 6) / t_dev,
+        "triplets_per_s": world * n_steps * (o * (o + 1) * (o + 2) // 6) / t_dev,
         "kernel_ms": {k: round(m, 3) for k, (m, _) in prof.items()},
         "roofline": roof,
         "clocks": clk,

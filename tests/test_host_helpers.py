@@ -50,3 +50,15 @@ def test_flop_and_byte_accounting():
     assert b64["lno_tile_adj"] == 32 and b32["lno_tile_adj"] == 28
     assert b64["lno_projection"] == b32["lno_projection"] == 40
     assert b64["lno_vgrad"] == 16
+
+
+@pytest.mark.parametrize("step_s", [0.5, 10.0, 40.0, 77.0, 300.0])
+def test_step_plan_fits_the_wall_clock_budget(step_s):
+    """The bench's plan: at least three warm-up steps when asked for >= 3, at
+    least one timed and one e2e step, and no more steps than the budget holds."""
+    budget, reserve, elapsed = 1450.0, 150.0, 60.0 + step_s
+    warm, timed, e2e = bench.plan_steps(step_s, elapsed, 20, 5, budget, reserve)
+    assert warm == 3 and 1 <= timed <= 20 and 1 <= e2e <= min(2, timed)
+    if timed > 1:   # everything planned fits (one timed step is the floor)
+        assert elapsed + (warm - 1 + timed + e2e) * step_s + reserve <= budget
+    assert bench.plan_steps(step_s, 1.0, 4, 1, 1e9, 0.0) == (1, 4, 2)

@@ -314,26 +314,19 @@ def run_accuracy(args, o, v, naux):
     stream = torch.cuda.current_stream(dev)
 
     def run(prec, tv=0):
-        triples.set_block_size(tv)
-        triples.set_chunk_range(a0, a1)
-        try:
-            t0 = torch.cuda.Event(enable_timing=True)
-            t1 = torch.cuda.Event(enable_timing=True)
-            t0.record(stream)
-            e, g = triples.energy_vjp(*xs, ybar=1.0, precision=prec, device=dev)
-            t1.record(stream)
-            torch.cuda.synchronize()
-        finally:
-            triples.set_block_size(0)
-            triples.set_chunk_range(0, 0)
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        e, g = triples.energy_vjp(*xs, ybar=1.0, precision=prec, device=dev, block_size=tv,
+                                  chunk_range=(a0, a1))
+        t1.record(stream)
+        torch.cuda.synchronize()
         return float(e), {k: t.cpu().numpy() for k, t in g.items()}, t0.elapsed_time(t1) / 1e3
 
     if args.slice:   # one-time set-up of both paths outside the timed calls
-        triples.set_chunk_range(0, 1)
         for prec in ("fp64", "mixed", "mixed_bf16"):
-            triples.energy_vjp(*xs, ybar=1.0, precision=prec, device=dev)
+            triples.energy_vjp(*xs, ybar=1.0, precision=prec, device=dev, chunk_range=(0, 1))
         torch.cuda.synchronize()
-        triples.set_chunk_range(0, 0)
     e64, g64, t64 = run("fp64", 16)
     e64b = e64 if args.slice else run("fp64", 8)[0]
 

@@ -5,6 +5,12 @@
  * Every entry point takes plain device pointers, sizes and a cudaStream_t
  * (passed as void*), allocates nothing itself unless stated, never
  * synchronises the stream, and returns a triples_status (0 = success).
+ * The library keeps no settings between calls: everything that shapes a
+ * call arrives with it (arguments, triples_options), so host threads may
+ * call it concurrently on different streams and workspaces (the reference's
+ * C kernels are likewise re-entrant).  The first call on a device does a
+ * one-time set-up (kernel attributes, constant tables) under a lock; make it
+ * before any stream capture.
  *
  * Array layouts are the reference's canonical ones (C order, FP64), i.e. the
  * leaves of pyscfad's ERI pytree and the CCSD amplitudes:
@@ -54,10 +60,32 @@ enum triples_precision {
     TRIPLES_PRECISION_MIXED_BF16 = 2  /* same with unscaled bf16 hi/lo splits (~16-bit) */
 };
 
+/* Per-call settings of triples_energy_vjp_ex / triples_workspace_size_ex.
+ * All zero (or a NULL pointer) gives the defaults the plain entry points use. */
+typedef struct triples_options {
+    /* virtual block size Tv of the chunk decomposition: 0 = default (16);
+     * rounded down to a power of two, clamped to [1,16] and to nocc*Tv <= 1024.
+     * Changes the workspace size and the FP64 summation order, nothing else. */
+    int block_size;
+    /* only the chunks whose largest virtual block index lies in
+     * [chunk_a0, chunk_a1) (chunk_a1 <= 0: no upper bound); (0, 0) = the whole
+     * problem.  The energy and gradients are then the partial sums over those
+     * chunks, which add up exactly over a partition of the blocks.  With
+     * Tv = 16, block A holds the virtual indices [16A, 16A+16), so slice
+     * [A, A+1) is the reference's job range a in [16A, 16A+16), b0 = 0,
+     * b1 = a1 of ccsd_t_energy_vjp (pyscfadlib/pyscfadlib/vjp/cc/ccsd_t_vjp.c:332-346). */
+    int chunk_a0, chunk_a1;
+    /* mixed precision: 64-wide K blocks the tensor cores accumulate in FP32
+     * before the partial result is added in higher precision; 0 = default (1). */
+    int accumulation_segment;
+} triples_options;
+
 /* Bytes of device workspace the calls below need for this problem.
  * want_grad = 0 sizes triples_energy, 1 sizes triples_energy_vjp. */
 size_t triples_workspace_size(int precision, int nocc, int nvir, int ovvv_packed,
                               int want_grad);
+size_t triples_workspace_size_ex(int precision, int nocc, int nvir, int ovvv_packed,
+                                 int want_grad, const triples_options *opt);
 
 /* E(T) into *e_out (device FP64 scalar).
  * Replaces the forward of pyscfad/cc/ccsd_t.py:37-42 (pyscf's ccsd_t.kernel). */
@@ -86,6 +114,21 @@ int triples_energy_vjp(void *stream, int precision, int nocc, int nvir, int ovvv
                        double *mo_energy_bar, double *t1_bar, double *t2_bar,
                        double *ovoo_bar, double *ovov_bar, double *ovvv_bar,
                        double *fvo_bar);
+
+/* triples_energy (want_grad = 0; gradient pointers may be NULL) or
+ * triples_energy_vjp (want_grad = 1) with per-call settings `opt` (NULL =
+ * defaults); the workspace is sized by triples_workspace_size_ex with the
+ * same `opt`. */
+int triples_energy_vjp_ex(void *stream, int precision, int nocc, int nvir, int ovvv_packed,
+                          const double *mo_energy, const double *t1, const double *t2,
+                          const double *ovoo, const double *ovov, const double *ovvv,
+                          const double *fvo, double ybar, int want_grad,
+                          const triples_options *opt,
+                          void *workspace, size_t workspace_bytes,
+                          double *e_out,
+                          double *mo_energy_bar, double *t1_bar, double *t2_bar,
+                          double *ovoo_bar, double *ovov_bar, double *ovvv_bar,
+                          double *fvo_bar);
 
 /* LNO (T): the triples energy of a local-natural-orbital fragment, in which
  * the first occupied index of the projected amplitude runs through the
@@ -128,6 +171,23 @@ int triples_lno_energy_vjp(void *stream, int precision, int nocc, int nvir, int 
  * as s + 3 (s / 16)), candidate maps [36][6] and [2][36][6] (a 16-byte aligned
  * block of 1808 bytes), then 16 patterns of {nslab, cand[36], prim[36]}. */
 size_t triples_lno_tables(void *out, size_t bytes);
+
+/* The LNO calls with per-call settings (triples_options; NULL = defaults;
+ * want_grad = 0 computes the energy alone and ignores the gradient
+ * pointers). */
+size_t triples_lno_workspace_size_ex(int precision, int nocc, int nvir, int ovvv_packed,
+                                     int want_grad, const triples_options *opt);
+
+int triples_lno_energy_vjp_ex(void *stream, int precision, int nocc, int nvir, int ovvv_packed,
+                              const double *mat, const double *mo_energy, const double *t1,
+                              const double *t2, const double *ovoo, const double *ovov,
+                              const double *ovvv, const double *fvo, double ybar, int want_grad,
+                              const triples_options *opt,
+                              void *workspace, size_t workspace_bytes,
+                              double *e_out, double *mat_bar,
+                              double *mo_energy_bar, double *t1_bar, double *t2_bar,
+                              double *ovoo_bar, double *ovov_bar, double *ovvv_bar,
+                              double *fvo_bar);
 
 /* Density-fitted inputs: the ovvv operand comes from the DF factors as the
  * reference's DF ERIs build it (pyscfad/cc/dfccsd.py:77-88):
@@ -173,10 +233,13 @@ int triples_energy_vjp_df(void *stream, int precision, int nocc, int nvir, int n
  * nvir up to 41).
  * The first call on a device looks up the array's device address and does the
  * library's one-time kernel set-up; make that first call before any stream
- * capture.  Each call clears the parts of the scratch that must start at zero.
- * All calls share the one array: calls whose GPU work overlaps (other streams,
- * other host threads) race and must be serialised by the caller.  Inputs,
- * outputs and results are exactly those of triples_energy_vjp. */
+ * capture.  The address is cached per device for the life of the process
+ * (it assumes the device's primary context is not reset).  Each call clears
+ * the parts of the scratch that must start at zero.  All calls share the one
+ * array: calls whose GPU work overlaps (other streams, other host threads)
+ * race and must be serialised by the caller.  Inputs, outputs and results are
+ * exactly those of triples_energy_vjp; triples_static_check_device_status
+ * reports device-side failures of the last static call. */
 int triples_energy_vjp_static(void *stream, int precision, int nocc, int nvir, int ovvv_packed,
                               const double *mo_energy, const double *t1, const double *t2,
                               const double *ovoo, const double *ovov, const double *ovvv,
@@ -191,40 +254,30 @@ int triples_energy_vjp_static(void *stream, int precision, int nocc, int nvir, i
  * TRIPLES_ERR_DEVICE_TIMEOUT. */
 int triples_check_device_status(void *stream, const void *workspace);
 
+/* triples_check_device_status for the fixed scratch of
+ * triples_energy_vjp_static on the current device. */
+int triples_static_check_device_status(void *stream);
+
+/* Device address and size of that fixed scratch on the current device (the
+ * workspace a static call used; its control block, with the device-side
+ * error bits, sits at offset 0). */
+int triples_static_scratch(void **ptr, size_t *bytes);
+
 /* Human-readable text for a triples_status value. */
 const char *triples_status_string(int status);
 
 /* The cudaError_t of the most recent failing CUDA call on this thread. */
 int triples_last_cuda_error(void);
 
-/* Tuning: virtual block size of the chunk decomposition (0 = default 16;
- * clamped to [1,16] and to nocc*Tv <= 1024).  Affects workspace size and
- * performance, not results beyond FP64 summation order. */
-void triples_set_block_size(int tv);
-
-/* Measurement: restrict the next calls to the chunks whose largest virtual
- * block index lies in [a0, a1) (a1 <= 0: no upper bound; (0, 0) restores the
- * full problem).  The energy and gradients are then the partial sums over
- * those chunks, which add up exactly over a partition of the blocks; used to
- * time or compare precisions on a slice of a problem too large to run whole
- * (the reference's own slicing is ccsd_t_energy_vjp's a0/a1 job range,
- * pyscfadlib/pyscfadlib/vjp/cc/ccsd_t_vjp.c:332-346). */
-void triples_set_chunk_range(int a0, int a1);
-
-/* Measurement: when enabled, every kernel launched by the calls above is
- * bracketed by CUDA events on the caller's stream (enabling clears earlier
- * records).  triples_profile_read() synchronises on those events and fills
+/* Measurement: when enabled, every kernel launched by the calls the calling
+ * host thread makes is bracketed by CUDA events on the caller's stream
+ * (enabling clears earlier records; other threads are not affected).
+ * triples_profile_read() synchronises on this thread's events and fills
  * per-category totals (milliseconds, launch counts) for up to max_categories
  * categories; it returns the number of categories, or -1 on error. */
 void triples_profile_enable(int on);
 int triples_profile_read(int max_categories, double *ms, int *launches);
 const char *triples_profile_name(int category);
-
-/* Tuning (mixed precision): number of 64-wide K blocks the tensor cores
- * accumulate in FP32 before the partial result is added in higher precision (default 1;
- * 0 restores the default).  Shorter segments trade epilogue work for accuracy
- * on long contractions. */
-void triples_set_accumulation_segment(int kblocks);
 
 /* Version of this library, e.g. "0.1.0". */
 const char *triples_version(void);

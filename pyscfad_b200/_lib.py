@@ -19,6 +19,19 @@ _lib = None
 _c_int, _c_size, _c_double, _vp = ctypes.c_int, ctypes.c_size_t, ctypes.c_double, ctypes.c_void_p
 
 
+class Options(ctypes.Structure):
+    """triples_options (include/pyscfad_b200.h): per-call settings."""
+    _fields_ = [("block_size", _c_int), ("chunk_a0", _c_int), ("chunk_a1", _c_int),
+                ("accumulation_segment", _c_int)]
+
+
+def options(block_size=0, chunk_range=None, accumulation_segment=0):
+    """An Options value; chunk_range = (a0, a1) restricts the call to the chunks
+    whose largest virtual block index lies in [a0, a1)."""
+    a0, a1 = chunk_range if chunk_range is not None else (0, 0)
+    return Options(int(block_size), int(a0), int(a1), int(accumulation_segment))
+
+
 class TriplesError(RuntimeError):
     """A C-ABI entry point returned a non-zero triples_status."""
 
@@ -47,6 +60,21 @@ def load():
     lib.triples_energy_vjp.restype = _c_int
     lib.triples_energy_vjp.argtypes = ([_vp, _c_int, _c_int, _c_int, _c_int] + [_vp] * 7 +
                                        [_c_double, _vp, _c_size, _vp] + [_vp] * 7)
+    _opt = ctypes.POINTER(Options)
+    lib.triples_workspace_size_ex.restype = _c_size
+    lib.triples_workspace_size_ex.argtypes = [_c_int] * 5 + [_opt]
+    lib.triples_energy_vjp_ex.restype = _c_int
+    lib.triples_energy_vjp_ex.argtypes = ([_vp, _c_int, _c_int, _c_int, _c_int] + [_vp] * 7 +
+                                          [_c_double, _c_int, _opt, _vp, _c_size, _vp] + [_vp] * 7)
+    lib.triples_lno_workspace_size_ex.restype = _c_size
+    lib.triples_lno_workspace_size_ex.argtypes = [_c_int] * 5 + [_opt]
+    lib.triples_lno_energy_vjp_ex.restype = _c_int
+    lib.triples_lno_energy_vjp_ex.argtypes = ([_vp, _c_int, _c_int, _c_int, _c_int] + [_vp] * 8 +
+                                              [_c_double, _c_int, _opt, _vp, _c_size, _vp] + [_vp] * 8)
+    lib.triples_static_check_device_status.restype = _c_int
+    lib.triples_static_check_device_status.argtypes = [_vp]
+    lib.triples_static_scratch.restype = _c_int
+    lib.triples_static_scratch.argtypes = [ctypes.POINTER(_vp), ctypes.POINTER(_c_size)]
     lib.triples_lno_workspace_size.restype = _c_size
     lib.triples_lno_workspace_size.argtypes = [_c_int] * 5
     lib.triples_lno_energy.restype = _c_int
@@ -73,12 +101,6 @@ def load():
     lib.triples_profile_read.argtypes = [_c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_c_int)]
     lib.triples_profile_name.restype = ctypes.c_char_p
     lib.triples_profile_name.argtypes = [_c_int]
-    lib.triples_set_accumulation_segment.restype = None
-    lib.triples_set_accumulation_segment.argtypes = [_c_int]
-    lib.triples_set_block_size.restype = None
-    lib.triples_set_block_size.argtypes = [_c_int]
-    lib.triples_set_chunk_range.restype = None
-    lib.triples_set_chunk_range.argtypes = [_c_int, _c_int]
     _lib = lib
     return lib
 

@@ -19,6 +19,7 @@ refreshes their values in place (same shapes) before the next ``run()``.
 """
 from __future__ import annotations
 
+import ctypes
 import json
 import os
 import time
@@ -69,27 +70,24 @@ class Autotuner:
         for tv in TV_CANDIDATES:
             if prob.nocc * tv > 1024:
                 continue
-            triples.set_block_size(tv)
-            try:
-                for rep in range(2):      # first call: one-time set-up; second: timed
-                    torch.cuda.synchronize()
-                    t0 = time.perf_counter()
-                    _call(lib, prec, prob, ws, stream)
-                    torch.cuda.synchronize()
-                    dt = time.perf_counter() - t0
-                times[tv] = dt
-            finally:
-                triples.set_block_size(0)
+            for rep in range(2):      # first call: one-time set-up; second: timed
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                _call(lib, prec, prob, ws, stream, tv)
+                torch.cuda.synchronize()
+                dt = time.perf_counter() - t0
+            times[tv] = dt
         tv = min(times, key=times.get)
         self.table[key] = tv
         return tv
 
 
-def _call(lib, prec, prob: _Problem, ws: torch.Tensor, stream: torch.cuda.Stream):
-    rc = lib.triples_energy_vjp(stream.cuda_stream, prec, prob.nocc, prob.nvir, int(prob.packed),
-                                *[a.data_ptr() for a in prob.inputs], 1.0, ws.data_ptr(), ws.numel(),
-                                prob.energy.data_ptr(), *[prob.grads[k].data_ptr() for k in KEYS])
-    _lib.check(rc, "triples_energy_vjp")
+def _call(lib, prec, prob: _Problem, ws: torch.Tensor, stream: torch.cuda.Stream, tv: int):
+    opt = _lib.options(block_size=tv)
+    rc = lib.triples_energy_vjp_ex(stream.cuda_stream, prec, prob.nocc, prob.nvir, int(prob.packed),
+                                   *[a.data_ptr() for a in prob.inputs], 1.0, 1, ctypes.byref(opt), ws.data_ptr(),
+                                   ws.numel(), prob.energy.data_ptr(), *[prob.grads[k].data_ptr() for k in KEYS])
+    _lib.check(rc, "triples_energy_vjp_ex")
 
 
 class BatchedTriples:
@@ -123,11 +121,9 @@ class BatchedTriples:
 
     # -- set-up ---------------------------------------------------------------
     def _size(self, prob: _Problem, tv: int) -> int:
-        triples.set_block_size(tv)
-        try:
-            return int(self.lib.triples_workspace_size(self.prec, prob.nocc, prob.nvir, int(prob.packed), 1))
-        finally:
-            triples.set_block_size(0)
+        opt = _lib.options(block_size=tv)
+        return int(self.lib.triples_workspace_size_ex(self.prec, prob.nocc, prob.nvir, int(prob.packed), 1,
+                                                      ctypes.byref(opt)))
 
     def _tune(self, tune: bool):
         stream = self.streams[0]
@@ -169,11 +165,7 @@ class BatchedTriples:
             for prob in self.problems:
                 if prob.lane != lane:
                     continue
-                triples.set_block_size(prob.tv)
-                try:
-                    _call(self.lib, self.prec, prob, self.workspaces[lane], st)
-                finally:
-                    triples.set_block_size(0)
+                _call(self.lib, self.prec, prob, self.workspaces[lane], st, prob.tv)
             join = torch.cuda.Event()
             join.record(st)
             main.wait_event(join)

@@ -111,7 +111,7 @@ __host__ __device__ inline int block_start(const Dims &d, int b) {
 
 // The six orderings of three slots, lexicographic: index = 2*first + (second is
 // the larger of the two remaining).
-__host__ __device__ inline void perm_of(int s, int out[3]) {
+__host__ __device__ constexpr inline void perm_of(int s, int out[3]) {
     const int first = s >> 1;
     const int lo = (first == 0) ? 1 : 0;
     const int hi = (first == 2) ? 1 : 2;
@@ -120,14 +120,14 @@ __host__ __device__ inline void perm_of(int s, int out[3]) {
     out[2] = (s & 1) ? lo : hi;
 }
 
-__host__ __device__ inline int perm_index(int a, int b) {
+__host__ __device__ constexpr inline int perm_index(int a, int b) {
     int lo = (a == 0) ? 1 : 0;  // smallest remaining slot
     return 2 * a + (b == lo ? 0 : 1);
 }
 
 // index of the ordering t -> P[s][P[pi][t]]
-__host__ __device__ inline int perm_compose(int s, int pi) {
-    int ps[3], pp[3];
+__host__ __device__ constexpr inline int perm_compose(int s, int pi) {
+    int ps[3] = {0, 0, 0}, pp[3] = {0, 0, 0};
     perm_of(s, ps);
     perm_of(pi, pp);
     return perm_index(ps[pp[0]], ps[pp[1]]);

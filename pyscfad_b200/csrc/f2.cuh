@@ -57,7 +57,10 @@ struct F2P {
     const double *wscale;
     double ybar;
     int want_grad;
-    double *e_part;     // energy partial of each CTA
+    double *e_part;     // energy partial of each CTA, at sub * n_ijk + rep
+    int rep0, sub0;     // first occupied representative / sub-range triple of this launch
+    int nsub_l;         // sub-range triples of this launch: block b -> sub0 + b % nsub_l, rep0 + b / nsub_l
+    int n_ijk;          // occupied representatives (stride of e_part)
     double *mo_bar, *t1_bar, *fvo_bar, *ovov_bar, *t2_bar;
 };
 
@@ -82,7 +85,7 @@ __host__ __device__ constexpr size_t f2_smem_bytes() {
     return sizeof(StageT) * (36 * F2Smem<SB>::REG + 2 * F2Smem<SB>::TAB + 2 * 3 * F2Smem<SB>::NV);
 }
 
-__device__ __forceinline__ int pair_index(int sp, int sq) { return 2 * sp + (sq > sp ? sq - 1 : sq); }
+__host__ __device__ constexpr inline int pair_index(int sp, int sq) { return 2 * sp + (sq > sp ? sq - 1 : sq); }
 
 // A z run of N contiguous values moved with the widest aligned vector access:
 // one warp instruction then fills whole 32-byte sectors instead of touching
@@ -248,8 +251,11 @@ __global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4) k_f2t(F2P<S
     const Dims &d = P.d;
     const int o = d.o, v = d.v;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int rep = blockIdx.x;
-    const F2Sub &R = P.sub[blockIdx.y];
+    // linear grid, sub-range triple fastest: the blocks of one representative
+    // run together, so the two 16-byte halves of each Wbar sector meet in L2
+    const int sub = P.sub0 + (int)(blockIdx.x % (unsigned)P.nsub_l);
+    const int rep = P.rep0 + (int)(blockIdx.x / (unsigned)P.nsub_l);
+    const F2Sub &R = P.sub[sub];
     const int ijk[3] = {P.ijk[3 * rep], P.ijk[3 * rep + 1], P.ijk[3 * rep + 2]};
 
     // canonical sub-range slot of each role (identical ranges share a slot)
@@ -487,7 +493,7 @@ __global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4) k_f2t(F2P<S
             es += s_red[0][w];
             ds += s_red[1][w];
         }
-        P.e_part[blockIdx.y * gridDim.x + blockIdx.x] = es;
+        P.e_part[(long long)sub * P.n_ijk + rep] = es;
         if (P.want_grad && ds != 0.0) {
             atomicAdd(&P.mo_bar[ijk[0]], ds);
             atomicAdd(&P.mo_bar[ijk[1]], ds);

@@ -7,7 +7,9 @@
 //   A(m,k) = A.p[apply(A.mn, m) + apply(A.k, k)], likewise B, A2, B2, C.
 //
 // 128x128 output tile, 256 threads, 8x8 outputs per thread, K tiles of 8,
-// register-staged double buffering.
+// register-staged double buffering.  The k part of every operand offset is
+// tabulated per K tile in shared memory two tiles ahead (16 threads, one
+// apply() each), so the loads themselves are one add per element.
 #pragma once
 #include "common.cuh"
 
@@ -41,10 +43,11 @@ struct GemmSmem {
     double As[2][kGBK][kGBM + 1];
     double Bs[2][kGBK][kGBN + 1];
     long long rowA[kGBM], rowB[kGBN], rowA2[kGBM], rowB2[kGBN];
+    long long koff[2][2][kGBK];   // [tile parity][A, B][k in tile]: k part of the offset (-1: k >= K)
 };
 
 template <typename T>
-__device__ __forceinline__ void gemm_load_tile(const GOpT<T> &op, const long long *rows, int K, int k0,
+__device__ __forceinline__ void gemm_load_tile(const GOpT<T> &op, const long long *rows, const long long *koff,
                                                int tid, double scale, double (&r)[4]) {
 #pragma unroll
     for (int i = 0; i < 4; i++) {
@@ -57,10 +60,9 @@ __device__ __forceinline__ void gemm_load_tile(const GOpT<T> &op, const long lon
             ml = e & 127;
             kl = e >> 7;
         }
-        int k = k0 + kl;
-        long long ro = rows[ml];
+        const long long ro = rows[ml], ko = koff[kl];
         double val = 0.0;
-        if (ro >= 0 && k < K) val = (double)op.p[ro + apply(op.k, k)] * scale;
+        if (ro >= 0 && ko >= 0) val = (double)op.p[ro + ko] * scale;
         r[i] = val;
     }
 }
@@ -111,19 +113,37 @@ __device__ void gemm_fp64_tile(const GemmArgsT<TA> &g, int m0, int n0, GemmSmem 
     const int kt_total = kt1 + kt2;
     double ra[4], rb[4];
 
+    // threads 0-15 tabulate the k offsets of tile kt (A for t < 8, B for 8 <= t < 16)
+    auto tab_koff = [&](int kt) {
+        if (tid < 2 * kGBK && kt < kt_total) {
+            const int which = tid >> 3, kl = tid & 7;
+            long long off = -1;
+            if (kt < kt1) {
+                const int k = kt * kGBK + kl;
+                if (k < g.K) off = which == 0 ? apply(g.A.k, k) : apply(g.B.k, k);
+            } else {
+                const int k = (kt - kt1) * kGBK + kl;
+                if (k < g.K2) off = which == 0 ? apply(g.A2.k, k) : apply(g.B2.k, k);
+            }
+            sm.koff[kt & 1][which][kl] = off;
+        }
+    };
     auto load = [&](int kt) {
+        const long long *ka = sm.koff[kt & 1][0], *kb = sm.koff[kt & 1][1];
         if (kt < kt1) {
-            gemm_load_tile(g.A, sm.rowA, g.K, kt * kGBK, tid, 1.0, ra);
-            gemm_load_tile(g.B, sm.rowB, g.K, kt * kGBK, tid, 1.0, rb);
+            gemm_load_tile(g.A, sm.rowA, ka, tid, 1.0, ra);
+            gemm_load_tile(g.B, sm.rowB, kb, tid, 1.0, rb);
         } else {
-            int k0 = (kt - kt1) * kGBK;
-            gemm_load_tile(g.A2, sm.rowA2, g.K2, k0, tid, g.alpha2, ra);
-            gemm_load_tile(g.B2, sm.rowB2, g.K2, k0, tid, 1.0, rb);
+            gemm_load_tile(g.A2, sm.rowA2, ka, tid, g.alpha2, ra);
+            gemm_load_tile(g.B2, sm.rowB2, kb, tid, 1.0, rb);
         }
     };
     auto kfA = [&](int kt) { return kt < kt1 ? g.A.kfast : g.A2.kfast; };
     auto kfB = [&](int kt) { return kt < kt1 ? g.B.kfast : g.B2.kfast; };
 
+    tab_koff(0);
+    tab_koff(1);
+    __syncthreads();
     if (kt_total > 0) {
         load(0);
         gemm_store_tile(sm.As[0], kfA(0), tid, ra);
@@ -133,6 +153,8 @@ __device__ void gemm_fp64_tile(const GemmArgsT<TA> &g, int m0, int n0, GemmSmem 
     for (int kt = 0; kt < kt_total; kt++) {
         const int buf = kt & 1;
         if (kt + 1 < kt_total) load(kt + 1);
+        // tile kt + 2 reuses the k table of tile kt, whose loads are done
+        tab_koff(kt + 2);
 #pragma unroll
         for (int kk = 0; kk < kGBK; kk++) {
             double a[8], b[8];

@@ -4,8 +4,10 @@
 // Reference path replaced: pyscfad/cc/ccsd_t.py:28-192 (forward through
 // pyscf's ccsd_t.kernel, backward through ccsd_t_energy_vjp,
 // pyscfadlib/pyscfadlib/vjp/cc/ccsd_t_vjp.c:332-497).
+#include <atomic>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -15,6 +17,7 @@
 #include "gemm_fp64.cuh"
 #include "tc_f1.cuh"
 #include "f2.cuh"
+#include "f2s.cuh"
 #include "tc_b1.cuh"
 #include "lno.cuh"
 #include "pyscfad_b200.h"
@@ -22,11 +25,9 @@
 
 namespace tb {
 
+// Thread-local error record; every other setting travels with the call
+// (Plan, from triples_options), so concurrent calls do not interfere.
 static thread_local int g_last_cuda_error = 0;
-static int g_tv_override = 0;
-static int g_chunk_a0 = 0, g_chunk_a1 = 0;   // chunk slice by largest virtual block (a1 <= 0: all)
-static int g_kseg = 1;     // K blocks per FP32 accumulation segment of the adjoint contractions
-static int g_kseg_f1 = 1;  // same for the W contraction
 
 #define TB_CUDA(call)                                     \
     do {                                                  \
@@ -52,10 +53,12 @@ struct ProfRec {
     int cat;
     cudaEvent_t a, b;
 };
-static bool g_prof = false;
-static std::vector<ProfRec> g_prof_recs;
-static std::vector<cudaEvent_t> g_event_pool;
-static size_t g_pool_used = 0;
+// Profiling records belong to the host thread that enabled them: each
+// thread sees only the launches of its own calls.
+static thread_local bool g_prof = false;
+static thread_local std::vector<ProfRec> g_prof_recs;
+static thread_local std::vector<cudaEvent_t> g_event_pool;
+static thread_local size_t g_pool_used = 0;
 
 static cudaEvent_t prof_event() {
     if (g_pool_used == g_event_pool.size()) {
@@ -90,8 +93,8 @@ static void prof_wrap(int cat, cudaStream_t st, F &&launch) {
 // ---------------------------------------------------------------------------
 // planning
 // ---------------------------------------------------------------------------
-static int choose_tv(int o, int v) {
-    int tv = g_tv_override > 0 ? g_tv_override : 16;
+static int choose_tv(int o, int tv_request) {
+    int tv = tv_request > 0 ? tv_request : 16;
     if (tv > kMaxTv) tv = kMaxTv;
     while (tv > 1 && tv * o > kMaxCols) tv >>= 1;
     int p2 = 1;   // largest power of two <= tv
@@ -146,12 +149,22 @@ static long long chunk_stage_elems(const ChunkDesc &ch, const Dims &d) {
     return s;
 }
 
-int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan &P, int lno) {
+int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan &P, int lno,
+              const triples_options *opt) {
     if (nocc < 1 || nvir < 1 || nocc > kMaxCols || nvir > 32767) return TRIPLES_ERR_INVALID_ARGUMENT;
     if (precision < TRIPLES_PRECISION_FP64 || precision > TRIPLES_PRECISION_MIXED_BF16)
         return TRIPLES_ERR_INVALID_ARGUMENT;
     if (lno && nocc > kLnoMaxO) return TRIPLES_ERR_UNSUPPORTED;
     P = Plan{};
+    if (opt) {
+        if (opt->block_size < 0 || opt->accumulation_segment < 0 || opt->chunk_a0 < 0)
+            return TRIPLES_ERR_INVALID_ARGUMENT;
+        P.a0 = opt->chunk_a0;
+        P.a1 = opt->chunk_a1;
+        P.kseg = opt->accumulation_segment > 0 ? opt->accumulation_segment : 1;
+    } else {
+        P.kseg = 1;
+    }
     P.lno = lno ? 1 : 0;
     P.prec = precision;
     P.want_grad = want_grad ? 1 : 0;
@@ -160,7 +173,7 @@ int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan
     d.o = nocc;
     d.v = nvir;
     d.n = nocc + nvir;
-    d.Tv = choose_tv(nocc, nvir);
+    d.Tv = choose_tv(nocc, opt ? opt->block_size : 0);
     if (lno) {
         // the projected epilogue keeps whole-chunk FP64 work arrays (6 o^3 Tv^3
         // values each at most): halve the block until they fit the budget
@@ -315,16 +328,38 @@ __global__ void k_prep_B2(const double *__restrict__ t2, Dims d, double *__restr
 // ---------------------------------------------------------------------------
 // 16-bit split operands for the tensor-core path
 // ---------------------------------------------------------------------------
+// Occupied representatives i >= j >= k: first the o(o-1)(o-2)/6 with
+// i > j > k (combinatorial order), then i == j > k, i > j == k and
+// i == j == k, so the epilogue can give the all-distinct ones their own
+// kernel with one contiguous range of blocks.
+__host__ __device__ inline int n_distinct_ijk(int o) { return o * (o - 1) * (o - 2) / 6; }
+
 __global__ void k_ijk_table(int o, int *ijk) {
-    // representatives i >= j >= k, enumerated i-major
-    const int n = o * (o + 1) * (o + 2) / 6;
+    const int n = o * (o + 1) * (o + 2) / 6, nd = n_distinct_ijk(o), np = o * (o - 1) / 2;
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
-        int i = 0;
-        while ((i + 1) * (i + 2) * (i + 3) / 6 <= r) i++;
-        int rem = r - i * (i + 1) * (i + 2) / 6;
-        int j = 0;
-        while ((j + 1) * (j + 2) / 2 <= rem) j++;
-        int k = rem - j * (j + 1) / 2;
+        int i, j, k;
+        if (r < nd) {
+            i = 2;
+            while ((i + 1) * i * (i - 1) / 6 <= r) i++;   // largest i with C(i,3) <= r
+            int rem = r - i * (i - 1) * (i - 2) / 6;
+            j = 1;
+            while ((j + 1) * j / 2 <= rem) j++;             // largest j with C(j,2) <= rem
+            k = rem - j * (j - 1) / 2;
+        } else {
+            int t = r - nd;
+            const int kind = t < np ? 0 : (t < 2 * np ? 1 : 2);
+            t -= kind * np;
+            if (kind == 2) {
+                i = j = k = t;
+            } else {
+                int a = 1;
+                while ((a + 1) * a / 2 <= t) a++;           // pair a > b, b = t - C(a,2)
+                const int b = t - a * (a - 1) / 2;
+                i = a;
+                j = kind == 0 ? a : b;
+                k = b;
+            }
+        }
         ijk[3 * r] = i;
         ijk[3 * r + 1] = j;
         ijk[3 * r + 2] = k;
@@ -831,15 +866,17 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t
                                   CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
                                   CUtensorMapFloatOOBfill);
 
+static EncodeTiledFn lookup_encode_fn() {
+    void *ptr = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+        return (EncodeTiledFn)ptr;
+    return nullptr;
+}
+
 static EncodeTiledFn get_encode_fn() {
-    static EncodeTiledFn fn = nullptr;
-    if (!fn) {
-        void *ptr = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = (EncodeTiledFn)ptr;
-    }
+    static const EncodeTiledFn fn = lookup_encode_fn();   // initialised once, thread-safe
     return fn;
 }
 
@@ -880,15 +917,40 @@ static int make_tmap_stage(CUtensorMap *tm, float *base, int o, int Tx, int Ty) 
     return r == CUDA_SUCCESS ? TRIPLES_OK : TRIPLES_ERR_CUDA;
 }
 
+// SM count of the current device (cached per device; the first writers
+// store the same value, so relaxed atomics suffice).
+constexpr int kMaxDev = 64;
+static std::atomic<int> g_num_sms[kMaxDev];
+
 static int num_sms() {
-    static int n = 0;
-    if (!n) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        if (n <= 0) n = 148;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev) return 148;
+    int n = g_num_sms[dev].load(std::memory_order_relaxed);
+    if (n <= 0) {
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+        g_num_sms[dev].store(n, std::memory_order_relaxed);
     }
     return n;
+}
+
+// One-time set-up per device and kind of work (shared-memory opt-ins and
+// constant tables), under a lock so that host threads making their first
+// call at the same time do it once.  Assumes the device's primary context
+// lives as long as the process (a cudaDeviceReset would need it again).
+enum InitKind { INIT_F2_F32 = 0, INIT_F2_F64, INIT_TC, INIT_LNO, INIT_NKINDS };
+static std::mutex g_init_mu;
+static bool g_init_done[kMaxDev][INIT_NKINDS];
+
+template <typename F>
+static int once_per_device(int kind, F &&setup) {
+    int dev = 0;
+    TB_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDev) return TRIPLES_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> lk(g_init_mu);
+    if (g_init_done[dev][kind]) return TRIPLES_OK;
+    const int rc = setup();
+    if (rc == TRIPLES_OK) g_init_done[dev][kind] = true;
+    return rc;
 }
 
 // LNO chunk epilogue (FP64): energy of the projected amplitudes and, with
@@ -898,28 +960,24 @@ template <typename StageT>
 static int lno_chunk(const Plan &P, const ChunkDesc &ch, cudaStream_t st, const TriplesIO &io, char *ws,
                      Ctrl *ctrl, const StageT *S, void *SW, const int *ijk, int split) {
     {
-        constexpr int kMaxDev = 64;
-        static bool ready[kMaxDev] = {};
-        int dev = 0;
-        TB_CUDA(cudaGetDevice(&dev));
-        if (dev < 0 || dev >= kMaxDev) return TRIPLES_ERR_UNSUPPORTED;
-        if (!ready[dev]) {
+        const int rc = once_per_device(INIT_LNO, [&]() -> int {
             const int ts = (int)lno_tile_smem();
             TB_CUDA(cudaFuncSetAttribute(k_lno_tile_fwd<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, ts));
             TB_CUDA(cudaFuncSetAttribute(k_lno_tile_fwd<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, ts));
             TB_CUDA(cudaFuncSetAttribute(k_lno_tile_adj<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, ts));
             TB_CUDA(cudaFuncSetAttribute(k_lno_tile_adj<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, ts));
             TB_CUDA(cudaFuncSetAttribute(k_lno_tile_adj<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, ts));
-            static LnoTables tabs;
+            LnoTables tabs;
             lno_build_tables(tabs);
             TB_CUDA(cudaMemcpyToSymbol(c_lno_tab, &tabs, sizeof(tabs)));
-            static LnoPattern pats[16];
+            LnoPattern pats[16];
             lno_build_patterns(pats);
             TB_CUDA(cudaMemcpyToSymbol(c_lno_pat, pats, sizeof(pats)));
             const int ps = (int)lno_proj_smem(kLnoMaxO);
             TB_CUDA(cudaFuncSetAttribute(k_lno_proj, cudaFuncAttributeMaxDynamicSharedMemorySize, ps));
-            ready[dev] = true;
-        }
+            return TRIPLES_OK;
+        });
+        if (rc != TRIPLES_OK) return rc;
     }
     const Dims &d = P.d;
     LnoArgs A;
@@ -1017,21 +1075,23 @@ template <typename StageT>
 static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
     constexpr int kSB = sizeof(StageT) == 4 ? 8 : 4;   // epilogue sub-block edge
     {
-        // once per device (and element type): shared-memory opt-in and the
+        // once per device and element type: shared-memory opt-in and the
         // constant tables of the epilogue's region patterns
-        constexpr int kMaxDev = 64;
-        static bool f2_ready[kMaxDev] = {};
-        int dev = 0;
-        TB_CUDA(cudaGetDevice(&dev));
-        if (dev < 0 || dev >= kMaxDev) return TRIPLES_ERR_UNSUPPORTED;
-        if (!f2_ready[dev]) {
+        const int rc = once_per_device(sizeof(StageT) == 4 ? INIT_F2_F32 : INIT_F2_F64, [&]() -> int {
             TB_CUDA(cudaFuncSetAttribute(k_f2t<StageT, kSB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)f2_smem_bytes<StageT, kSB>()));
-            static F2Pattern pats[kF2Patterns];
+            if (sizeof(StageT) == 4) {
+                TB_CUDA(cudaFuncSetAttribute(k_f2s<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)F2sSmem::BYTES));
+                TB_CUDA(cudaFuncSetAttribute(k_f2s<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)F2sSmem::BYTES));
+            }
+            F2Pattern pats[kF2Patterns];
             f2_build_patterns(pats);
             TB_CUDA(cudaMemcpyToSymbol(c_f2pat, pats, sizeof(pats)));
-            f2_ready[dev] = true;
-        }
+            return TRIPLES_OK;
+        });
+        if (rc != TRIPLES_OK) return rc;
     }
     const Dims d = P.d;
     const bool mixed = P.prec != TRIPLES_PRECISION_FP64;
@@ -1082,10 +1142,10 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
     // 16-bit split operands and tensor maps (tensor-core path)
     constexpr int BN = 256;
     CUtensorMap tmA1, tmB1, tmA2, tmB2, tmA1m, tmA2m, tmB1z[5], tmB2z[5];
-    auto dA1mn = [&]() { static uint64_t dd[5]; dd[0] = P.Kp8; dd[1] = v; dd[2] = o; dd[3] = v; dd[4] = 2; return dd; };
-    auto dA2mn = [&]() { static uint64_t dd[5]; dd[0] = P.Op8; dd[1] = v; dd[2] = o; dd[3] = o; dd[4] = 2; return dd; };
-    auto dB1mn = [&]() { static uint64_t dd[5]; dd[0] = P.Kp8; dd[1] = v; dd[2] = o; dd[3] = o; dd[4] = 2; return dd; };
-    auto dB2mn = [&]() { static uint64_t dd[5]; dd[0] = P.Op8; dd[1] = v; dd[2] = o; dd[3] = v; dd[4] = 2; return dd; };
+    const uint64_t dA1mn[5] = {(uint64_t)P.Kp8, v, o, v, 2};
+    const uint64_t dA2mn[5] = {(uint64_t)P.Op8, v, o, o, 2};
+    const uint64_t dB1mn[5] = {(uint64_t)P.Kp8, v, o, o, 2};
+    const uint64_t dB2mn[5] = {(uint64_t)P.Op8, v, o, v, 2};
     if (mixed) {
         const long long npair = (long long)v * (v + 1) / 2;
         TB_KLAUNCH(P_PREP, k_absmax<<<grid1d((long long)o * v * (P.packed ? npair : (long long)v * v), 256), 256, 0, st>>>(
@@ -1135,18 +1195,17 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
             // second operands of the adjoint contractions (MN-major boxes)
             const uint32_t bX[5] = {64, 16, 4, 1, 1};
             int rc;
-            if ((rc = make_tmap5(&tmA1m, ws + P.off_A1h, bf16, dA1mn(), bX)) != TRIPLES_OK) return rc;
-            if ((rc = make_tmap5(&tmA2m, ws + P.off_A2h, bf16, dA2mn(), bX)) != TRIPLES_OK) return rc;
+            if ((rc = make_tmap5(&tmA1m, ws + P.off_A1h, bf16, dA1mn, bX)) != TRIPLES_OK) return rc;
+            if ((rc = make_tmap5(&tmA2m, ws + P.off_A2h, bf16, dA2mn, bX)) != TRIPLES_OK) return rc;
             for (int lt = 0; lt < 5; lt++) {
                 const uint32_t tz = 1u << lt;
                 const uint32_t bZ[5] = {64, tz, 64 / tz, 1, 1};
-                if ((rc = make_tmap5(&tmB1z[lt], ws + P.off_B1h, bf16, dB1mn(), bZ)) != TRIPLES_OK) return rc;
-                if ((rc = make_tmap5(&tmB2z[lt], ws + P.off_B2h, bf16, dB2mn(), bZ)) != TRIPLES_OK) return rc;
+                if ((rc = make_tmap5(&tmB1z[lt], ws + P.off_B1h, bf16, dB1mn, bZ)) != TRIPLES_OK) return rc;
+                if ((rc = make_tmap5(&tmB2z[lt], ws + P.off_B2h, bf16, dB2mn, bZ)) != TRIPLES_OK) return rc;
             }
             TB_CUDA(cudaMemsetAsync(SW, 0, P.wbar_elems * 4, st));
         }
-        static bool attr_set = false;
-        if (!attr_set) {
+        const int arc = once_per_device(INIT_TC, [&]() -> int {
             TB_CUDA(cudaFuncSetAttribute(k_f1_tc<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcCfg<BN>::SMEM));
             TB_CUDA(cudaFuncSetAttribute(k_b1_tc<false, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          TcB1Cfg<false, 128>::SMEM));
@@ -1156,12 +1215,13 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                                          TcB1Cfg<false, 64>::SMEM));
             TB_CUDA(cudaFuncSetAttribute(k_b1_tc<true, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          TcB1Cfg<true, 64>::SMEM));
-            attr_set = true;
-        }
+            return TRIPLES_OK;
+        });
+        if (arc != TRIPLES_OK) return arc;
     }
 
     for (int A = 0; A < P.nb; A++) {
-        if (A < g_chunk_a0 || (g_chunk_a1 > 0 && A >= g_chunk_a1)) continue;
+        if (A < P.a0 || (P.a1 > 0 && A >= P.a1)) continue;
         for (int B = 0; B <= A; B++)
             for (int C = 0; C <= B; C++) {
                 ChunkDesc ch;
@@ -1188,7 +1248,7 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                     T.wmax_bits = &ctrl->wmax_bits;
                     T.err = &ctrl->err;
                     T.bf16 = bf16 ? 1 : 0;
-                    T.kseg = g_kseg_f1;
+                    T.kseg = P.kseg;
                     for (int t = 0; t < 6; t++) T.tmS_ok[t] = 0;
                     for (int t = 0; t < ch.nperm; t++) {
                         const PermBlock &pb = ch.pb[t];
@@ -1219,27 +1279,39 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                     const int rc = lno_chunk<StageT>(P, ch, st, io, ws, ctrl, S, SW, ijk, mixed ? (bf16 ? 2 : 1) : 0);
                     if (rc != TRIPLES_OK) return rc;
                 } else {
-                    // F2: energy (+ adjoint of the raw amplitudes)
+                    // F2: energy (+ adjoint of the raw amplitudes).  Sub-range
+                    // triples of three distinct full 8-wide sub-ranges come first;
+                    // with the all-distinct occupied representatives (the first
+                    // n_distinct_ijk of the table) they go to the lean kernel k_f2s
+                    // in the mixed modes, every other CTA to k_f2t.
                     F2P<StageT> F;
                     F.d = d;
                     F.ch = ch;
                     F.nsub = 0;
                     int nsb[3];
                     for (int t = 0; t < 3; t++) nsb[t] = (ch.nabc[t] + kSB - 1) / kSB;
+                    F2Sub rest[kMaxSub];
+                    int nrest = 0;
                     for (int sa = 0; sa < nsb[0]; sa++)
                         for (int sb = 0; sb < nsb[1]; sb++) {
                             if (ch.blk[0] == ch.blk[1] && sb > sa) continue;
                             for (int sc = 0; sc < nsb[2]; sc++) {
                                 if (ch.blk[1] == ch.blk[2] && sc > sb) continue;
-                                F2Sub &u = F.sub[F.nsub++];
+                                F2Sub u;
                                 const int si[3] = {sa, sb, sc};
                                 for (int t = 0; t < 3; t++) {
                                     u.st[t] = ch.base[t] + si[t] * kSB;
                                     int len = ch.nabc[t] - si[t] * kSB;
                                     u.len[t] = len < kSB ? len : kSB;
                                 }
+                                const bool simple = mixed && u.len[0] == 8 && u.len[1] == 8 && u.len[2] == 8 &&
+                                                    u.st[0] != u.st[1] && u.st[1] != u.st[2] && u.st[0] != u.st[2];
+                                if (simple) F.sub[F.nsub++] = u;
+                                else rest[nrest++] = u;
                             }
                         }
+                    const int n_simple_sub = F.nsub;
+                    for (int t = 0; t < nrest; t++) F.sub[F.nsub++] = rest[t];
                     F.ijk = ijk;
                     F.mo_e = io.mo_energy; F.t1 = io.t1; F.t2 = io.t2; F.ovov = io.ovov; F.fvo = io.fvo;
                     F.S = S;
@@ -1253,10 +1325,34 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                     F.ybar = io.ybar;
                     F.want_grad = P.want_grad;
                     F.e_part = e_part;
+                    F.n_ijk = P.n_ijk;
                     F.mo_bar = io.mo_energy_bar;
                     F.t1_bar = io.t1_bar; F.fvo_bar = io.fvo_bar; F.ovov_bar = io.ovov_bar; F.t2_bar = io.t2_bar;
-                    TB_KLAUNCH(P_F2, (k_f2t<StageT, kSB><<<dim3(P.n_ijk, F.nsub), F2Smem<kSB>::NT,
-                                                           f2_smem_bytes<StageT, kSB>(), st>>>(F)));
+                    const int nd = mixed ? n_distinct_ijk(d.o) : 0;
+                    auto f2t = [&](int rep0, int nrep, int sub0, int nsub_l) -> int {
+                        if (nrep <= 0 || nsub_l <= 0) return TRIPLES_OK;
+                        F.rep0 = rep0;
+                        F.sub0 = sub0;
+                        F.nsub_l = nsub_l;
+                        TB_KLAUNCH(P_F2, (k_f2t<StageT, kSB><<<(unsigned)(nrep * nsub_l), F2Smem<kSB>::NT,
+                                                               f2_smem_bytes<StageT, kSB>(), st>>>(F)));
+                        return TRIPLES_OK;
+                    };
+                    if (nd > 0 && n_simple_sub > 0) {
+                        F.rep0 = 0;
+                        F.sub0 = 0;
+                        F.nsub_l = n_simple_sub;
+                        F2P<float> Ff;
+                        std::memcpy(&Ff, &F, sizeof(F));   // StageT = float in the mixed modes
+                        const unsigned nb = (unsigned)(nd * n_simple_sub);
+                        if (bf16)
+                            TB_KLAUNCH(P_F2, (k_f2s<2><<<nb, F2sSmem::NT, F2sSmem::BYTES, st>>>(Ff)));
+                        else
+                            TB_KLAUNCH(P_F2, (k_f2s<1><<<nb, F2sSmem::NT, F2sSmem::BYTES, st>>>(Ff)));
+                    }
+                    int frc;
+                    if ((frc = f2t(0, nd, n_simple_sub, F.nsub - n_simple_sub)) != TRIPLES_OK) return frc;
+                    if ((frc = f2t(nd, P.n_ijk - nd, 0, F.nsub)) != TRIPLES_OK) return frc;
                     TB_KLAUNCH(P_F2, k_f2_energy_sum<<<1, 256, 0, st>>>(e_part, P.n_ijk * F.nsub, &ctrl->e_acc));
                 }
                 if (!P.want_grad) continue;
@@ -1285,7 +1381,7 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                     B.wscale = &ctrl->wscale;
                     B.err = &ctrl->err;
                     B.bf16 = bf16 ? 1 : 0;
-                    B.kseg = g_kseg;
+                    B.kseg = P.kseg;
                     auto grid_of = [&]() {
                         B.cum[0] = 0;
                         for (int t = 0; t < ch.nperm; t++)
@@ -1380,16 +1476,6 @@ int run_triples(const Plan &P, cudaStream_t st, const TriplesIO &io) {
     return run_impl<float>(P, st, io);
 }
 
-void set_block_size(int tv) { g_tv_override = tv; }
-void set_chunk_range(int a0, int a1) {
-    g_chunk_a0 = a0 > 0 ? a0 : 0;
-    g_chunk_a1 = a1;
-}
-void set_kseg(int k) {
-    g_kseg = k > 0 ? k : 1;
-    g_kseg_f1 = g_kseg;
-}
-
 void profile_enable(int on) {
     g_prof = on != 0;
     g_prof_recs.clear();
@@ -1425,15 +1511,20 @@ void set_last_cuda_error(int e) { g_last_cuda_error = e; }
 extern "C" {
 
 size_t triples_workspace_size(int precision, int nocc, int nvir, int ovvv_packed, int want_grad) {
+    return triples_workspace_size_ex(precision, nocc, nvir, ovvv_packed, want_grad, nullptr);
+}
+
+size_t triples_workspace_size_ex(int precision, int nocc, int nvir, int ovvv_packed, int want_grad,
+                                 const triples_options *opt) {
     tb::Plan P;
-    if (tb::make_plan(precision, nocc, nvir, ovvv_packed, want_grad, P) != TRIPLES_OK) return 0;
+    if (tb::make_plan(precision, nocc, nvir, ovvv_packed, want_grad, P, 0, opt) != TRIPLES_OK) return 0;
     return P.total;
 }
 
 static int triples_call(void *stream, int precision, int nocc, int nvir, int ovvv_packed, int want_grad,
-                        const tb::TriplesIO &io, size_t workspace_bytes) {
+                        const triples_options *opt, const tb::TriplesIO &io, size_t workspace_bytes) {
     tb::Plan P;
-    int rc = tb::make_plan(precision, nocc, nvir, ovvv_packed, want_grad, P);
+    int rc = tb::make_plan(precision, nocc, nvir, ovvv_packed, want_grad, P, 0, opt);
     if (rc != TRIPLES_OK) return rc;
     if (!io.workspace || workspace_bytes < P.total) return TRIPLES_ERR_WORKSPACE;
     if (!io.mo_energy || !io.t1 || !io.t2 || !io.ovoo || !io.ovov || !io.ovvv || !io.fvo || !io.e_out)
@@ -1451,7 +1542,7 @@ int triples_energy(void *stream, int precision, int nocc, int nvir, int ovvv_pac
     tb::TriplesIO io{};
     io.mo_energy = mo_energy; io.t1 = t1; io.t2 = t2; io.ovoo = ovoo; io.ovov = ovov;
     io.ovvv = ovvv; io.fvo = fvo; io.ybar = 1.0; io.workspace = workspace; io.e_out = e_out;
-    return triples_call(stream, precision, nocc, nvir, ovvv_packed, 0, io, workspace_bytes);
+    return triples_call(stream, precision, nocc, nvir, ovvv_packed, 0, nullptr, io, workspace_bytes);
 }
 
 int triples_energy_vjp(void *stream, int precision, int nocc, int nvir, int ovvv_packed,
@@ -1460,25 +1551,43 @@ int triples_energy_vjp(void *stream, int precision, int nocc, int nvir, int ovvv
                        void *workspace, size_t workspace_bytes, double *e_out, double *mo_energy_bar,
                        double *t1_bar, double *t2_bar, double *ovoo_bar, double *ovov_bar,
                        double *ovvv_bar, double *fvo_bar) {
+    return triples_energy_vjp_ex(stream, precision, nocc, nvir, ovvv_packed, mo_energy, t1, t2, ovoo, ovov,
+                                 ovvv, fvo, ybar, 1, nullptr, workspace, workspace_bytes, e_out, mo_energy_bar,
+                                 t1_bar, t2_bar, ovoo_bar, ovov_bar, ovvv_bar, fvo_bar);
+}
+
+int triples_energy_vjp_ex(void *stream, int precision, int nocc, int nvir, int ovvv_packed,
+                          const double *mo_energy, const double *t1, const double *t2, const double *ovoo,
+                          const double *ovov, const double *ovvv, const double *fvo, double ybar,
+                          int want_grad, const triples_options *opt, void *workspace, size_t workspace_bytes,
+                          double *e_out, double *mo_energy_bar, double *t1_bar, double *t2_bar,
+                          double *ovoo_bar, double *ovov_bar, double *ovvv_bar, double *fvo_bar) {
     tb::TriplesIO io{};
     io.mo_energy = mo_energy; io.t1 = t1; io.t2 = t2; io.ovoo = ovoo; io.ovov = ovov;
-    io.ovvv = ovvv; io.fvo = fvo; io.ybar = ybar; io.workspace = workspace; io.e_out = e_out;
-    io.mo_energy_bar = mo_energy_bar; io.t1_bar = t1_bar; io.t2_bar = t2_bar; io.ovoo_bar = ovoo_bar;
-    io.ovov_bar = ovov_bar; io.ovvv_bar = ovvv_bar; io.fvo_bar = fvo_bar;
-    return triples_call(stream, precision, nocc, nvir, ovvv_packed, 1, io, workspace_bytes);
+    io.ovvv = ovvv; io.fvo = fvo; io.ybar = want_grad ? ybar : 1.0; io.workspace = workspace; io.e_out = e_out;
+    if (want_grad) {
+        io.mo_energy_bar = mo_energy_bar; io.t1_bar = t1_bar; io.t2_bar = t2_bar; io.ovoo_bar = ovoo_bar;
+        io.ovov_bar = ovov_bar; io.ovvv_bar = ovvv_bar; io.fvo_bar = fvo_bar;
+    }
+    return triples_call(stream, precision, nocc, nvir, ovvv_packed, want_grad ? 1 : 0, opt, io, workspace_bytes);
 }
 
 // ---- LNO (projected) energy ----
 size_t triples_lno_workspace_size(int precision, int nocc, int nvir, int ovvv_packed, int want_grad) {
+    return triples_lno_workspace_size_ex(precision, nocc, nvir, ovvv_packed, want_grad, nullptr);
+}
+
+size_t triples_lno_workspace_size_ex(int precision, int nocc, int nvir, int ovvv_packed, int want_grad,
+                                     const triples_options *opt) {
     tb::Plan P;
-    if (tb::make_plan(precision, nocc, nvir, ovvv_packed, want_grad, P, 1) != TRIPLES_OK) return 0;
+    if (tb::make_plan(precision, nocc, nvir, ovvv_packed, want_grad, P, 1, opt) != TRIPLES_OK) return 0;
     return P.total;
 }
 
 static int triples_lno_call(void *stream, int precision, int nocc, int nvir, int ovvv_packed, int want_grad,
-                            const tb::TriplesIO &io, size_t workspace_bytes) {
+                            const triples_options *opt, const tb::TriplesIO &io, size_t workspace_bytes) {
     tb::Plan P;
-    int rc = tb::make_plan(precision, nocc, nvir, ovvv_packed, want_grad, P, 1);
+    int rc = tb::make_plan(precision, nocc, nvir, ovvv_packed, want_grad, P, 1, opt);
     if (rc != TRIPLES_OK) return rc;
     if (!io.workspace || workspace_bytes < P.total) return TRIPLES_ERR_WORKSPACE;
     if (!io.mat || !io.mo_energy || !io.t1 || !io.t2 || !io.ovoo || !io.ovov || !io.ovvv || !io.fvo || !io.e_out)
@@ -1493,11 +1602,9 @@ int triples_lno_energy(void *stream, int precision, int nocc, int nvir, int ovvv
                        const double *mo_energy, const double *t1, const double *t2, const double *ovoo,
                        const double *ovov, const double *ovvv, const double *fvo, void *workspace,
                        size_t workspace_bytes, double *e_out) {
-    tb::TriplesIO io{};
-    io.mat = mat;
-    io.mo_energy = mo_energy; io.t1 = t1; io.t2 = t2; io.ovoo = ovoo; io.ovov = ovov;
-    io.ovvv = ovvv; io.fvo = fvo; io.ybar = 1.0; io.workspace = workspace; io.e_out = e_out;
-    return triples_lno_call(stream, precision, nocc, nvir, ovvv_packed, 0, io, workspace_bytes);
+    return triples_lno_energy_vjp_ex(stream, precision, nocc, nvir, ovvv_packed, mat, mo_energy, t1, t2, ovoo, ovov,
+                                     ovvv, fvo, 1.0, 0, nullptr, workspace, workspace_bytes, e_out, nullptr,
+                                     nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
 }
 
 int triples_lno_energy_vjp(void *stream, int precision, int nocc, int nvir, int ovvv_packed, const double *mat,
@@ -1506,14 +1613,29 @@ int triples_lno_energy_vjp(void *stream, int precision, int nocc, int nvir, int 
                            void *workspace, size_t workspace_bytes, double *e_out, double *mat_bar,
                            double *mo_energy_bar, double *t1_bar, double *t2_bar, double *ovoo_bar,
                            double *ovov_bar, double *ovvv_bar, double *fvo_bar) {
+    return triples_lno_energy_vjp_ex(stream, precision, nocc, nvir, ovvv_packed, mat, mo_energy, t1, t2, ovoo, ovov,
+                                     ovvv, fvo, ybar, 1, nullptr, workspace, workspace_bytes, e_out, mat_bar,
+                                     mo_energy_bar, t1_bar, t2_bar, ovoo_bar, ovov_bar, ovvv_bar, fvo_bar);
+}
+
+int triples_lno_energy_vjp_ex(void *stream, int precision, int nocc, int nvir, int ovvv_packed, const double *mat,
+                              const double *mo_energy, const double *t1, const double *t2, const double *ovoo,
+                              const double *ovov, const double *ovvv, const double *fvo, double ybar,
+                              int want_grad, const triples_options *opt, void *workspace, size_t workspace_bytes,
+                              double *e_out, double *mat_bar, double *mo_energy_bar, double *t1_bar,
+                              double *t2_bar, double *ovoo_bar, double *ovov_bar, double *ovvv_bar,
+                              double *fvo_bar) {
     tb::TriplesIO io{};
     io.mat = mat;
     io.mo_energy = mo_energy; io.t1 = t1; io.t2 = t2; io.ovoo = ovoo; io.ovov = ovov;
-    io.ovvv = ovvv; io.fvo = fvo; io.ybar = ybar; io.workspace = workspace; io.e_out = e_out;
-    io.mat_bar = mat_bar;
-    io.mo_energy_bar = mo_energy_bar; io.t1_bar = t1_bar; io.t2_bar = t2_bar; io.ovoo_bar = ovoo_bar;
-    io.ovov_bar = ovov_bar; io.ovvv_bar = ovvv_bar; io.fvo_bar = fvo_bar;
-    return triples_lno_call(stream, precision, nocc, nvir, ovvv_packed, 1, io, workspace_bytes);
+    io.ovvv = ovvv; io.fvo = fvo; io.ybar = want_grad ? ybar : 1.0; io.workspace = workspace; io.e_out = e_out;
+    if (want_grad) {
+        io.mat_bar = mat_bar;
+        io.mo_energy_bar = mo_energy_bar; io.t1_bar = t1_bar; io.t2_bar = t2_bar; io.ovoo_bar = ovoo_bar;
+        io.ovov_bar = ovov_bar; io.ovvv_bar = ovvv_bar; io.fvo_bar = fvo_bar;
+    }
+    return triples_lno_call(stream, precision, nocc, nvir, ovvv_packed, want_grad ? 1 : 0, opt, io,
+                            workspace_bytes);
 }
 
 // ---- LNO host tables (introspection) ----
@@ -1629,7 +1751,33 @@ int triples_energy_vjp_df(void *stream, int precision, int nocc, int nvir, int n
 static constexpr size_t kStaticScratchBytes = TRIPLES_STATIC_SCRATCH_BYTES;
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
 static constexpr int kStaticMaxDevices = 64;
-static void *g_static_scratch_addr[kStaticMaxDevices] = {};
+// Device address of the array per device, looked up once with that device
+// current.  Host threads making their first call on a device at the same
+// time both store the same address; the cache assumes the device's primary
+// context lives as long as the process.
+static std::atomic<void *> g_static_scratch_addr[kStaticMaxDevices];
+
+static int static_scratch_address(void **addr_out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        tb::set_last_cuda_error((int)e);
+        return TRIPLES_ERR_CUDA;
+    }
+    if (dev < 0 || dev >= kStaticMaxDevices) return TRIPLES_ERR_UNSUPPORTED;
+    void *addr = g_static_scratch_addr[dev].load(std::memory_order_acquire);
+    if (addr == nullptr) {
+        // the array's host-side name is only a stand-in for the symbol
+        e = cudaGetSymbolAddress(&addr, g_static_scratch);
+        if (e != cudaSuccess || addr == nullptr) {
+            tb::set_last_cuda_error((int)e);
+            return TRIPLES_ERR_CUDA;
+        }
+        g_static_scratch_addr[dev].store(addr, std::memory_order_release);
+    }
+    *addr_out = addr;
+    return TRIPLES_OK;
+}
 
 int triples_energy_vjp_static(void *stream, int precision, int nocc, int nvir, int ovvv_packed,
                               const double *mo_energy, const double *t1, const double *t2,
@@ -1640,27 +1788,26 @@ int triples_energy_vjp_static(void *stream, int precision, int nocc, int nvir, i
     const size_t need = triples_workspace_size(precision, nocc, nvir, ovvv_packed, 1);
     if (need == 0) return TRIPLES_ERR_INVALID_ARGUMENT;
     if (need > kStaticScratchBytes) return TRIPLES_ERR_WORKSPACE;   // problem too large for the fixed scratch
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) {
-        tb::set_last_cuda_error((int)e);
-        return TRIPLES_ERR_CUDA;
-    }
-    if (dev < 0 || dev >= kStaticMaxDevices) return TRIPLES_ERR_UNSUPPORTED;
-    if (g_static_scratch_addr[dev] == nullptr) {
-        // once per device, with that device current: the device address of the
-        // array (its host-side name is only a stand-in for the symbol)
-        void *addr = nullptr;
-        e = cudaGetSymbolAddress(&addr, g_static_scratch);
-        if (e != cudaSuccess || addr == nullptr) {
-            tb::set_last_cuda_error((int)e);
-            return TRIPLES_ERR_CUDA;
-        }
-        g_static_scratch_addr[dev] = addr;
-    }
+    void *scratch = nullptr;
+    const int rc = static_scratch_address(&scratch);
+    if (rc != TRIPLES_OK) return rc;
     return triples_energy_vjp(stream, precision, nocc, nvir, ovvv_packed, mo_energy, t1, t2, ovoo, ovov, ovvv,
-                              fvo, ybar, g_static_scratch_addr[dev], kStaticScratchBytes, e_out, mo_energy_bar,
-                              t1_bar, t2_bar, ovoo_bar, ovov_bar, ovvv_bar, fvo_bar);
+                              fvo, ybar, scratch, kStaticScratchBytes, e_out, mo_energy_bar, t1_bar, t2_bar,
+                              ovoo_bar, ovov_bar, ovvv_bar, fvo_bar);
+}
+
+int triples_static_scratch(void **ptr, size_t *bytes) {
+    if (!ptr) return TRIPLES_ERR_INVALID_ARGUMENT;
+    const int rc = static_scratch_address(ptr);
+    if (rc == TRIPLES_OK && bytes) *bytes = kStaticScratchBytes;
+    return rc;
+}
+
+int triples_static_check_device_status(void *stream) {
+    void *scratch = nullptr;
+    const int rc = static_scratch_address(&scratch);
+    if (rc != TRIPLES_OK) return rc;
+    return triples_check_device_status(stream, scratch);
 }
 
 int triples_check_device_status(void *stream, const void *workspace) {
@@ -1690,12 +1837,6 @@ const char *triples_status_string(int status) {
 int triples_last_cuda_error(void) { return tb::last_cuda_error(); }
 
 const char *triples_version(void) { return "0.1.0"; }
-
-void triples_set_block_size(int tv) { tb::set_block_size(tv); }
-
-void triples_set_chunk_range(int a0, int a1) { tb::set_chunk_range(a0, a1); }
-
-void triples_set_accumulation_segment(int kblocks) { tb::set_kseg(kblocks); }
 
 void triples_profile_enable(int on) { tb::profile_enable(on); }
 

@@ -4,6 +4,7 @@
 
 #include "common.cuh"
 #include "f2.cuh"
+#include "pyscfad_b200.h"
 
 namespace tb {
 
@@ -32,6 +33,8 @@ static_assert(sizeof(Ctrl) <= kCtrlBytes, "control block too large");
 
 struct Plan {
     Dims d;
+    int a0, a1;      // chunk slice by largest virtual block (a1 <= 0: no upper bound)
+    int kseg;        // 64-wide K blocks per FP32 accumulation segment (mixed precision)
     int prec, want_grad, packed;
     int lno;         // projected (LNO) energy: whole-chunk work arrays off_L
     int nb;          // number of virtual blocks
@@ -59,7 +62,8 @@ struct TriplesIO {
     double *mat_bar;
 };
 
-int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan &P, int lno = 0);
+int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan &P, int lno = 0,
+              const triples_options *opt = nullptr);
 int run_triples(const Plan &P, cudaStream_t st, const TriplesIO &io);
 int gemm_plain(cudaStream_t st, int M, int N, int K, const double *A, long long ams, long long aks,
                const double *B, long long bms, long long bks, double *C, long long cms, long long cns);

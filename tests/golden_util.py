@@ -10,6 +10,7 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 KEYS = ("mo_energy", "t1", "t2", "ovoo", "ovov", "ovvv", "fvo")
 LNO_PREFIX = "lno_"
 DF_PREFIX = "df_"
+SLICE_PREFIX = "slice_"   # one virtual slice of a benchmark-size problem (tests/golden/make_slices.py)
 
 
 def _all():
@@ -18,7 +19,7 @@ def _all():
 
 def names():
     """Canonical (T) fixtures."""
-    return [n for n in _all() if not n.startswith((LNO_PREFIX, DF_PREFIX))]
+    return [n for n in _all() if not n.startswith((LNO_PREFIX, DF_PREFIX, SLICE_PREFIX))]
 
 
 def df_names():

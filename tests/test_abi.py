@@ -107,3 +107,28 @@ def test_lno_workspace_fits_one_b200_at_the_largest_fragments():
             grad = lib.triples_lno_workspace_size(prec, o, v, 1, 1)
             energy = lib.triples_lno_workspace_size(prec, o, v, 1, 0)
             assert 0 < energy < grad < 150e9, (prec, o, v, grad)
+
+
+def test_options_are_per_call_and_validated():
+    """Block size, chunk slice and accumulation segment travel with the call
+    (triples_options): no process-wide setter exists, a NULL options pointer
+    means the defaults, and negative settings are refused."""
+    lib = _lib.load()
+    for gone in ("triples_set_block_size", "triples_set_chunk_range", "triples_set_accumulation_segment"):
+        assert not hasattr(lib, gone), gone
+    base = lib.triples_workspace_size(1, 20, 180, 1, 1)
+    assert lib.triples_workspace_size_ex(1, 20, 180, 1, 1, None) == base
+    assert lib.triples_workspace_size_ex(1, 20, 180, 1, 1, ctypes.byref(_lib.options())) == base
+    small = lib.triples_workspace_size_ex(1, 20, 180, 1, 1, ctypes.byref(_lib.options(block_size=4)))
+    assert 0 < small < base
+    # the default plan is not changed by an earlier call with other options
+    assert lib.triples_workspace_size(1, 20, 180, 1, 1) == base
+    assert lib.triples_workspace_size_ex(1, 20, 180, 1, 1, ctypes.byref(_lib.options(block_size=-1))) == 0
+    assert lib.triples_workspace_size_ex(1, 20, 180, 1, 1, ctypes.byref(_lib.options(chunk_range=(-1, 0)))) == 0
+    assert lib.triples_lno_workspace_size_ex(1, 20, 180, 1, 1, ctypes.byref(_lib.options(block_size=4))) < \
+        lib.triples_lno_workspace_size(1, 20, 180, 1, 1)
+    # energy-only calls may pass NULL gradient pointers; missing inputs are still refused
+    null = None
+    rc = lib.triples_energy_vjp_ex(null, 0, 5, 19, 1, *([null] * 7), 1.0, 0, None, ctypes.c_void_p(256),
+                                   1 << 30, ctypes.c_void_p(256), *([null] * 7))
+    assert rc == 1

@@ -29,11 +29,7 @@ def _relerr(a, b):
 
 
 def _single(p, precision, tv):
-    triples.set_block_size(tv)
-    try:
-        e, g = triples.energy_vjp(*(p[k] for k in triples.KEYS), precision=precision, device="cuda")
-    finally:
-        triples.set_block_size(0)
+    e, g = triples.energy_vjp(*(p[k] for k in triples.KEYS), precision=precision, device="cuda", block_size=tv)
     return float(e), g
 
 

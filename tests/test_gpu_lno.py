@@ -24,18 +24,12 @@ def _relerr(a, b):
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-7))
 
 
-def _run(inp, mat, packed=True, ybar=1.0, precision="fp64"):
+def _run(inp, mat, packed=True, ybar=1.0, precision="fp64", block_size=0):
     ovvv = inp.ovvv_tril() if packed else inp.ovvv
     e, g = triples.lno_energy_vjp(mat, inp.mo_energy, inp.t1, inp.t2, inp.ovoo, inp.ovov, ovvv, inp.fvo,
-                                  ybar=ybar, precision=precision, device="cuda")
+                                  ybar=ybar, precision=precision, device="cuda", block_size=block_size)
     torch.cuda.synchronize()
     return float(e), {k: v.cpu().numpy() for k, v in g.items()}
-
-
-@pytest.fixture(autouse=True)
-def _reset_block_size():
-    yield
-    triples.set_block_size(0)
 
 
 @pytest.mark.parametrize("name", G.lno_names())
@@ -90,9 +84,8 @@ def test_lno_energy_only_matches_vjp_energy():
 @pytest.mark.parametrize("tv", [1, 2, 4, 8])
 def test_lno_block_sizes(tv):
     """Many chunks, degenerate (A == B, B == C) and ragged blocks."""
-    triples.set_block_size(tv)
     inp, e_ref, g_ref, z = G.load("lno_o4v9")
-    e, g = _run(inp, z["in_mat"], packed=False)
+    e, g = _run(inp, z["in_mat"], packed=False, block_size=tv)
     assert abs(e - e_ref) <= E_RTOL * abs(e_ref)
     for k in KEYS:
         assert _relerr(g[k], g_ref[k]) < G_RTOL, k

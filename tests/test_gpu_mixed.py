@@ -23,17 +23,11 @@ def _relerr(a, b):
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-7))
 
 
-def _run(inp, packed, precision):
+def _run(inp, packed, precision, **opt):
     ovvv = inp.ovvv_tril() if packed else inp.ovvv
     e, g = triples.energy_vjp(inp.mo_energy, inp.t1, inp.t2, inp.ovoo, inp.ovov, ovvv, inp.fvo,
-                              precision=precision, device="cuda")
+                              precision=precision, device="cuda", **opt)
     return float(e), {k: v.cpu().numpy() for k, v in g.items()}
-
-
-@pytest.fixture(autouse=True)
-def _reset_block_size():
-    yield
-    triples.set_block_size(0)
 
 
 @pytest.mark.parametrize("precision", ["mixed", "mixed_bf16"])
@@ -50,9 +44,8 @@ def test_mixed_vs_reference_golden(name, precision):
 
 @pytest.mark.parametrize("tv", [2, 4])
 def test_mixed_block_sizes(tv):
-    triples.set_block_size(tv)
     inp, e_ref, g_ref, _ = G.load("o4v9_fvo")
-    e, g = _run(inp, False, "mixed")
+    e, g = _run(inp, False, "mixed", block_size=tv)
     assert abs(e - e_ref) <= 1e-6 * abs(e_ref)
     for k in G.KEYS:
         assert _relerr(g[k], g_ref[k]) < 1e-5, k
@@ -102,3 +95,25 @@ def test_mixed_odd_shapes_vs_oracle(o, v):
     assert abs(e - e_ref) <= 1e-6 * max(abs(e_ref), 1e-12)
     for k in G.KEYS:
         assert _relerr(g[k], g_ref[k]) < 1e-5, k
+
+
+@pytest.mark.parametrize("precision", ["mixed", "mixed_bf16"])
+@pytest.mark.parametrize("o,v,seed", [(10, 48, 51), (6, 64, 52)])
+def test_lean_epilogue_shapes_vs_fp64(precision, o, v, seed):
+    """Shapes where most epilogue blocks take the lean all-distinct kernel
+    (i > j > k, three distinct full 8-wide sub-ranges) and the rest the
+    generic one: the mixed result against the FP64 path on the same inputs,
+    with its oracle check at the smaller shape."""
+    inp = make_inputs(o, v, 3 * (o + v), seed=seed, fvo_sigma=1e-3)
+    e64, g64 = _run(inp, True, "fp64")
+    e, g = _run(inp, True, precision)
+    te, tg = TOL[precision]
+    assert abs(e - e64) <= te * abs(e64), (e, e64)
+    for k in G.KEYS:
+        assert _relerr(g[k], g64[k]) < tg, (k, _relerr(g[k], g64[k]))
+    if o * v <= 400:
+        e_ref, g_ref = O.oracle_energy_vjp(inp)
+        assert abs(e64 - e_ref) <= 1e-12 * abs(e_ref)
+        g_ref = dict(g_ref, ovvv=O.fold_ovvv_tril(g_ref["ovvv"]))
+        for k in G.KEYS:
+            assert _relerr(g64[k], g_ref[k]) < 1e-10, k

@@ -22,18 +22,12 @@ def _relerr(a, b):
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-7))
 
 
-def _run(inp, packed, precision="fp64", ybar=1.0):
+def _run(inp, packed, precision="fp64", ybar=1.0, **opt):
     ovvv = inp.ovvv_tril() if packed else inp.ovvv
     e, g = triples.energy_vjp(inp.mo_energy, inp.t1, inp.t2, inp.ovoo, inp.ovov, ovvv, inp.fvo,
-                              ybar=ybar, precision=precision, device="cuda")
+                              ybar=ybar, precision=precision, device="cuda", **opt)
     torch.cuda.synchronize()
     return float(e), {k: v.cpu().numpy() for k, v in g.items()}
-
-
-@pytest.fixture(autouse=True)
-def _reset_block_size():
-    yield
-    triples.set_block_size(0)
 
 
 @pytest.mark.parametrize("name", G.names())
@@ -50,9 +44,8 @@ def test_fp64_matches_reference_golden(name, packed):
 @pytest.mark.parametrize("tv", [1, 2, 4, 8, 16])
 def test_fp64_block_sizes(tv):
     """Chunk decomposition with degenerate (A==B, B==C) and ragged blocks."""
-    triples.set_block_size(tv)
     inp, e_ref, g_ref, _ = G.load("o4v9_fvo")
-    e, g = _run(inp, packed=False)
+    e, g = _run(inp, packed=False, block_size=tv)
     assert abs(e - e_ref) <= FP64_E_RTOL * abs(e_ref)
     for k in G.KEYS:
         assert _relerr(g[k], g_ref[k]) < FP64_G_RTOL, k
@@ -93,17 +86,10 @@ def test_repeated_calls_are_stable():
 def test_fp64_chunk_slices_partition_the_problem(tv):
     """Energies and gradients of chunk slices that partition the virtual
     blocks add up to the full result (the basis of slice timing)."""
-    triples.set_block_size(tv)
     inp, e_ref, g_ref, _ = G.load("o5v19_fvo")
     nb = len(triples.block_sizes(inp.t1.shape[1], tv))
     cut = nb // 2
-    try:
-        parts = []
-        for a0, a1 in ((0, cut), (cut, nb)):
-            triples.set_chunk_range(a0, a1)
-            parts.append(_run(inp, packed=True))
-    finally:
-        triples.set_chunk_range(0, 0)
+    parts = [_run(inp, packed=True, block_size=tv, chunk_range=(a0, a1)) for a0, a1 in ((0, cut), (cut, nb))]
     e = parts[0][0] + parts[1][0]
     assert abs(e - e_ref) <= FP64_E_RTOL * abs(e_ref)
     for k in G.KEYS:

@@ -4,12 +4,16 @@ Golden fixtures come from the reference library compiled unchanged from
 pyscfadlib/pyscfadlib/vjp/cc/*.c (tests/golden/make_golden.py).  Tolerances
 are FP64 summation-order level.
 """
+import os
+
 import numpy as np
 import pytest
 
 from oracle import oracle as O
 from pyscfad_b200.synthetic import make_inputs
 from tests import golden_util as G
+
+HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 def _relerr(a, b):
@@ -172,3 +176,35 @@ def test_df_fixture_is_the_factor_chain_of_the_packed_cotangent(name):
     assert np.allclose(vb, z["grad_Lvv"], rtol=0, atol=1e-14 * np.abs(vb).max())
     o, v = int(z["nocc"]), int(z["nvir"])
     assert np.allclose((z["in_Lov"].T @ z["in_Lvv"]).reshape(o, v, -1), z["in_ovvv_tril"], rtol=0, atol=1e-14)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built here")
+@pytest.mark.parametrize("A", [0, 1, 2])
+def test_reference_aslice_blocking_matches_oracle_slice(A):
+    """tests/golden/make_slices.py drives the reference's ccsd_t_energy_vjp
+    the way pyscfad/cc/ccsd_t.py:145-175 blocks it for one a-range; that slice
+    equals our C restatement's slice a in [16A, 16A+16), and its energy follows
+    from the gradients by Euler's theorem."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("make_slices", os.path.join(HERE, "golden", "make_slices.py"))
+    M = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(M)
+    inp = make_inputs(5, 40, 60, seed=3, fvo_sigma=1e-3)
+    a0, a1 = 16 * A, min(40, 16 * A + 16)
+    g = M.ref_vjp_aslice(inp, a0, a1)
+    e_or, g_or = O.oracle_energy_vjp(inp, a0=a0, a1=a1)
+    g_or = dict(g_or, ovvv=O.fold_ovvv_tril(g_or["ovvv"]))
+    assert abs(M.euler_energy(inp, g) - e_or) <= 1e-13 * abs(e_or)
+    for k in g:
+        assert np.abs(g[k] - g_or[k]).max() <= 1e-13 * np.abs(g_or[k]).max(), k
+
+
+def test_slice_fixture_is_consistent():
+    z = np.load(os.path.join(HERE, "golden", "slice_o20v180_a3.npz"))
+    assert int(z["a0"]) == 16 * int(z["block"]) and int(z["a1"]) == int(z["a0"]) + 16
+    assert abs(float(z["e"]) - float(z["e_oracle"])) <= 1e-11 * abs(float(z["e"]))
+    for k in ("t2", "ovoo", "ovov", "ovvv"):
+        assert z["idx_" + k].size == z["val_" + k].size > 1000
+        assert np.all(np.diff(z["idx_" + k]) > 0)
+        assert np.abs(z["val_" + k]).max() <= float(z["norm_" + k])

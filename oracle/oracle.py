@@ -37,10 +37,38 @@ def _ptr(a: np.ndarray):
     return a.ctypes.data_as(ctypes.c_void_p)
 
 
+# where the reference checkout and the BLAS the reference library links live
+# on the machine that builds the checker (override with REF / OPENBLAS_DIR)
+_REF_DEFAULT = "/root/reference/pyscfadlib/pyscfadlib"
+
+
+def _openblas_dir():
+    """The folder of the OpenBLAS bundled with the opencv wheel of this image
+    (it exports dgemm_/dgemv_), found through the installed package."""
+    import importlib.util
+    spec = importlib.util.find_spec("cv2")
+    if spec is None or not spec.origin:
+        return ""
+    site = os.path.dirname(os.path.dirname(spec.origin))
+    for name in sorted(os.listdir(site)):
+        if name.startswith("opencv_python") and name.endswith(".libs"):
+            return os.path.join(site, name)
+    return ""
+
+
 def build():
     """Compile the oracle (and the reference library when its sources exist)."""
     import subprocess
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    env = dict(os.environ)
+    if not env.get("REF") and os.path.isdir(_REF_DEFAULT):
+        env["REF"] = _REF_DEFAULT
+    if not env.get("OPENBLAS_DIR"):
+        env["OPENBLAS_DIR"] = _openblas_dir()
+    args = ["make", "-s", "-C", HERE]
+    for k in ("REF", "OPENBLAS_DIR"):
+        if env.get(k):
+            args.append(f"{k}={env[k]}")
+    subprocess.run(args, check=True, env=env)
 
 
 def _lib(name):

@@ -78,6 +78,10 @@ typedef struct triples_options {
     /* mixed precision: 64-wide K blocks the tensor cores accumulate in FP32
      * before the partial result is added in higher precision; 0 = default (1). */
     int accumulation_segment;
+    /* mixed precision: N tile of the W contraction, 128 or 256 columns
+     * (8 or 16 occupied indices x 16 virtuals); 0 = the one that pads nocc
+     * least.  Performance only. */
+    int tile_n;
 } triples_options;
 
 /* Bytes of device workspace the calls below need for this problem.

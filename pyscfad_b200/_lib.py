@@ -22,14 +22,14 @@ _c_int, _c_size, _c_double, _vp = ctypes.c_int, ctypes.c_size_t, ctypes.c_double
 class Options(ctypes.Structure):
     """triples_options (include/pyscfad_b200.h): per-call settings."""
     _fields_ = [("block_size", _c_int), ("chunk_a0", _c_int), ("chunk_a1", _c_int),
-                ("accumulation_segment", _c_int)]
+                ("accumulation_segment", _c_int), ("tile_n", _c_int)]
 
 
-def options(block_size=0, chunk_range=None, accumulation_segment=0):
+def options(block_size=0, chunk_range=None, accumulation_segment=0, tile_n=0):
     """An Options value; chunk_range = (a0, a1) restricts the call to the chunks
     whose largest virtual block index lies in [a0, a1)."""
     a0, a1 = chunk_range if chunk_range is not None else (0, 0)
-    return Options(int(block_size), int(a0), int(a1), int(accumulation_segment))
+    return Options(int(block_size), int(a0), int(a1), int(accumulation_segment), int(tile_n))
 
 
 class TriplesError(RuntimeError):

@@ -162,9 +162,12 @@ int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan
         P.a0 = opt->chunk_a0;
         P.a1 = opt->chunk_a1;
         P.kseg = opt->accumulation_segment > 0 ? opt->accumulation_segment : 1;
+        if (opt->tile_n != 0 && opt->tile_n != 128 && opt->tile_n != 256) return TRIPLES_ERR_INVALID_ARGUMENT;
+        P.f1_bn = opt->tile_n;
     } else {
         P.kseg = 1;
     }
+    if (P.f1_bn == 0) P.f1_bn = ((nocc + 7) / 8) * 8 < ((nocc + 15) / 16) * 16 ? 128 : 256;
     P.lno = lno ? 1 : 0;
     P.prec = precision;
     P.want_grad = want_grad ? 1 : 0;
@@ -1139,8 +1142,11 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
         TB_KLAUNCH(P_PREP, k_prep_B2<<<grid1d((long long)v * o * v * o, 256), 256, 0, st>>>(io.t2, d, B2));
     }
 
-    // 16-bit split operands and tensor maps (tensor-core path)
-    constexpr int BN = 256;
+    // 16-bit split operands and tensor maps (tensor-core path).  The W
+    // contraction's N tile is BN = 16 * RT columns (RT occupied r values x 16 z):
+    // 256 unless 128 covers nocc with fewer padded r values (nocc % 16 in
+    // 1..8, e.g. nocc = 40: three 16-r tiles hold 48 r, five 8-r tiles 40).
+    const int f1_bn = P.f1_bn;
     CUtensorMap tmA1, tmB1, tmA2, tmB2, tmA1m, tmA2m, tmB1z[5], tmB2z[5];
     const uint64_t dA1mn[5] = {(uint64_t)P.Kp8, v, o, v, 2};
     const uint64_t dA2mn[5] = {(uint64_t)P.Op8, v, o, o, 2};
@@ -1182,7 +1188,7 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
             const uint64_t dA1[5] = {(uint64_t)P.Kp8, v, o, v, 2};
             const uint32_t bA[5] = {64, 16, 8, 1, 1};
             const uint64_t dB1[5] = {(uint64_t)P.Kp8, v, o, o, 2};
-            const uint32_t bB[5] = {64, 16, (uint32_t)TcCfg<BN>::RT, 1, 1};
+            const uint32_t bB[5] = {64, 16, (uint32_t)(f1_bn / 16), 1, 1};
             const uint64_t dA2[5] = {(uint64_t)P.Op8, v, o, o, 2};
             const uint64_t dB2[5] = {(uint64_t)P.Op8, v, o, v, 2};
             int rc;
@@ -1206,7 +1212,8 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
             TB_CUDA(cudaMemsetAsync(SW, 0, P.wbar_elems * 4, st));
         }
         const int arc = once_per_device(INIT_TC, [&]() -> int {
-            TB_CUDA(cudaFuncSetAttribute(k_f1_tc<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcCfg<BN>::SMEM));
+            TB_CUDA(cudaFuncSetAttribute(k_f1_tc<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcCfg<256>::SMEM));
+            TB_CUDA(cudaFuncSetAttribute(k_f1_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcCfg<128>::SMEM));
             TB_CUDA(cudaFuncSetAttribute(k_b1_tc<false, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          TcB1Cfg<false, 128>::SMEM));
             TB_CUDA(cudaFuncSetAttribute(k_b1_tc<true, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1237,7 +1244,8 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                     T.d = d;
                     T.ch = ch;
                     T.mt_count = (d.o + 7) / 8;
-                    T.nt_count = (d.o + TcCfg<BN>::RT - 1) / TcCfg<BN>::RT;
+                    const int rt = f1_bn / 16;
+                    T.nt_count = (d.o + rt - 1) / rt;
                     T.cum[0] = 0;
                     for (int t = 0; t < ch.nperm; t++)
                         T.cum[t + 1] = T.cum[t] + ch.pb[t].Ty * d.o * T.mt_count * T.nt_count;
@@ -1260,7 +1268,10 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                     }
                     const int tiles = T.cum[ch.nperm];
                     const int grid = tiles < num_sms() ? tiles : num_sms();
-                    TB_KLAUNCH(P_F1, k_f1_tc<BN><<<grid, kF1Threads, TcCfg<BN>::SMEM, st>>>(tmA1, tmB1, tmA2, tmB2, T));
+                    if (f1_bn == 128)
+                        TB_KLAUNCH(P_F1, k_f1_tc<128><<<grid, kF1Threads, TcCfg<128>::SMEM, st>>>(tmA1, tmB1, tmA2, tmB2, T));
+                    else
+                        TB_KLAUNCH(P_F1, k_f1_tc<256><<<grid, kF1Threads, TcCfg<256>::SMEM, st>>>(tmA1, tmB1, tmA2, tmB2, T));
                 } else {
                     GemmLaunch<double> L;
                     L.d = d;

@@ -35,6 +35,7 @@ struct Plan {
     Dims d;
     int a0, a1;      // chunk slice by largest virtual block (a1 <= 0: no upper bound)
     int kseg;        // 64-wide K blocks per FP32 accumulation segment (mixed precision)
+    int f1_bn;       // N tile of the tensor-core W contraction (128 or 256)
     int prec, want_grad, packed;
     int lno;         // projected (LNO) energy: whole-chunk work arrays off_L
     int nb;          // number of virtual blocks

@@ -94,13 +94,13 @@ def _device_of(device, t1):
 
 
 def _run(mo_energy, t1, t2, ovoo, ovov, ovvv, fvo, ybar, want_grad, precision, device, stream, check,
-         block_size, chunk_range, accumulation_segment):
+         block_size, chunk_range, accumulation_segment, tile_n=0):
     lib = _lib.load()
     device = _device_of(device, t1)
     args = [_as_dev(a, device) for a in (mo_energy, t1, t2, ovoo, ovov, ovvv, fvo)]
     o, v, packed = _shapes(*args[1:], args[0])
     prec = _lib.PRECISION[precision]
-    opt = _lib.options(block_size, chunk_range, accumulation_segment)
+    opt = _lib.options(block_size, chunk_range, accumulation_segment, tile_n)
     nbytes = lib.triples_workspace_size_ex(prec, o, v, int(packed), int(want_grad), ctypes.byref(opt))
     if nbytes == 0:
         raise _lib.TriplesError(1, "triples_workspace_size_ex")
@@ -130,12 +130,13 @@ def energy(mo_energy, t1, t2, ovoo, ovov, ovvv, fvo, precision="fp64", device=No
 
 
 def energy_vjp(mo_energy, t1, t2, ovoo, ovov, ovvv, fvo, ybar=1.0, precision="fp64",
-               device=None, stream=None, check=True, block_size=0, chunk_range=None, accumulation_segment=0):
+               device=None, stream=None, check=True, block_size=0, chunk_range=None, accumulation_segment=0,
+               tile_n=0):
     """E(T) and dE/d(inputs) * ybar.  Gradients have the input layouts; for a
     packed ovvv the gradient is the reference's packed-tril fold
     (pyscfad/cc/ccsd_t.py:184-191).  Returns (e, dict)."""
     return _run(mo_energy, t1, t2, ovoo, ovov, ovvv, fvo, ybar, True, precision, device, stream, check,
-                block_size, chunk_range, accumulation_segment)
+                block_size, chunk_range, accumulation_segment, tile_n)
 
 
 def _check_mat(mat, o):

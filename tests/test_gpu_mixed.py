@@ -117,3 +117,16 @@ def test_lean_epilogue_shapes_vs_fp64(precision, o, v, seed):
         g_ref = dict(g_ref, ovvv=O.fold_ovvv_tril(g_ref["ovvv"]))
         for k in G.KEYS:
             assert _relerr(g64[k], g_ref[k]) < 1e-10, k
+
+
+@pytest.mark.parametrize("o,v", [(12, 40), (20, 33)])
+def test_w_contraction_n_tiles_agree(o, v):
+    """The 128- and 256-column N tiles of the tensor-core W contraction give the
+    same result (same K order per element): any nocc pads differently."""
+    inp = make_inputs(o, v, 3 * (o + v), seed=60 + o, fvo_sigma=1e-3)
+    args = (inp.mo_energy, inp.t1, inp.t2, inp.ovoo, inp.ovov, inp.ovvv_tril(), inp.fvo)
+    e1, g1 = triples.energy_vjp(*args, precision="mixed", device="cuda", tile_n=128)
+    e2, g2 = triples.energy_vjp(*args, precision="mixed", device="cuda", tile_n=256)
+    assert abs(float(e1) - float(e2)) <= 1e-12 * abs(float(e2))
+    for k in G.KEYS:
+        assert _relerr(g1[k].cpu().numpy(), g2[k].cpu().numpy()) < 1e-12, k

@@ -290,6 +290,8 @@ def run_batched(args):
             "autotune_s": t_tune, "capture_s": t_cap,
             "tuned_block_sizes": {str(k): v for k, v in sorted(
                 {tv: sum(1 for p in bt.problems if p.tv == tv) for tv in (4, 8, 16)}.items())},
+            "tuned_w_tiles": {str(k): v for k, v in sorted(
+                {tn: sum(1 for p in bt.problems if p.tile_n == tn) for tn in (0, 128, 256)}.items())},
             "e_sum": float(e_graph.sum())}
     print(json.dumps(line))
 

@@ -5,9 +5,11 @@ a screening or training workload has hundreds of small, differently sized
 problems, each far too small to fill a B200.  ``BatchedTriples``:
 
 * tunes, per problem shape (nocc, nvir, precision), the chunk block size Tv
-  (which sets the GEMM tile population and the epilogue schedule) by timing
-  each candidate once and keeping the fastest (``Autotuner``; results are
-  cached per process and can be saved to / loaded from a JSON file);
+  (which sets the GEMM tile population and the epilogue schedule) and, in
+  the mixed modes, the N tile of the tensor-core W contraction (128 or 256
+  columns) by timing each candidate once and keeping the fastest
+  (``Autotuner``; results are cached per process and can be saved to /
+  loaded from a JSON file);
 * assigns the problems to ``lanes`` CUDA streams (largest first, each to the
   least-loaded lane), one workspace per lane, so small problems run side by
   side on the GPU;
@@ -31,6 +33,7 @@ from . import _lib, triples
 
 KEYS = triples.KEYS
 TV_CANDIDATES = (4, 8, 16)
+TILE_N_CANDIDATES = (128, 256)   # tensor-core W contraction (mixed precision only)
 
 
 @dataclass
@@ -42,11 +45,13 @@ class _Problem:
     grads: dict       # device tensors, KEYS -> gradient
     energy: torch.Tensor
     tv: int = 16
+    tile_n: int = 0
     lane: int = 0
 
 
 class Autotuner:
-    """Block size Tv per (nocc, nvir, precision, packed), chosen by timing."""
+    """(block size Tv, W-contraction N tile) per (nocc, nvir, precision,
+    packed), chosen by timing every candidate pair once."""
 
     def __init__(self, path: str | None = None):
         self.path = path
@@ -60,30 +65,39 @@ class Autotuner:
             with open(self.path, "w") as f:
                 json.dump({json.dumps(list(k)): v for k, v in self.table.items()}, f, indent=1)
 
-    def best(self, prob: _Problem, precision: str, ws: torch.Tensor, stream: torch.cuda.Stream) -> int:
+    def best(self, prob: _Problem, precision: str, ws: torch.Tensor, stream: torch.cuda.Stream):
         key = (prob.nocc, prob.nvir, precision, int(prob.packed))
         if key in self.table:
-            return int(self.table[key])
+            return _choice(self.table[key])
         lib = _lib.load()
         prec = _lib.PRECISION[precision]
         times = {}
+        tile_ns = TILE_N_CANDIDATES if precision != "fp64" else (0,)
         for tv in TV_CANDIDATES:
             if prob.nocc * tv > 1024:
                 continue
-            for rep in range(2):      # first call: one-time set-up; second: timed
-                torch.cuda.synchronize()
-                t0 = time.perf_counter()
-                _call(lib, prec, prob, ws, stream, tv)
-                torch.cuda.synchronize()
-                dt = time.perf_counter() - t0
-            times[tv] = dt
-        tv = min(times, key=times.get)
-        self.table[key] = tv
-        return tv
+            for tn in tile_ns:
+                for rep in range(2):      # first call: one-time set-up; second: timed
+                    torch.cuda.synchronize()
+                    t0 = time.perf_counter()
+                    _call(lib, prec, prob, ws, stream, tv, tn)
+                    torch.cuda.synchronize()
+                    dt = time.perf_counter() - t0
+                times[(tv, tn)] = dt
+        tv, tn = min(times, key=times.get)
+        self.table[key] = [tv, tn]
+        return tv, tn
 
 
-def _call(lib, prec, prob: _Problem, ws: torch.Tensor, stream: torch.cuda.Stream, tv: int):
-    opt = _lib.options(block_size=tv)
+def _choice(entry):
+    """A table entry: [Tv, N tile] (a bare Tv from older tables means the default N tile)."""
+    if isinstance(entry, (list, tuple)):
+        return int(entry[0]), int(entry[1])
+    return int(entry), 0
+
+
+def _call(lib, prec, prob: _Problem, ws: torch.Tensor, stream: torch.cuda.Stream, tv: int, tile_n: int = 0):
+    opt = _lib.options(block_size=tv, tile_n=tile_n)
     rc = lib.triples_energy_vjp_ex(stream.cuda_stream, prec, prob.nocc, prob.nvir, int(prob.packed),
                                    *[a.data_ptr() for a in prob.inputs], 1.0, 1, ctypes.byref(opt), ws.data_ptr(),
                                    ws.numel(), prob.energy.data_ptr(), *[prob.grads[k].data_ptr() for k in KEYS])
@@ -131,6 +145,7 @@ class BatchedTriples:
         for prob in self.problems:
             if not tune:
                 prob.tv = 16 if prob.nocc * 16 <= 1024 else 8
+                prob.tile_n = 0
                 continue
             key = (prob.nocc, prob.nvir, self.precision, int(prob.packed))
             if key not in self.autotuner.table:
@@ -139,7 +154,7 @@ class BatchedTriples:
                     scratch = torch.empty(need, dtype=torch.uint8, device=self.device)
                 with torch.cuda.stream(stream):
                     self.autotuner.best(prob, self.precision, scratch, stream)
-            prob.tv = int(self.autotuner.table[key])
+            prob.tv, prob.tile_n = _choice(self.autotuner.table[key])
         torch.cuda.synchronize()
 
     def _cost(self, prob: _Problem) -> float:
@@ -165,7 +180,7 @@ class BatchedTriples:
             for prob in self.problems:
                 if prob.lane != lane:
                     continue
-                _call(self.lib, self.prec, prob, self.workspaces[lane], st, prob.tv)
+                _call(self.lib, self.prec, prob, self.workspaces[lane], st, prob.tv, prob.tile_n)
             join = torch.cuda.Event()
             join.record(st)
             main.wait_event(join)

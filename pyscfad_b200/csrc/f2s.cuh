@@ -124,10 +124,15 @@ __device__ __forceinline__ void f2s_region(const F2P<float> &P, const float2 *sG
     const float2 *g = sG + s * C::PLANE;
     const float2 *tab = tOT + (pair * 6 + spair) * C::TBLK;
     float a1[8], f1[8];
-#pragma unroll
-    for (int z = 0; z < 8; z++) {
-        a1[z] = tT1[pt2 * 24 + pp2 * 8 + z];
-        f1[z] = tFV[pt2 * 24 + pp2 * 8 + z];
+    {
+        // rows of 8 floats at 32-byte aligned offsets: two 16-byte loads each
+        const float4 *ra = reinterpret_cast<const float4 *>(tT1 + pt2 * 24 + pp2 * 8);
+        const float4 *rf = reinterpret_cast<const float4 *>(tFV + pt2 * 24 + pp2 * 8);
+        const float4 a_lo = ra[0], a_hi = ra[1], f_lo = rf[0], f_hi = rf[1];
+        a1[0] = a_lo.x; a1[1] = a_lo.y; a1[2] = a_lo.z; a1[3] = a_lo.w;
+        a1[4] = a_hi.x; a1[5] = a_hi.y; a1[6] = a_hi.z; a1[7] = a_hi.w;
+        f1[0] = f_lo.x; f1[1] = f_lo.y; f1[2] = f_lo.z; f1[3] = f_lo.w;
+        f1[4] = f_hi.x; f1[5] = f_hi.y; f1[6] = f_hi.z; f1[7] = f_hi.w;
     }
     float colv[16];
 #pragma unroll
@@ -201,6 +206,9 @@ __global__ void __launch_bounds__(F2sSmem::NT, 2) k_f2s(F2P<float> P) {
     const int rep = P.rep0 + (int)(blockIdx.x / (unsigned)P.nsub_l);
     const F2Sub &R = P.sub[sub];
     const int ijk[3] = {P.ijk[3 * rep], P.ijk[3 * rep + 1], P.ijk[3 * rep + 2]};
+    // scalars needed later, fetched while the tiles load
+    const double e_ijk = P.mo_e[ijk[0]] + P.mo_e[ijk[1]] + P.mo_e[ijk[2]];
+    const float wscf = P.want_grad ? (float)*P.wscale : 1.0f;
 
     if (tid < 36) {
         // region pi*6 + rho: staging ordering tau holding the sub-range ordering pi
@@ -287,7 +295,6 @@ __global__ void __launch_bounds__(F2sSmem::NT, 2) k_f2s(F2P<float> P) {
     __syncthreads();
 
     // ---- orbit items: two per thread ----
-    const double e_ijk = P.mo_e[ijk[0]] + P.mo_e[ijk[1]] + P.mo_e[ijk[2]];
     double e_loc = 0.0, dd_loc = 0.0;
     float2 gres[2][6];
 #pragma unroll
@@ -358,13 +365,22 @@ __global__ void __launch_bounds__(F2sSmem::NT, 2) k_f2s(F2P<float> P) {
             for (int s = 0; s < 6; s++)
                 gres[it][s] = make_float2((float)(g0 * (Z[s] + RW[s])), (float)(g0 * 0.5 * RW[s]));
             dd_loc += ddi;
-            // d E / d e_abc = -ddi: the a-slot is uniform over the warp
+            // d E / d e_abc = -ddi.  Over a warp the a-slot is uniform, the b-slot
+            // is fixed within 8-lane groups and the c-slot is lane % 8: reduce
+            // with shuffles first, then one shared atomic per distinct slot.
             double da = -ddi;
+            double db = da;
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) da += __shfl_down_sync(0xffffffffu, da, off);
-            if (lane == 0) atomicAdd(&s_evbar[loc[0]], da);
-            atomicAdd(&s_evbar[8 + loc[1]], -ddi);
-            atomicAdd(&s_evbar[16 + loc[2]], -ddi);
+            for (int off = 4; off > 0; off >>= 1) db += __shfl_xor_sync(0xffffffffu, db, off);
+            double dc = da;
+            dc += __shfl_xor_sync(0xffffffffu, dc, 8);
+            dc += __shfl_xor_sync(0xffffffffu, dc, 16);
+            double dsum = db;
+            dsum += __shfl_xor_sync(0xffffffffu, dsum, 8);
+            dsum += __shfl_xor_sync(0xffffffffu, dsum, 16);
+            if (lane == 0) atomicAdd(&s_evbar[loc[0]], dsum);
+            if ((lane & 7) == 0) atomicAdd(&s_evbar[8 + loc[1]], db);
+            if (lane < 8) atomicAdd(&s_evbar[16 + loc[2]], dc);
         }
     }
 
@@ -404,7 +420,6 @@ __global__ void __launch_bounds__(F2sSmem::NT, 2) k_f2s(F2P<float> P) {
     if (tid < 24 && s_evbar[tid] != 0.0) atomicAdd(&P.mo_bar[o + R.st[tid >> 3] + (tid & 7)], s_evbar[tid]);
 
     // ---- write back Wbar and add the V-term gradients: one region per warp at a time ----
-    const float wscf = (float)*P.wscale;
 #pragma unroll 1
     for (int reg = warp; reg < 36; reg += NW) {
         const int pi = reg / 6, rho = reg % 6;

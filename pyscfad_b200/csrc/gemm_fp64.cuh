@@ -1,13 +1,16 @@
-// FP64 SIMT GEMM tile with multi-index operand maps.  This is the "plain FP64
+// FP64 GEMM tile with multi-index operand maps.  This is the "plain FP64
 // GPU form" of the (T) contractions: the same chunked algorithm as the
-// tensor-core path, computed with DFMA.
+// mixed-precision path, computed on the FP64 tensor cores
+// (mma.sync.m8n8k4.f64: per 8x8 output tile a thread holds D[g][2t..2t+1],
+// and A[g][t], B[t][g] of each k-step, g = lane / 4, t = lane % 4).
 //
 //   C(m,n) = alpha * [ sum_k A(m,k) B(n,k) + alpha2 * sum_k A2(m,k) B2(n,k) ]
 //            (+ C(m,n) when accumulate)
 //   A(m,k) = A.p[apply(A.mn, m) + apply(A.k, k)], likewise B, A2, B2, C.
 //
-// 128x128 output tile, 256 threads, 8x8 outputs per thread, K tiles of 8,
-// register-staged double buffering.  The k part of every operand offset is
+// 128x128 output tile, 256 threads (8 warps as 2 x 4, each 64 x 32 = 8 x 4
+// MMA tiles), K tiles of 8 (two k-steps of 4), register-staged double
+// buffering.  The k part of every operand offset is
 // tabulated per K tile in shared memory two tiles ahead (16 threads, one
 // apply() each), so the loads themselves are one add per element.
 #pragma once
@@ -39,9 +42,13 @@ using GemmArgs = GemmArgsT<double>;
 
 constexpr int kGBM = 128, kGBN = 128, kGBK = 8;
 
+// Row stride 132 = 4 (mod 16): the fragment loads of a half-warp (g in 0..3,
+// t in 0..3 at t * 132 + g) hit 16 distinct 8-byte banks.
+constexpr int kGLd = kGBM + 4;
+
 struct GemmSmem {
-    double As[2][kGBK][kGBM + 1];
-    double Bs[2][kGBK][kGBN + 1];
+    double As[2][kGBK][kGLd];
+    double Bs[2][kGBK][kGLd];
     long long rowA[kGBM], rowB[kGBN], rowA2[kGBM], rowB2[kGBN];
     long long koff[2][2][kGBK];   // [tile parity][A, B][k in tile]: k part of the offset (-1: k >= K)
 };
@@ -67,7 +74,7 @@ __device__ __forceinline__ void gemm_load_tile(const GOpT<T> &op, const long lon
     }
 }
 
-__device__ __forceinline__ void gemm_store_tile(double (*S)[kGBM + 1], int kfast, int tid,
+__device__ __forceinline__ void gemm_store_tile(double (*S)[kGLd], int kfast, int tid,
                                                 const double (&r)[4]) {
 #pragma unroll
     for (int i = 0; i < 4; i++) {
@@ -84,10 +91,18 @@ __device__ __forceinline__ void gemm_store_tile(double (*S)[kGBM + 1], int kfast
     }
 }
 
+__device__ __forceinline__ void dmma_884(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
 template <typename TA>
 __device__ void gemm_fp64_tile(const GemmArgsT<TA> &g, int m0, int n0, GemmSmem &sm) {
     const int tid = threadIdx.x;
-    const int tx = tid & 15, ty = tid >> 4;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int fg = lane >> 2, ft = lane & 3;                 // fragment row / k index
+    const int wm0 = (warp >> 2) * 64, wn0 = (warp & 3) * 32;  // this warp's 64 x 32 block
     if (tid < 128) {
         int m = m0 + tid;
         bool ok = m < g.M;
@@ -102,11 +117,11 @@ __device__ void gemm_fp64_tile(const GemmArgsT<TA> &g, int m0, int n0, GemmSmem 
     }
     __syncthreads();
 
-    double acc[8][8];
+    double acc[8][4][2];   // [m tile][n tile][column pair]
 #pragma unroll
     for (int i = 0; i < 8; i++)
 #pragma unroll
-        for (int j = 0; j < 8; j++) acc[i][j] = 0.0;
+        for (int j = 0; j < 4; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
 
     const int kt1 = (g.K + kGBK - 1) / kGBK;
     const int kt2 = (g.K2 > 0) ? (g.K2 + kGBK - 1) / kGBK : 0;
@@ -156,16 +171,16 @@ __device__ void gemm_fp64_tile(const GemmArgsT<TA> &g, int m0, int n0, GemmSmem 
         // tile kt + 2 reuses the k table of tile kt, whose loads are done
         tab_koff(kt + 2);
 #pragma unroll
-        for (int kk = 0; kk < kGBK; kk++) {
-            double a[8], b[8];
+        for (int ks = 0; ks < kGBK; ks += 4) {
+            double a[8], b[4];
 #pragma unroll
-            for (int i = 0; i < 8; i++) a[i] = sm.As[buf][kk][ty + 16 * i];
+            for (int i = 0; i < 8; i++) a[i] = sm.As[buf][ks + ft][wm0 + 8 * i + fg];
 #pragma unroll
-            for (int j = 0; j < 8; j++) b[j] = sm.Bs[buf][kk][tx + 16 * j];
+            for (int j = 0; j < 4; j++) b[j] = sm.Bs[buf][ks + ft][wn0 + 8 * j + fg];
 #pragma unroll
             for (int i = 0; i < 8; i++)
 #pragma unroll
-                for (int j = 0; j < 8; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+                for (int j = 0; j < 4; j++) dmma_884(acc[i][j][0], acc[i][j][1], a[i], b[j]);
         }
         if (kt + 1 < kt_total) {
             gemm_store_tile(sm.As[buf ^ 1], kfA(kt + 1), tid, ra);
@@ -176,15 +191,16 @@ __device__ void gemm_fp64_tile(const GemmArgsT<TA> &g, int m0, int n0, GemmSmem 
 
 #pragma unroll
     for (int i = 0; i < 8; i++) {
-        int m = m0 + ty + 16 * i;
+        int m = m0 + wm0 + 8 * i + fg;
         if (m >= g.M) continue;
         long long cmo = apply(g.cm, m);
 #pragma unroll
-        for (int j = 0; j < 8; j++) {
-            int n = n0 + tx + 16 * j;
+        for (int jj = 0; jj < 8; jj++) {
+            const int j = jj >> 1, c = jj & 1;
+            int n = n0 + wn0 + 8 * j + 2 * ft + c;
             if (n >= g.N) continue;
             long long off = cmo + apply(g.cn, n);
-            double val = g.alpha * acc[i][j];
+            double val = g.alpha * acc[i][j][c];
             if (g.accumulate == 2) {
                 atomicAdd(&g.C[off], val);
                 continue;

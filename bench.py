@@ -315,35 +315,51 @@ def run_accuracy(args, o, v, naux):
     a0, a1 = args.slice if args.slice else (0, 0)
     stream = torch.cuda.current_stream(dev)
 
+    # The FP64 form may run with a smaller virtual block (--fp64-block) so its
+    # FP64 staging fits next to the inputs at the largest sizes; a slice of
+    # 16-wide blocks [a0, a1) is the slice [a0 16/tv, a1 16/tv) of tv-wide
+    # blocks (the same virtual triples a >= b >= c with a in [16 a0, 16 a1)).
+    tv64 = args.fp64_block
+
     def run(prec, tv=0):
+        s = 16 // (tv or 16)
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
         t0.record(stream)
         e, g = triples.energy_vjp(*xs, ybar=1.0, precision=prec, device=dev, block_size=tv,
-                                  chunk_range=(a0, a1))
+                                  chunk_range=(a0 * s, a1 * s))
         t1.record(stream)
         torch.cuda.synchronize()
-        return float(e), {k: t.cpu().numpy() for k, t in g.items()}, t0.elapsed_time(t1) / 1e3
+        out = float(e), {k: t.cpu().numpy() for k, t in g.items()}, t0.elapsed_time(t1) / 1e3
+        del g
+        triples.release_workspace()
+        torch.cuda.empty_cache()
+        return out
 
+    precs = ("mixed",) if args.no_bf16 else ("mixed", "mixed_bf16")
     if args.slice:   # one-time set-up of both paths outside the timed calls
-        for prec in ("fp64", "mixed", "mixed_bf16"):
-            triples.energy_vjp(*xs, ybar=1.0, precision=prec, device=dev, chunk_range=(0, 1))
-        torch.cuda.synchronize()
-    e64, g64, t64 = run("fp64", 16)
-    e64b = e64 if args.slice else run("fp64", 8)[0]
+        for prec in ("fp64",) + precs:
+            s = 16 // tv64 if prec == "fp64" else 1
+            triples.energy_vjp(*xs, ybar=1.0, precision=prec, device=dev, chunk_range=(0, s),
+                               block_size=tv64 if prec == "fp64" else 0)
+            torch.cuda.synchronize()
+            triples.release_workspace()
+            torch.cuda.empty_cache()
+    e64, g64, t64 = run("fp64", tv64)
+    e64b = e64 if args.slice else run("fp64", 8 if tv64 == 16 else 16)[0]
 
     def relerr(a, b):
         return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
 
     out = {"workload": args.workload, "nocc": o, "nvir": v, "naux": naux, "scale": args.scale,
-           "e_fp64": e64, "fp64_seconds": t64}
+           "e_fp64": e64, "fp64_seconds": t64, "fp64_block": tv64}
     if args.slice:
         frac = triples.chunk_fraction(v, a0, a1)
         out.update({"slice_blocks": [a0, a1], "slice_fraction_of_amplitudes": frac,
                     "fp64_seconds_full_extrapolated": t64 / frac})
     else:
         out.update({"fp64_noise_abs": abs(e64 - e64b), "fp64_noise_rel": abs(e64 - e64b) / abs(e64)})
-    for prec in ("mixed", "mixed_bf16"):
+    for prec in precs:
         e, g, tm = run(prec)
         out[prec] = {"e": e, "abs_dE": abs(e - e64), "rel_dE": abs(e - e64) / abs(e64), "seconds": tm,
                      "speedup_vs_fp64": t64 / tm,
@@ -523,6 +539,9 @@ def main():
     ap.add_argument("--slice", type=int, nargs=2, metavar=("A0", "A1"), default=None,
                     help="with --accuracy: only the chunks whose largest virtual block is in [A0, A1), "
                          "timed in both precisions (FP64 vs mixed on identical work)")
+    ap.add_argument("--fp64-block", type=int, default=16, choices=[4, 8, 16],
+                    help="with --accuracy: virtual block size of the FP64 run (8 or 4 shrink its FP64 staging)")
+    ap.add_argument("--no-bf16", action="store_true", help="with --accuracy: skip the bf16 mode")
     ap.add_argument("--batched", action="store_true",
                     help="instead of the headline: 256 uneven problems (nocc 4-12, nvir 20-80, naux 4(o+v)) "
                          "as one CUDA-graph launch vs one call per problem; one JSON line")

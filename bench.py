@@ -316,9 +316,11 @@ def run_accuracy(args, o, v, naux):
     stream = torch.cuda.current_stream(dev)
 
     # The FP64 form may run with a smaller virtual block (--fp64-block) so its
-    # FP64 staging fits next to the inputs at the largest sizes; a slice of
-    # 16-wide blocks [a0, a1) is the slice [a0 16/tv, a1 16/tv) of tv-wide
-    # blocks (the same virtual triples a >= b >= c with a in [16 a0, 16 a1)).
+    # FP64 staging fits next to the inputs at the largest sizes (likewise
+    # --mixed-block); a slice of 16-wide blocks [a0, a1) is the slice
+    # [a0 16/tv, a1 16/tv) of tv-wide blocks (the same virtual triples
+    # a >= b >= c with a in [16 a0, 16 a1)).  Gradients stay on the device and
+    # are compared there, one input at a time.
     tv64 = args.fp64_block
 
     def run(prec, tv=0):
@@ -330,18 +332,18 @@ def run_accuracy(args, o, v, naux):
                                   chunk_range=(a0 * s, a1 * s))
         t1.record(stream)
         torch.cuda.synchronize()
-        out = float(e), {k: t.cpu().numpy() for k, t in g.items()}, t0.elapsed_time(t1) / 1e3
-        del g
+        out = float(e), g, t0.elapsed_time(t1) / 1e3
         triples.release_workspace()
         torch.cuda.empty_cache()
         return out
 
     precs = ("mixed",) if args.no_bf16 else ("mixed", "mixed_bf16")
+    tvm = args.mixed_block if args.mixed_block != 16 else 0
     if args.slice:   # one-time set-up of both paths outside the timed calls
         for prec in ("fp64",) + precs:
-            s = 16 // tv64 if prec == "fp64" else 1
-            triples.energy_vjp(*xs, ybar=1.0, precision=prec, device=dev, chunk_range=(0, s),
-                               block_size=tv64 if prec == "fp64" else 0)
+            tvp = tv64 if prec == "fp64" else (tvm or 16)
+            triples.energy_vjp(*xs, ybar=1.0, precision=prec, device=dev, chunk_range=(0, 16 // tvp),
+                               block_size=tvp)
             torch.cuda.synchronize()
             triples.release_workspace()
             torch.cuda.empty_cache()
@@ -349,10 +351,10 @@ def run_accuracy(args, o, v, naux):
     e64b = e64 if args.slice else run("fp64", 8 if tv64 == 16 else 16)[0]
 
     def relerr(a, b):
-        return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+        return float((a - b).abs().max() / max(float(b.abs().max()), 1e-300))
 
     out = {"workload": args.workload, "nocc": o, "nvir": v, "naux": naux, "scale": args.scale,
-           "e_fp64": e64, "fp64_seconds": t64, "fp64_block": tv64}
+           "e_fp64": e64, "fp64_seconds": t64, "fp64_block": tv64, "mixed_block": tvm or 16}
     if args.slice:
         frac = triples.chunk_fraction(v, a0, a1)
         out.update({"slice_blocks": [a0, a1], "slice_fraction_of_amplitudes": frac,
@@ -360,10 +362,12 @@ def run_accuracy(args, o, v, naux):
     else:
         out.update({"fp64_noise_abs": abs(e64 - e64b), "fp64_noise_rel": abs(e64 - e64b) / abs(e64)})
     for prec in precs:
-        e, g, tm = run(prec)
+        e, g, tm = run(prec, tvm)
         out[prec] = {"e": e, "abs_dE": abs(e - e64), "rel_dE": abs(e - e64) / abs(e64), "seconds": tm,
                      "speedup_vs_fp64": t64 / tm,
                      "grad_rel_err": {k: relerr(g[k], g64[k]) for k in g64}}
+        del g
+        torch.cuda.empty_cache()
     print(json.dumps(out))
 
 
@@ -531,6 +535,9 @@ def main():
     ap.add_argument("--budget", type=float, default=1450.0,
                     help="wall-clock seconds the whole run may take; timed steps beyond it are not run "
                          "(the line reports the count timed)")
+    ap.add_argument("--e2e-host-gb", type=float, default=32.0,
+                    help="largest pinned host buffers (inputs + gradients) the e2e leg may allocate; the "
+                         "headline workload needs 22 GB")
     ap.add_argument("--cpu-reserve", type=float, default=150.0,
                     help="seconds of the budget kept for the CPU-baseline leg")
     ap.add_argument("--accuracy", action="store_true",
@@ -541,6 +548,8 @@ def main():
                          "timed in both precisions (FP64 vs mixed on identical work)")
     ap.add_argument("--fp64-block", type=int, default=16, choices=[4, 8, 16],
                     help="with --accuracy: virtual block size of the FP64 run (8 or 4 shrink its FP64 staging)")
+    ap.add_argument("--mixed-block", type=int, default=16, choices=[4, 8, 16],
+                    help="with --accuracy: virtual block size of the mixed-precision runs")
     ap.add_argument("--no-bf16", action="store_true", help="with --accuracy: skip the bf16 mode")
     ap.add_argument("--batched", action="store_true",
                     help="instead of the headline: 256 uneven problems (nocc 4-12, nvir 20-80, naux 4(o+v)) "
@@ -596,6 +605,7 @@ def main():
     inp["ovvv"] = inp["ovvv"][:, :, il, jl].contiguous()   # packed DF layout (dfccsd.py:88)
     keys = triples.KEYS
     dev_args = [inp[k] for k in keys]
+    ovvv_gb = inp["ovvv"].numel() * 8 / 1e9
     torch.cuda.synchronize()
 
     def barrier():
@@ -656,31 +666,47 @@ def main():
     value = job_throughput(world, n_steps, flops["step"], t_dev)
 
     # end-to-end through the public API with host buffers: pinned host inputs
-    # copied in and E plus every gradient copied out, inside the timed region
-    host_in = [a.cpu().pin_memory() for a in dev_args]
-    h2d = sum(a.numel() * a.element_size() for a in host_in)
-    grads_host = {k: torch.empty(a.shape, dtype=a.dtype, pin_memory=True) for k, a in zip(keys, dev_args)}
-    e_host = torch.empty((), dtype=torch.float64, pin_memory=True)
-    d2h = 8 + sum(t.numel() * t.element_size() for t in grads_host.values())
-    barrier()
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(n_e2e):
-        dev_in = [a.to(dev, non_blocking=True) for a in host_in]
-        ee, gg = triples.energy_vjp(*dev_in, ybar=1.0, precision=args.precision, device=dev, check=False)
-        e_host.copy_(ee, non_blocking=True)
-        for k in keys:
-            grads_host[k].copy_(gg[k], non_blocking=True)
-        del dev_in, gg
-    e1.record()
-    torch.cuda.synchronize()
-    barrier()
-    t_e2e = e0.elapsed_time(e1) / 1e3
-    t_e2e = max_over_ranks(t_e2e, dev)
-    e2e_value = job_throughput(world, n_e2e, flops["step"], t_e2e)
-    del host_in
+    # copied in and E plus every gradient copied out, inside the timed region.
+    # The device-resident inputs are dropped first (the e2e call copies its
+    # own); pinned host buffers above --e2e-host-gb (inputs + gradients) are
+    # not attempted, and the line says so.
+    in_bytes = sum(a.numel() * a.element_size() for a in dev_args)
+    h2d = in_bytes
+    d2h = 8 + in_bytes
+    e2e_value, e2e_note = None, None
+    if (h2d + d2h) / 1e9 > args.e2e_host_gb:
+        e2e_note = ("not run: %.1f GB of pinned host buffers exceed the %.0f GB allowed by --e2e-host-gb"
+                    % ((h2d + d2h) / 1e9, args.e2e_host_gb))
+    else:
+        host_in = []
+        for a in dev_args:
+            hb = torch.empty(a.shape, dtype=a.dtype, pin_memory=True)
+            hb.copy_(a)
+            host_in.append(hb)
+        grads_host = {k: torch.empty(a.shape, dtype=a.dtype, pin_memory=True) for k, a in zip(keys, dev_args)}
+        e_host = torch.empty((), dtype=torch.float64, pin_memory=True)
+        del dev_args, inp
+        triples.release_workspace()
+        torch.cuda.empty_cache()
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(n_e2e):
+            dev_in = [a.to(dev, non_blocking=True) for a in host_in]
+            ee, gg = triples.energy_vjp(*dev_in, ybar=1.0, precision=args.precision, device=dev, check=False)
+            e_host.copy_(ee, non_blocking=True)
+            for k in keys:
+                grads_host[k].copy_(gg[k], non_blocking=True)
+            del dev_in, gg
+        e1.record()
+        torch.cuda.synchronize()
+        barrier()
+        t_e2e = e0.elapsed_time(e1) / 1e3
+        t_e2e = max_over_ranks(t_e2e, dev)
+        e2e_value = job_throughput(world, n_e2e, flops["step"], t_e2e)
+        del host_in, grads_host
 
     # roofline of the dominant kernel class
     peaks = {}
@@ -745,13 +771,13 @@ def main():
         "data": DATA,
         "config": {"workload": args.workload, "nocc": o, "nvir": v, "naux": naux, "precision": args.precision,
                    "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (packed ovvv %.1f GB)" % (inp["ovvv"].numel() * 8 / 1e9),
+                   "l2": "inputs larger than L2 (packed ovvv %.1f GB)" % (ovvv_gb),
                    "e_t": e_val,
                    "step_plan": ("warm-up %d, timed %d of %d requested, e2e %d: the steps that fit a %d s "
                                  "wall-clock budget at %.1f s per step" % (n_warm, n_steps, args.steps, n_e2e,
                                                                            args.budget, step_s))},
         "e2e": {"value": e2e_value, "unit": "TFLOP/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "steps": n_e2e},
+                "steps": n_e2e if e2e_value is not None else 0, **({"note": e2e_note} if e2e_note else {})},
         "gpu_launches": int(sum(c for _, c in prof.values())),
         "triplets_per_s": world * n_steps * (o * (o + 1) * (o + 2) // 6) / t_dev,
         "kernel_ms": {k: round(m, 3) for k, (m, _) in prof.items()},

@@ -101,3 +101,39 @@ def test_energy_without_gradients_takes_the_energy_only_call():
     e = ccsd_t.ccsd_t_energy(*ts, torch.tensor(inp.t1, device=dev), torch.tensor(inp.t2, device=dev))
     assert not e.requires_grad
     assert abs(float(e) - e_ref) <= E_RTOL * abs(e_ref)
+
+
+class _FakeCCSD:
+    """The attributes pyscfad's CCSD.ccsd_t reads (ccsd.py:420-429)."""
+
+    def __init__(self, inp, eris):
+        self.t1, self.t2, self.mo_coeff, self.verbose, self.max_memory = inp.t1, inp.t2, "C", 0, 4000
+        self._eris, self.ao2mo_calls = eris, []
+
+    def ao2mo(self, mo_coeff):
+        self.ao2mo_calls.append(mo_coeff)
+        return self._eris
+
+
+@pytest.mark.parametrize("precision,etol", [("fp64", E_RTOL), ("mixed", 1e-6)])
+def test_ccsd_t_method_routes_to_the_gpu_kernel(precision, etol):
+    from pyscfad_b200.cc import ccsd as gpu_ccsd
+
+    inp, e_ref, _, _ = G.load("o5v19_fvo")
+    eris, _ = _eris_and_cc(inp)
+
+    class CC(_FakeCCSD):
+        pass
+
+    gpu_ccsd.install(CC, precision=precision)
+    mycc = CC(inp, eris)
+    e = mycc.ccsd_t()                      # defaults: self.t1, self.t2, self.ao2mo(self.mo_coeff)
+    assert mycc.ao2mo_calls == ["C"]
+    assert abs(e - e_ref) <= etol * abs(e_ref)
+    e2 = mycc.ccsd_t(inp.t1, inp.t2, eris)  # explicit arguments: no ao2mo
+    assert mycc.ao2mo_calls == ["C"] and e2 == e
+
+    class CC2(gpu_ccsd.CCSDTriplesMixin, _FakeCCSD):
+        triples_precision = precision
+
+    assert abs(CC2(inp, eris).ccsd_t() - e_ref) <= etol * abs(e_ref)

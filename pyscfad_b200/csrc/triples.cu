@@ -17,7 +17,7 @@
 #include "gemm_fp64.cuh"
 #include "tc_f1.cuh"
 #include "f2.cuh"
-#include "f2s.cuh"
+#include "f2p.cuh"
 #include "tc_b1.cuh"
 #include "lno.cuh"
 #include "pyscfad_b200.h"
@@ -167,7 +167,13 @@ int make_plan(int precision, int nocc, int nvir, int packed, int want_grad, Plan
     } else {
         P.kseg = 1;
     }
-    if (P.f1_bn == 0) P.f1_bn = ((nocc + 7) / 8) * 8 < ((nocc + 15) / 16) * 16 ? 128 : 256;
+    // W-contraction N tile: 256 columns (16 r x 16 z) unless padding nocc to
+    // 16 wastes more than a quarter of the r values and 8-wide r tiles waste
+    // less (measured at nocc = 40: 256 is 3% faster despite 48 padded r)
+    if (P.f1_bn == 0) {
+        const int p16 = ((nocc + 15) / 16) * 16, p8 = ((nocc + 7) / 8) * 8;
+        P.f1_bn = (4 * p16 > 5 * nocc && p8 < p16) ? 128 : 256;
+    }
     P.lno = lno ? 1 : 0;
     P.prec = precision;
     P.want_grad = want_grad ? 1 : 0;
@@ -1084,10 +1090,10 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
             TB_CUDA(cudaFuncSetAttribute(k_f2t<StageT, kSB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)f2_smem_bytes<StageT, kSB>()));
             if (sizeof(StageT) == 4) {
-                TB_CUDA(cudaFuncSetAttribute(k_f2s<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)F2sSmem::BYTES));
-                TB_CUDA(cudaFuncSetAttribute(k_f2s<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)F2sSmem::BYTES));
+                TB_CUDA(cudaFuncSetAttribute(k_f2p<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)F2pSmem::BYTES));
+                TB_CUDA(cudaFuncSetAttribute(k_f2p<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)F2pSmem::BYTES));
             }
             F2Pattern pats[kF2Patterns];
             f2_build_patterns(pats);
@@ -1293,7 +1299,7 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                     // F2: energy (+ adjoint of the raw amplitudes).  Sub-range
                     // triples of three distinct full 8-wide sub-ranges come first;
                     // with the all-distinct occupied representatives (the first
-                    // n_distinct_ijk of the table) they go to the lean kernel k_f2s
+                    // n_distinct_ijk of the table) they go to the persistent kernel k_f2p
                     // in the mixed modes, every other CTA to k_f2t.
                     F2P<StageT> F;
                     F.d = d;
@@ -1355,11 +1361,12 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                         F.nsub_l = n_simple_sub;
                         F2P<float> Ff;
                         std::memcpy(&Ff, &F, sizeof(F));   // StageT = float in the mixed modes
-                        const unsigned nb = (unsigned)(nd * n_simple_sub);
+                        const int nitems = nd * n_simple_sub;
+                        const unsigned nb = (unsigned)(nitems < num_sms() ? nitems : num_sms());
                         if (bf16)
-                            TB_KLAUNCH(P_F2, (k_f2s<2><<<nb, F2sSmem::NT, F2sSmem::BYTES, st>>>(Ff)));
+                            TB_KLAUNCH(P_F2, (k_f2p<2><<<nb, F2pSmem::NT, F2pSmem::BYTES, st>>>(Ff, nitems)));
                         else
-                            TB_KLAUNCH(P_F2, (k_f2s<1><<<nb, F2sSmem::NT, F2sSmem::BYTES, st>>>(Ff)));
+                            TB_KLAUNCH(P_F2, (k_f2p<1><<<nb, F2pSmem::NT, F2pSmem::BYTES, st>>>(Ff, nitems)));
                     }
                     int frc;
                     if ((frc = f2t(0, nd, n_simple_sub, F.nsub - n_simple_sub)) != TRIPLES_OK) return frc;

@@ -661,6 +661,7 @@ def main():
     t_dev = s0.elapsed_time(s1) / 1e3
     t_dev = max_over_ranks(t_dev, dev)
     _lib.check(triples.device_status(dev), "timed steps")
+    peak_mem = torch.cuda.max_memory_allocated(dev)   # inputs + gradients + workspace, input generation included
 
     flops = algorithmic_flops(o, v)
     value = job_throughput(world, n_steps, flops["step"], t_dev)
@@ -780,6 +781,7 @@ def main():
                 "steps": n_e2e if e2e_value is not None else 0, **({"note": e2e_note} if e2e_note else {})},
         "gpu_launches": int(sum(c for _, c in prof.values())),
         "triplets_per_s": world * n_steps * (o * (o + 1) * (o + 2) // 6) / t_dev,
+        "device_peak_gb": round(peak_mem / 1e9, 2),
         "kernel_ms": {k: round(m, 3) for k, (m, _) in prof.items()},
         "roofline": roof,
         "clocks": clk,

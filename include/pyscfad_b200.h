@@ -79,8 +79,8 @@ typedef struct triples_options {
      * before the partial result is added in higher precision; 0 = default (1). */
     int accumulation_segment;
     /* mixed precision: N tile of the W contraction, 128 or 256 columns
-     * (8 or 16 occupied indices x 16 virtuals); 0 = the one that pads nocc
-     * least.  Performance only. */
+     * (8 or 16 occupied indices x 16 virtuals); 0 = 256 unless padding nocc
+     * to 16 wastes over a quarter of it.  Performance only. */
     int tile_n;
 } triples_options;
 

@@ -229,9 +229,10 @@ def load_traffic(workload, precision):
 
 
 def run_batched(args):
-    """Many small uneven problems: one CUDA-graph replay of the whole batch against
-    one E+VJP call per problem on one stream (each call being the kernel sequence
-    of one problem)."""
+    """Many small uneven problems: the batch engine (one launch per kernel kind
+    and chunk step over all problems) replayed as one CUDA graph, against one
+    E+VJP call per problem on one stream and against the per-problem calls
+    spread over 8 streams and captured as one graph."""
     import numpy as np
     import torch
 
@@ -249,12 +250,6 @@ def run_batched(args):
         il, jl = torch.tril_indices(v, v, device=dev)
         inp["ovvv"] = inp["ovvv"][:, :, il, jl].contiguous()
         probs.append({k: inp[k] for k in triples.KEYS})
-    t0 = time.perf_counter()
-    bt = BatchedTriples(probs, precision=args.precision, lanes=8, autotuner=Autotuner())
-    t_tune = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    bt.capture()
-    t_cap = time.perf_counter() - t0
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
 
     def timed(fn, reps):
@@ -268,30 +263,54 @@ def run_batched(args):
         torch.cuda.synchronize()
         return ev[0].elapsed_time(ev[1]) / 1e3 / reps
 
+    t0 = time.perf_counter()
+    bt = BatchedTriples(probs, precision=args.precision, tune=False, engine="batch")
+    t_create = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    bt.capture()
+    t_cap = time.perf_counter() - t0
+    lib = bt.lib
+    lib.triples_profile_enable(1)
     t_graph = timed(bt.run, max(args.steps, 3))
     e_graph = np.array([e for e, _ in bt.results()])
     bt.check()
-    # one call per problem, default block size, one stream
+    t_eager = timed(bt.run_eager, 1)
+    import ctypes
+    ncat = 16
+    ms, cnt = (ctypes.c_double * ncat)(), (ctypes.c_int * ncat)()
+    ncat = lib.triples_profile_read(ncat, ms, cnt)
+    lib.triples_profile_enable(0)
+    launches_eager = int(sum(cnt[i] for i in range(ncat)))   # profiled: the eager runs (warm-up + timed)
+    nrun = max(args.warmup, 1) + 1
+    kernel_ms = {lib.triples_profile_name(i).decode(): round(ms[i] / nrun, 3) for i in range(ncat) if cnt[i]}
+    flops = sum(8.0 * p["t1"].shape[0] ** 3 * p["t1"].shape[1] ** 4 for p in probs)
 
     def one_by_one():
         for p in probs:
             triples.energy_vjp(*(p[k] for k in triples.KEYS), precision=args.precision, device=dev, check=False)
 
     t_single = timed(one_by_one, 1)
-    t_lanes = timed(bt.run_eager, 1)
+    del bt
+    torch.cuda.empty_cache()
+    lanes = BatchedTriples(probs, precision=args.precision, lanes=8, tune=False, engine="lanes")
+    lanes.capture()
+    t_lanes = timed(lanes.run, max(args.steps, 3))
     n = len(probs)
     line = {"metric": "(T) E+VJP instances/s, batched uneven problems", "impl": "ours",
             "config": {"workload": "batched_c3", "instances": n, "nocc": "U{4..12}", "nvir": "U{20..80}",
-                       "naux": "4(o+v)", "precision": args.precision, "lanes": bt.lanes},
+                       "naux": "4(o+v)", "precision": args.precision, "engine": "batch (one launch per kernel "
+                       "kind and chunk step over all problems), one CUDA graph"},
             "unit": "instances/s", "higher_is_better": True,
+            "value": n / t_graph,
             "graph_instances_per_s": n / t_graph, "graph_ms_per_batch": t_graph * 1e3,
-            "one_call_per_instance_per_s": n / t_single, "eager_lanes_per_s": n / t_lanes,
-            "speedup_graph_vs_one_call_per_instance": t_single / t_graph,
-            "autotune_s": t_tune, "capture_s": t_cap,
-            "tuned_block_sizes": {str(k): v for k, v in sorted(
-                {tv: sum(1 for p in bt.problems if p.tv == tv) for tv in (4, 8, 16)}.items())},
-            "tuned_w_tiles": {str(k): v for k, v in sorted(
-                {tn: sum(1 for p in bt.problems if p.tile_n == tn) for tn in (0, 128, 256)}.items())},
+            "tflops_at_8o3v4": flops / t_graph / 1e12,
+            "eager_batch_instances_per_s": n / t_eager,
+            "launches_per_batch": launches_eager // nrun, "kernel_ms_per_batch_eager": kernel_ms,
+            "one_call_per_instance_per_s": n / t_single,
+            "lanes_graph_instances_per_s": n / t_lanes,
+            "speedup_vs_one_call_per_instance": t_single / t_graph,
+            "speedup_vs_lanes_graph": t_lanes / t_graph,
+            "create_s": t_create, "capture_s": t_cap,
             "e_sum": float(e_graph.sum())}
     print(json.dumps(line))
 

@@ -267,6 +267,52 @@ int triples_static_check_device_status(void *stream);
  * error bits, sits at offset 0). */
 int triples_static_scratch(void **ptr, size_t *bytes);
 
+/* ---- batched calls: many (T) problems of uneven size -------------------------
+ *
+ * The reference evaluates one molecule per call (pyscfad/cc/ccsd_t.py:28-192,
+ * ccsd_t_energy_vjp at pyscfadlib/pyscfadlib/vjp/cc/ccsd_t_vjp.c:332-346);
+ * these entry points run E(T) and its VJP (one adjoint seed for all) for a
+ * list of problems, each with the layouts and outputs of
+ * triples_energy_vjp.  In the mixed modes every kernel kind is launched once
+ * per chunk step over the corresponding chunk of every problem, instead of
+ * once per chunk per problem; an FP64 batch runs its problems one after
+ * another. */
+typedef struct triples_problem {
+    int nocc, nvir, ovvv_packed;
+    int block_size;   /* virtual block size, 0 = default (triples_options.block_size) */
+    int tile_n;       /* W-contraction N tile, 0 = default (triples_options.tile_n) */
+    const double *mo_energy, *t1, *t2, *ovoo, *ovov, *ovvv, *fvo;
+    double *e_out;
+    double *mo_energy_bar, *t1_bar, *t2_bar, *ovoo_bar, *ovov_bar, *ovvv_bar, *fvo_bar;
+} triples_problem;
+
+typedef struct triples_batch triples_batch;   /* opaque */
+
+/* Bytes of device workspace a batch of these problems needs (0 on invalid
+ * arguments): every problem's workspace plus the batch's job tables. */
+size_t triples_batch_workspace_size(int precision, int nprob, const triples_problem *probs);
+
+/* Plans the batch over `workspace` and writes its job tables there (a
+ * blocking host-to-device copy: not for stream capture).  The problems'
+ * buffers and the workspace must stay allocated, at the same addresses, for
+ * as long as the batch is used; their values may change between runs.
+ * *batch receives a handle for triples_batch_run / _destroy. */
+int triples_batch_create(int precision, int nprob, const triples_problem *probs, double ybar, void *workspace,
+                         size_t workspace_bytes, triples_batch **batch);
+
+/* Runs the whole batch on `stream` (asynchronous; no host allocation and no
+ * synchronisation, so it can be captured into a CUDA graph after a first
+ * eager run has done the library's one-time device set-up).  Runs of the
+ * same batch on different streams race on its workspace. */
+int triples_batch_run(triples_batch *batch, void *stream);
+
+/* Synchronises `stream` and reports device-side failures of the last run
+ * (TRIPLES_ERR_DEVICE_TIMEOUT if any problem's bounded waits gave up). */
+int triples_batch_check_device_status(triples_batch *batch, void *stream);
+
+/* Frees the handle (not the workspace). */
+void triples_batch_destroy(triples_batch *batch);
+
 /* Human-readable text for a triples_status value. */
 const char *triples_status_string(int status);
 

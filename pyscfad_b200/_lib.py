@@ -32,6 +32,15 @@ def options(block_size=0, chunk_range=None, accumulation_segment=0, tile_n=0):
     return Options(int(block_size), int(a0), int(a1), int(accumulation_segment), int(tile_n))
 
 
+class Problem(ctypes.Structure):
+    """triples_problem (include/pyscfad_b200.h): one problem of a batch."""
+    _fields_ = ([("nocc", _c_int), ("nvir", _c_int), ("ovvv_packed", _c_int), ("block_size", _c_int),
+                 ("tile_n", _c_int)] +
+                [(k, _vp) for k in ("mo_energy", "t1", "t2", "ovoo", "ovov", "ovvv", "fvo", "e_out",
+                                    "mo_energy_bar", "t1_bar", "t2_bar", "ovoo_bar", "ovov_bar", "ovvv_bar",
+                                    "fvo_bar")])
+
+
 class TriplesError(RuntimeError):
     """A C-ABI entry point returned a non-zero triples_status."""
 
@@ -89,6 +98,17 @@ def load():
     lib.triples_energy_vjp_df.restype = _c_int
     lib.triples_energy_vjp_df.argtypes = ([_vp] + [_c_int] * 4 + [_vp] * 8 + [_c_double, _vp, _c_size, _vp] +
                                           [_vp] * 8)
+    _prob = ctypes.POINTER(Problem)
+    lib.triples_batch_workspace_size.restype = _c_size
+    lib.triples_batch_workspace_size.argtypes = [_c_int, _c_int, _prob]
+    lib.triples_batch_create.restype = _c_int
+    lib.triples_batch_create.argtypes = [_c_int, _c_int, _prob, _c_double, _vp, _c_size, ctypes.POINTER(_vp)]
+    lib.triples_batch_run.restype = _c_int
+    lib.triples_batch_run.argtypes = [_vp, _vp]
+    lib.triples_batch_check_device_status.restype = _c_int
+    lib.triples_batch_check_device_status.argtypes = [_vp, _vp]
+    lib.triples_batch_destroy.restype = None
+    lib.triples_batch_destroy.argtypes = [_vp]
     lib.triples_status_string.restype = ctypes.c_char_p
     lib.triples_status_string.argtypes = [_c_int]
     lib.triples_last_cuda_error.restype = _c_int

@@ -2,19 +2,28 @@
 
 The reference evaluates one molecule per call (pyscfad/cc/ccsd_t.py:28-192);
 a screening or training workload has hundreds of small, differently sized
-problems, each far too small to fill a B200.  ``BatchedTriples``:
+problems, each far too small to fill a B200.  ``BatchedTriples`` runs E(T)
+and its VJP for all of them with one of two engines:
 
-* tunes, per problem shape (nocc, nvir, precision), the chunk block size Tv
-  (which sets the GEMM tile population and the epilogue schedule) and, in
-  the mixed modes, the N tile of the tensor-core W contraction (128 or 256
-  columns) by timing each candidate once and keeping the fastest
-  (``Autotuner``; results are cached per process and can be saved to /
-  loaded from a JSON file);
-* assigns the problems to ``lanes`` CUDA streams (largest first, each to the
-  least-loaded lane), one workspace per lane, so small problems run side by
-  side on the GPU;
-* captures every call of every lane into ONE CUDA graph; ``run()`` replays it
-  with a single launch and no host work per problem.
+* ``engine="batch"`` (default in the mixed modes): the library's batched
+  entry points (``triples_batch_*``).  Each problem keeps its own workspace;
+  chunk step c launches every kernel kind (W contraction, Wbar scale,
+  epilogue, energy sum, the four adjoint contractions) ONCE over the c-th
+  chunk of every problem, the persistent kernels pulling tiles from a job
+  table built when the batch is created.  A batch of 256 small problems is
+  a few hundred launches instead of tens of thousands.
+* ``engine="lanes"``: one ``triples_energy_vjp_ex`` call per problem, spread
+  over ``lanes`` CUDA streams (largest first, each to the least-loaded
+  lane), one workspace per lane.
+
+Either way ``capture()`` records the whole batch as ONE CUDA graph and
+``run()`` replays it with a single launch and no host work per problem.
+``Autotuner`` picks, per problem shape (nocc, nvir, precision), the chunk
+block size Tv and, in the mixed modes, the N tile of the tensor-core W
+contraction (128 or 256 columns) by timing each candidate once (results are
+cached per process and can be saved to / loaded from a JSON file); the batch
+engine uses the tuned N tile with Tv = 16, which keeps the number of chunk
+steps smallest.
 
 Inputs are copied once into device buffers owned by the batch; ``update()``
 refreshes their values in place (same shapes) before the next ``run()``.
@@ -112,11 +121,14 @@ class BatchedTriples:
     """
 
     def __init__(self, problems, precision: str = "mixed", lanes: int = 8, device=None,
-                 autotuner: Autotuner | None = None, tune: bool = True):
+                 autotuner: Autotuner | None = None, tune: bool = True, engine: str | None = None):
         self.device = torch.device(device or "cuda")
         self.precision = precision
         self.lib = _lib.load()
         self.prec = _lib.PRECISION[precision]
+        self.engine = engine or ("batch" if precision != "fp64" else "lanes")
+        if self.engine not in ("batch", "lanes"):
+            raise ValueError(f"unknown engine {self.engine!r}")
         self.problems: list[_Problem] = []
         for p in problems:
             ins = [torch.as_tensor(p[k], dtype=torch.float64).to(self.device).contiguous() for k in KEYS]
@@ -129,9 +141,45 @@ class BatchedTriples:
         self.autotuner = autotuner or Autotuner()
         self._tune(tune)
         self._assign_lanes()
-        self.workspaces = [torch.empty(max(self._ws_bytes(l), 256), dtype=torch.uint8, device=self.device)
-                           for l in range(self.lanes)]
         self.graph = None
+        self.handle = None
+        if self.engine == "batch":
+            for prob in self.problems:
+                prob.tv = 16 if prob.nocc * 16 <= 1024 else 8
+            self._create_batch()
+            self.workspaces = []
+        else:
+            self.workspaces = [torch.empty(max(self._ws_bytes(l), 256), dtype=torch.uint8, device=self.device)
+                               for l in range(self.lanes)]
+
+    def _create_batch(self):
+        n = len(self.problems)
+        arr = (_lib.Problem * n)()
+        for i, prob in enumerate(self.problems):
+            q = arr[i]
+            q.nocc, q.nvir, q.ovvv_packed = prob.nocc, prob.nvir, int(prob.packed)
+            q.block_size, q.tile_n = prob.tv, prob.tile_n
+            for k, a in zip(KEYS, prob.inputs):
+                setattr(q, k, a.data_ptr())
+            q.e_out = prob.energy.data_ptr()
+            for k in KEYS:
+                setattr(q, k + "_bar", prob.grads[k].data_ptr())
+        self._problem_array = arr
+        nbytes = int(self.lib.triples_batch_workspace_size(self.prec, n, arr))
+        if nbytes == 0:
+            raise _lib.TriplesError(1, "triples_batch_workspace_size")
+        self.batch_workspace = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        handle = ctypes.c_void_p()
+        torch.cuda.synchronize(self.device)
+        _lib.check(self.lib.triples_batch_create(self.prec, n, arr, 1.0, self.batch_workspace.data_ptr(), nbytes,
+                                                 ctypes.byref(handle)), "triples_batch_create")
+        self.handle = handle
+
+    def __del__(self):
+        handle = getattr(self, "handle", None)
+        if handle is not None and handle.value:
+            self.lib.triples_batch_destroy(handle)
+            self.handle = None
 
     # -- set-up ---------------------------------------------------------------
     def _size(self, prob: _Problem, tv: int) -> int:
@@ -171,8 +219,12 @@ class BatchedTriples:
         return max([self._size(p, p.tv) for p in self.problems if p.lane == lane] or [0])
 
     def _enqueue(self):
-        """All calls of all lanes on their streams, forked from / joined into the current stream."""
+        """The whole batch on the current stream (batch engine), or all calls of all
+        lanes on their streams, forked from / joined into the current stream."""
         main = torch.cuda.current_stream(self.device)
+        if self.engine == "batch":
+            _lib.check(self.lib.triples_batch_run(self.handle, main.cuda_stream), "triples_batch_run")
+            return
         fork = torch.cuda.Event()
         fork.record(main)
         for lane, st in enumerate(self.streams):
@@ -218,7 +270,11 @@ class BatchedTriples:
         return [(float(p.energy), p.grads) for p in self.problems]
 
     def check(self):
-        """Device-side status of every lane's last call (synchronises)."""
+        """Device-side status of the last run (synchronises)."""
+        if self.engine == "batch":
+            _lib.check(self.lib.triples_batch_check_device_status(
+                self.handle, torch.cuda.current_stream(self.device).cuda_stream), "batched run")
+            return
         for lane, st in enumerate(self.streams):
             _lib.check(self.lib.triples_check_device_status(st.cuda_stream, self.workspaces[lane].data_ptr()),
                        f"batched lane {lane}")

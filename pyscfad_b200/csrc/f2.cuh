@@ -228,8 +228,26 @@ __device__ __forceinline__ T group_reduce_scatter(T (&v)[NV], int lane) {
     return r;
 }
 
-template <typename StageT, int SB>
-__global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4) k_f2t(F2P<StageT> P) {
+// BATCH = false: the CTAs of one launch segment (parameters P0).  BATCH =
+// true: the CTAs of njobs segments (chunks of different problems) numbered job
+// after job (job_start[j] = first CTA of job j), parameters in device memory.
+template <typename StageT, int SB, bool BATCH>
+__global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4)
+    k_f2t(const __grid_constant__ F2P<StageT> P0, const F2P<StageT> *__restrict__ jobs,
+          const int *__restrict__ job_start, int njobs) {
+    int blk = (int)blockIdx.x;
+    const F2P<StageT> *Pp = &P0;
+    if constexpr (BATCH) {
+        int lo = 0, hi = njobs - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (job_start[mid] <= blk) lo = mid;
+            else hi = mid - 1;
+        }
+        blk -= job_start[lo];
+        Pp = &jobs[lo];
+    }
+    const F2P<StageT> &P = *Pp;
     using C = F2Smem<SB>;
     constexpr int NT = C::NT, IPT = C::IPT;
     constexpr int REG = C::REG, NV = C::NV, NVP = C::NVP;
@@ -253,8 +271,8 @@ __global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4) k_f2t(F2P<S
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     // linear grid, sub-range triple fastest: the blocks of one representative
     // run together, so the two 16-byte halves of each Wbar sector meet in L2
-    const int sub = P.sub0 + (int)(blockIdx.x % (unsigned)P.nsub_l);
-    const int rep = P.rep0 + (int)(blockIdx.x / (unsigned)P.nsub_l);
+    const int sub = P.sub0 + (int)((unsigned)blk % (unsigned)P.nsub_l);
+    const int rep = P.rep0 + (int)((unsigned)blk / (unsigned)P.nsub_l);
     const F2Sub &R = P.sub[sub];
     const int ijk[3] = {P.ijk[3 * rep], P.ijk[3 * rep + 1], P.ijk[3 * rep + 2]};
 
@@ -660,7 +678,7 @@ __global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4) k_f2t(F2P<S
 }
 
 // Sum of the per-CTA energy partials of one epilogue launch, in a fixed order.
-__global__ void k_f2_energy_sum(const double *__restrict__ e_part, int n, double *e_acc) {
+__device__ __forceinline__ void energy_sum_body(const double *__restrict__ e_part, int n, double *e_acc) {
     __shared__ double s[256];
     double acc = 0.0;
     for (int b = threadIdx.x; b < n; b += blockDim.x) acc += e_part[b];
@@ -671,6 +689,10 @@ __global__ void k_f2_energy_sum(const double *__restrict__ e_part, int n, double
         __syncthreads();
     }
     if (threadIdx.x == 0) *e_acc += s[0];
+}
+
+__global__ void k_f2_energy_sum(const double *__restrict__ e_part, int n, double *e_acc) {
+    energy_sum_body(e_part, n, e_acc);
 }
 
 }  // namespace tb

@@ -60,10 +60,33 @@ struct TcB1Cfg {
     static_assert(NACC * BN <= 512, "TMEM holds 512 columns");
 };
 
-template <bool A_MN, int BN>
+// BATCH = false: one chunk (parameters P0).  BATCH = true: the tiles of njobs
+// chunks (of different problems, one kind) numbered job after job
+// (job_start[j] = first tile of job j, job_start[njobs] = total), parameters
+// in device memory.
+template <bool A_MN, int BN, bool BATCH>
 __global__ void __launch_bounds__(kB1Threads, 1)
-    k_b1_tc(const __grid_constant__ TcB1Params P) {
+    k_b1_tc(const __grid_constant__ TcB1Params P0, const TcB1Params *__restrict__ jobs,
+            const int *__restrict__ job_start, int njobs) {
     using C = TcB1Cfg<A_MN, BN>;
+    // job of global tile t (BATCH) and the tile's index within it (each role
+    // walks its tiles in increasing order: after the first binary search the
+    // job index only moves forward); parameters are bound with
+    // BATCH ? jobs[j] : P0, the __grid_constant__ parameter in the
+    // single-chunk kernel
+    int jcur = -1;
+    auto job_tile = [&](int t, int &lt) -> int {
+        if constexpr (BATCH) {
+            if (jcur < 0) jcur = job_of(job_start, njobs, t);
+            while (jcur + 1 < njobs && job_start[jcur + 1] <= t) jcur++;
+            lt = t - job_start[jcur];
+            return jcur;
+        } else {
+            lt = t;
+            return 0;
+        }
+    };
+    const TcB1Params &Pfirst = BATCH ? jobs[0] : P0;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint64_t *full = (uint64_t *)(smem + C::STAGES * C::STAGE_BYTES);
@@ -88,10 +111,10 @@ __global__ void __launch_bounds__(kB1Threads, 1)
         mbar_init(drain, 1);
         fence_mbar_init();
     }
-    if (warp == 0 && lane == 0) {
-        for (int t = 0; t < P.nperm; t++) {
-            tma_prefetch_desc(&P.tmA[t]);
-            tma_prefetch_desc(&P.tmB[t]);
+    if (!BATCH && warp == 0 && lane == 0) {
+        for (int t = 0; t < P0.nperm; t++) {
+            tma_prefetch_desc(&P0.tmA[t]);
+            tma_prefetch_desc(&P0.tmB[t]);
         }
     }
     if (warp == 1) {
@@ -103,10 +126,9 @@ __global__ void __launch_bounds__(kB1Threads, 1)
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
     volatile int *abortp = &s_abort;
-    const int total = P.cum[P.nperm];
-    const int o = P.d.o;
-    // tile t -> ordering, batch, M tile, N tile
-    auto decode = [&](int t, int &tau, int &b, int &mt, int &nt) {
+    const int total = BATCH ? job_start[njobs] : P0.cum[P0.nperm];
+    // tile t of the chunk with parameters P -> ordering, batch, M tile, N tile
+    auto decode = [&](const TcB1Params &P, int t, int &tau, int &b, int &mt, int &nt) {
         tau = 0;
         while (tau + 1 < P.nperm && t >= P.cum[tau + 1]) tau++;
         int rem = t - P.cum[tau];
@@ -126,8 +148,11 @@ __global__ void __launch_bounds__(kB1Threads, 1)
         for (int s = 0; s < C::STAGES; s++) pending[s] = false;
         bool ok = true;
         for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+            int lt;
+            const int jb = job_tile(t, lt);
+            const TcB1Params &P = BATCH ? jobs[jb] : P0;
             int tau, b, mt, nt;
-            decode(t, tau, b, mt, nt);
+            decode(P, lt, tau, b, mt, nt);
             const PermBlock &pb = P.pb[tau];
             const int Ty = pb.Ty, Tz = pb.Tz;
             const int nk = P.nk_outer[tau] * P.nk_inner[tau];
@@ -180,7 +205,7 @@ __global__ void __launch_bounds__(kB1Threads, 1)
         }
         if (!ok) {
             *abortp = 1;
-            atomicOr(P.err, 8);
+            atomicOr(Pfirst.err, 8);
             for (int s = 0; s < C::STAGES; s++)
                 if (pending[s]) {
                     for (uint32_t i = 0; i < kSpinLimit && !mbar_try_wait(&full[s], pend_phase[s]); i++) {
@@ -189,14 +214,17 @@ __global__ void __launch_bounds__(kB1Threads, 1)
         }
     } else if (warp == 1 && lane == 0) {
         // ---------------- MMA issuer: one TMEM buffer per K segment ----------------
-        const uint32_t idesc = make_idesc_f16(kTcBM, BN, P.bf16 != 0, A_MN, true);
+        const uint32_t idesc = make_idesc_f16(kTcBM, BN, Pfirst.bf16 != 0, A_MN, true);
         int stage = 0;
         uint32_t phase = 0;
         int seg = 0;   // running segment counter (same sequence as the epilogue)
         bool ok = true;
         for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+            int lt;
+            const int jb = job_tile(t, lt);
+            const TcB1Params &P = BATCH ? jobs[jb] : P0;
             int tau, b, mt, nt;
-            decode(t, tau, b, mt, nt);
+            decode(P, lt, tau, b, mt, nt);
             const int nk = P.nk_outer[tau] * P.nk_inner[tau];
             for (int k0 = 0; k0 < nk && ok; k0 += P.kseg, seg++) {
                 const int acc = seg % C::NACC;
@@ -246,7 +274,7 @@ __global__ void __launch_bounds__(kB1Threads, 1)
         }
         if (!ok) {
             *abortp = 1;
-            atomicOr(P.err, 16);
+            atomicOr(Pfirst.err, 16);
         }
         umma_commit(drain);
         for (uint32_t i = 0; i < kSpinLimit && !mbar_try_wait(drain, 0); i++) {
@@ -257,13 +285,16 @@ __global__ void __launch_bounds__(kB1Threads, 1)
         const int quarter = warp & 3;         // TMEM lane quarter this warp may access
         const int half = (warp - 2) >> 2;     // which half of the columns
         const int row = quarter * 32 + lane;
-        const int v = P.d.v, Kp = P.d.Kp;
-        const double sc = P.sign / ((*P.wscale) * (*P.oscale));
+        const double sc0 = BATCH ? 0.0 : P0.sign / ((*P0.wscale) * (*P0.oscale));   // single chunk: read once
         int seg = 0;
         bool ok = true;
         for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+            int lt;
+            const int jb = job_tile(t, lt);
+            const TcB1Params &P = BATCH ? jobs[jb] : P0;
+            const int o = P.d.o, v = P.d.v, Kp = P.d.Kp;
             int tau, b, mt, nt;
-            decode(t, tau, b, mt, nt);
+            decode(P, lt, tau, b, mt, nt);
             const PermBlock &pb = P.pb[tau];
             const int Tz = pb.Tz;
             const int nk = P.nk_outer[tau] * P.nk_inner[tau];
@@ -279,7 +310,7 @@ __global__ void __launch_bounds__(kB1Threads, 1)
                 if (!mbar_wait(&tfull[accA], (uint32_t)((seg / C::NACC) & 1), abortp) ||
                     (two && !mbar_wait(&tfull[accB], (uint32_t)(((seg + 1) / C::NACC) & 1), abortp))) {
                     *abortp = 1;
-                    atomicOr(P.err, 32);
+                    atomicOr(Pfirst.err, 32);
                     ok = false;
                     break;
                 }
@@ -306,6 +337,7 @@ __global__ void __launch_bounds__(kB1Threads, 1)
                 if (!two) seg -= 1;   // an odd tail used one accumulator
             }
             if (!ok) break;
+            const double sc = BATCH ? P.sign / ((*P.wscale) * (*P.oscale)) : sc0;
             long long roff = -1;
             if (P.kind == 0 || P.kind == 2) {
                 const int p = mt * 8 + row / 16, x = row % 16;

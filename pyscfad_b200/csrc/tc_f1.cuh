@@ -72,12 +72,56 @@ __device__ __forceinline__ F1Tile f1_decode(const TcF1Params &P, int t) {
     return T;
 }
 
-template <int BN>
+// Operand tensor maps of one W contraction (16-bit hi/lo splits).
+struct F1Maps {
+    CUtensorMap a1, b1, a2, b2;
+};
+
+// One problem's chunk in a batched launch: its maps and parameters, in device
+// memory (written before the launch, 64-byte aligned).
+struct alignas(64) F1Job {
+    F1Maps m;
+    TcF1Params P;
+};
+
+// Index j of the job that holds global work index t: start[j] <= t < start[j+1].
+__device__ __forceinline__ int job_of(const int *__restrict__ start, int njobs, int t) {
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (start[mid] <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// BATCH = false: one chunk (maps M0, parameters P0).  BATCH = true: the tiles
+// of njobs chunks (of different problems) numbered job after job
+// (job_start[j] = first tile of job j, job_start[njobs] = total); every tile
+// reads its job's maps and parameters.
+template <int BN, bool BATCH>
 __global__ void __launch_bounds__(kF1Threads, 1)
-    k_f1_tc(const __grid_constant__ CUtensorMap tmA1, const __grid_constant__ CUtensorMap tmB1,
-            const __grid_constant__ CUtensorMap tmA2, const __grid_constant__ CUtensorMap tmB2,
-            const __grid_constant__ TcF1Params P) {
+    k_f1_tc(const __grid_constant__ F1Maps M0, const __grid_constant__ TcF1Params P0,
+            const F1Job *__restrict__ jobs, const int *__restrict__ job_start, int njobs) {
     using C = TcCfg<BN>;
+    // job of global tile t (BATCH) and the tile's index within it
+    // (each role walks its tiles in increasing order: after the first binary
+    // search the job index only moves forward)
+    int jcur = -1;
+    auto job_tile = [&](int t, int &lt) -> int {
+        if constexpr (BATCH) {
+            if (jcur < 0) jcur = job_of(job_start, njobs, t);
+            while (jcur + 1 < njobs && job_start[jcur + 1] <= t) jcur++;
+            lt = t - job_start[jcur];
+            return jcur;
+        } else {
+            lt = t;
+            return 0;
+        }
+    };
+    // the parameters themselves are bound with BATCH ? jobs[j].X : X0, which
+    // folds to the __grid_constant__ parameter in the single-chunk kernel
+    const TcF1Params &Pfirst = BATCH ? jobs[0].P : P0;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     float *sstore = (float *)(smem + C::STAGES * C::STAGE_BYTES);   // 1024-byte aligned boxes
@@ -103,11 +147,11 @@ __global__ void __launch_bounds__(kF1Threads, 1)
         mbar_init(drain, 1);
         fence_mbar_init();
     }
-    if (warp == 0 && lane == 0) {
-        tma_prefetch_desc(&tmA1);
-        tma_prefetch_desc(&tmB1);
-        tma_prefetch_desc(&tmA2);
-        tma_prefetch_desc(&tmB2);
+    if (!BATCH && warp == 0 && lane == 0) {
+        tma_prefetch_desc(&M0.a1);
+        tma_prefetch_desc(&M0.b1);
+        tma_prefetch_desc(&M0.a2);
+        tma_prefetch_desc(&M0.b2);
     }
     if (warp == 1) {
         tmem_alloc(tmem_slot, C::TMEM_COLS);
@@ -118,8 +162,7 @@ __global__ void __launch_bounds__(kF1Threads, 1)
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
     volatile int *abortp = &s_abort;
-    const int total = P.cum[P.ch.nperm];
-    const int nkb = P.nkb1 + P.nkb2;
+    const int total = BATCH ? job_start[njobs] : P0.cum[P0.ch.nperm];
 
     if (warp == 0 && lane == 0) {
         // ---------------- TMA producer ----------------
@@ -130,9 +173,14 @@ __global__ void __launch_bounds__(kF1Threads, 1)
         for (int s = 0; s < C::STAGES; s++) pending[s] = false;
         bool ok = true;
         for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
-            const F1Tile T = f1_decode(P, t);
+            int lt;
+            const int jb = job_tile(t, lt);
+            const TcF1Params &P = BATCH ? jobs[jb].P : P0;
+            const F1Maps &M = BATCH ? jobs[jb].m : M0;
+            const F1Tile T = f1_decode(P, lt);
             const PermBlock &pb = P.ch.pb[T.tau];
             const int yg = pb.Y0 + T.y;
+            const int nkb = P.nkb1 + P.nkb2;
             for (int kb = 0; kb < nkb; kb++) {
                 if (!mbar_wait(&empty[stage], phase ^ 1u, abortp)) {
                     ok = false;
@@ -146,16 +194,16 @@ __global__ void __launch_bounds__(kF1Threads, 1)
                 uint8_t *sBl = sB + C::B_BYTES;
                 if (kb < P.nkb1) {
                     const int f0 = kb * kTcBK;
-                    tma_load_5d(sA, &tmA1, &full[stage], f0, pb.X0, T.mt * 8, yg, 0);
-                    tma_load_5d(sAl, &tmA1, &full[stage], f0, pb.X0, T.mt * 8, yg, 1);
-                    tma_load_5d(sB, &tmB1, &full[stage], f0, pb.Z0, T.nt * C::RT, T.q, 0);
-                    tma_load_5d(sBl, &tmB1, &full[stage], f0, pb.Z0, T.nt * C::RT, T.q, 1);
+                    tma_load_5d(sA, &M.a1, &full[stage], f0, pb.X0, T.mt * 8, yg, 0);
+                    tma_load_5d(sAl, &M.a1, &full[stage], f0, pb.X0, T.mt * 8, yg, 1);
+                    tma_load_5d(sB, &M.b1, &full[stage], f0, pb.Z0, T.nt * C::RT, T.q, 0);
+                    tma_load_5d(sBl, &M.b1, &full[stage], f0, pb.Z0, T.nt * C::RT, T.q, 1);
                 } else {
                     const int m0 = (kb - P.nkb1) * kTcBK;
-                    tma_load_5d(sA, &tmA2, &full[stage], m0, pb.X0, T.mt * 8, T.q, 0);
-                    tma_load_5d(sAl, &tmA2, &full[stage], m0, pb.X0, T.mt * 8, T.q, 1);
-                    tma_load_5d(sB, &tmB2, &full[stage], m0, pb.Z0, T.nt * C::RT, yg, 0);
-                    tma_load_5d(sBl, &tmB2, &full[stage], m0, pb.Z0, T.nt * C::RT, yg, 1);
+                    tma_load_5d(sA, &M.a2, &full[stage], m0, pb.X0, T.mt * 8, T.q, 0);
+                    tma_load_5d(sAl, &M.a2, &full[stage], m0, pb.X0, T.mt * 8, T.q, 1);
+                    tma_load_5d(sB, &M.b2, &full[stage], m0, pb.Z0, T.nt * C::RT, yg, 0);
+                    tma_load_5d(sBl, &M.b2, &full[stage], m0, pb.Z0, T.nt * C::RT, yg, 1);
                 }
                 pending[stage] = true;
                 pend_phase[stage] = phase;
@@ -167,7 +215,7 @@ __global__ void __launch_bounds__(kF1Threads, 1)
         }
         if (!ok) {
             *abortp = 1;
-            atomicOr(P.err, 1);
+            atomicOr(Pfirst.err, 1);
             // let copies already in flight land before the CTA can exit
             for (int s = 0; s < C::STAGES; s++)
                 if (pending[s]) {
@@ -177,12 +225,16 @@ __global__ void __launch_bounds__(kF1Threads, 1)
         }
     } else if (warp == 1 && lane == 0) {
         // ---------------- MMA issuer: one TMEM buffer per K segment ----------------
-        const uint32_t idesc = make_idesc_f16(kTcBM, BN, P.bf16 != 0, false, false);
+        const uint32_t idesc = make_idesc_f16(kTcBM, BN, Pfirst.bf16 != 0, false, false);
         int stage = 0;
         uint32_t phase = 0;
         int seg = 0;
         bool ok = true;
         for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+            int lt;
+            const int jb = job_tile(t, lt);
+            const TcF1Params &P = BATCH ? jobs[jb].P : P0;
+            const int nkb = P.nkb1 + P.nkb2;
             for (int k0 = 0; k0 < nkb && ok; k0 += P.kseg, seg++) {
                 const int acc = seg & 1;
                 const uint32_t accph = (seg >> 1) & 1;
@@ -225,7 +277,7 @@ __global__ void __launch_bounds__(kF1Threads, 1)
         }
         if (!ok) {
             *abortp = 1;
-            atomicOr(P.err, 2);
+            atomicOr(Pfirst.err, 2);
         }
         // all MMAs of this thread complete before TMEM can be released
         umma_commit(drain);
@@ -237,12 +289,23 @@ __global__ void __launch_bounds__(kF1Threads, 1)
         const int quarter = warp & 3;
         const int half = (warp - 2) >> 2;
         const int row = quarter * 32 + lane;
-        const int o = P.d.o;
-        const float sc = *P.out_scale;
         float wmax = 0.f;
+        unsigned *wmax_dst = Pfirst.wmax_bits;   // running max |W| goes to the tile's problem
+        const float sc0 = BATCH ? 0.f : *P0.out_scale;   // single chunk: read once
         int seg = 0;
         bool ok = true;
         for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+            int lt;
+            const int jb = job_tile(t, lt);
+            const TcF1Params &P = BATCH ? jobs[jb].P : P0;
+            const int o = P.d.o;
+            const int nkb = P.nkb1 + P.nkb2;
+            if (BATCH && P.wmax_bits != wmax_dst) {
+                for (int off = 16; off > 0; off >>= 1) wmax = fmaxf(wmax, __shfl_xor_sync(0xffffffffu, wmax, off));
+                if (lane == 0 && wmax > 0.f) atomicMax(wmax_dst, __float_as_uint(wmax));
+                wmax = 0.f;
+                wmax_dst = P.wmax_bits;
+            }
             float accf[HC];
 #pragma unroll
             for (int j = 0; j < HC; j++) accf[j] = 0.f;
@@ -251,7 +314,7 @@ __global__ void __launch_bounds__(kF1Threads, 1)
                 const uint32_t accph = (seg >> 1) & 1;
                 if (!mbar_wait(&tfull[acc], accph, abortp)) {
                     *abortp = 1;
-                    atomicOr(P.err, 4);
+                    atomicOr(Pfirst.err, 4);
                     ok = false;
                     break;
                 }
@@ -270,7 +333,8 @@ __global__ void __launch_bounds__(kF1Threads, 1)
                 if (lane == 0) mbar_arrive(&tempty[acc]);
             }
             if (!ok) break;
-            const F1Tile T = f1_decode(P, t);
+            const float sc = BATCH ? *P.out_scale : sc0;
+            const F1Tile T = f1_decode(P, lt);
             const PermBlock &pb = P.ch.pb[T.tau];
             const int p = T.mt * 8 + row / 16;
             const int x = row % 16;
@@ -344,7 +408,7 @@ __global__ void __launch_bounds__(kF1Threads, 1)
         }
         if (lane == 0) bulk_wait0();   // this warp's stores complete before the CTA retires
         for (int off = 16; off > 0; off >>= 1) wmax = fmaxf(wmax, __shfl_xor_sync(0xffffffffu, wmax, off));
-        if (lane == 0 && wmax > 0.f) atomicMax(P.wmax_bits, __float_as_uint(wmax));
+        if (lane == 0 && wmax > 0.f) atomicMax(wmax_dst, __float_as_uint(wmax));
     }
     tc_fence_before();
     __syncthreads();

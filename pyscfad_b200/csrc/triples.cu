@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <new>
 #include <vector>
 
 #include "common.cuh"
@@ -407,8 +408,9 @@ __global__ void k_make_scales(Ctrl *ctrl, int scaled) {
 // pass over Wbar:  |Wbar| <= 2|ybar| (144 max|w| + 36 max|v|) / min|D| over the
 // chunk (|Z| <= 12 max|X|, |X| <= 6 max|w| + 3 max|v|, |R WW| <= 72 max|w|,
 // orbit weight <= 2).  Resets the running max |w| for the next chunk.
-__global__ void k_chunk_scale(Ctrl *ctrl, const double *__restrict__ mo_e, int o, int a0, int na, int b0,
-                              int nb, int c0, int nc, double ybar, int scaled, int lno) {
+__device__ __forceinline__ void chunk_scale_body(Ctrl *ctrl, const double *__restrict__ mo_e, int o, int a0,
+                                                 int na, int b0, int nb, int c0, int nc, double ybar, int scaled,
+                                                 int lno) {
     __shared__ double s_min[3], s_maxo;
     const double inf = 1e300;
     if (threadIdx.x < 4) {
@@ -437,6 +439,33 @@ __global__ void k_chunk_scale(Ctrl *ctrl, const double *__restrict__ mo_e, int o
         ctrl->wscale = scaled ? pow2_scale(bound) : 1.0;
         ctrl->wmax_bits = 0u;
     }
+}
+
+__global__ void k_chunk_scale(Ctrl *ctrl, const double *__restrict__ mo_e, int o, int a0, int na, int b0,
+                              int nb, int c0, int nc, double ybar, int scaled, int lno) {
+    chunk_scale_body(ctrl, mo_e, o, a0, na, b0, nb, c0, nc, ybar, scaled, lno);
+}
+
+// Per problem of a batched chunk step: the chunk's virtual ranges for the
+// Wbar scale, and the energy partials of its epilogue.
+struct ChunkAux {
+    Ctrl *ctrl;
+    const double *mo_e;
+    const double *e_part;
+    double ybar;
+    int o, a0, na, b0, nb, c0, nc, n_part;
+};
+
+// one 32-thread block per problem
+__global__ void k_chunk_scale_batch(const ChunkAux *__restrict__ aux, int scaled) {
+    const ChunkAux &A = aux[blockIdx.x];
+    chunk_scale_body(A.ctrl, A.mo_e, A.o, A.a0, A.na, A.b0, A.nb, A.c0, A.nc, A.ybar, scaled, 0);
+}
+
+// one 256-thread block per problem: the chunk's energy partials, fixed order
+__global__ void k_energy_sum_batch(const ChunkAux *__restrict__ aux) {
+    const ChunkAux &A = aux[blockIdx.x];
+    energy_sum_body(A.e_part, A.n_part, &A.ctrl->e_acc);
 }
 
 template <typename H>
@@ -1080,28 +1109,244 @@ static int lno_chunk(const Plan &P, const ChunkDesc &ch, cudaStream_t st, const 
     return TRIPLES_OK;
 }
 
+// ---------------------------------------------------------------------------
+// one-time device set-up and the mixed-precision kernel parameters of a call
+// and of one chunk, shared by the single-problem and the batched drivers
+// ---------------------------------------------------------------------------
 template <typename StageT>
-static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
-    constexpr int kSB = sizeof(StageT) == 4 ? 8 : 4;   // epilogue sub-block edge
-    {
-        // once per device and element type: shared-memory opt-in and the
-        // constant tables of the epilogue's region patterns
-        const int rc = once_per_device(sizeof(StageT) == 4 ? INIT_F2_F32 : INIT_F2_F64, [&]() -> int {
-            TB_CUDA(cudaFuncSetAttribute(k_f2t<StageT, kSB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)f2_smem_bytes<StageT, kSB>()));
-            if (sizeof(StageT) == 4) {
-                TB_CUDA(cudaFuncSetAttribute(k_f2p<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)F2pSmem::BYTES));
-                TB_CUDA(cudaFuncSetAttribute(k_f2p<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)F2pSmem::BYTES));
-            }
-            F2Pattern pats[kF2Patterns];
-            f2_build_patterns(pats);
-            TB_CUDA(cudaMemcpyToSymbol(c_f2pat, pats, sizeof(pats)));
-            return TRIPLES_OK;
-        });
-        if (rc != TRIPLES_OK) return rc;
+static int setup_epilogue() {
+    constexpr int kSB = sizeof(StageT) == 4 ? 8 : 4;
+    // once per device and element type: shared-memory opt-in and the
+    // constant tables of the epilogue's region patterns
+    return once_per_device(sizeof(StageT) == 4 ? INIT_F2_F32 : INIT_F2_F64, [&]() -> int {
+        TB_CUDA(cudaFuncSetAttribute(k_f2t<StageT, kSB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)f2_smem_bytes<StageT, kSB>()));
+        TB_CUDA(cudaFuncSetAttribute(k_f2t<StageT, kSB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)f2_smem_bytes<StageT, kSB>()));
+        if (sizeof(StageT) == 4) {
+            TB_CUDA(cudaFuncSetAttribute(k_f2p<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F2pSmem::BYTES));
+            TB_CUDA(cudaFuncSetAttribute(k_f2p<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F2pSmem::BYTES));
+        }
+        F2Pattern pats[kF2Patterns];
+        f2_build_patterns(pats);
+        TB_CUDA(cudaMemcpyToSymbol(c_f2pat, pats, sizeof(pats)));
+        return TRIPLES_OK;
+    });
+}
+
+static int setup_tensor_cores() {
+    return once_per_device(INIT_TC, [&]() -> int {
+        TB_CUDA(cudaFuncSetAttribute(k_f1_tc<256, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcCfg<256>::SMEM));
+        TB_CUDA(cudaFuncSetAttribute(k_f1_tc<128, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcCfg<128>::SMEM));
+        TB_CUDA(cudaFuncSetAttribute(k_f1_tc<256, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcCfg<256>::SMEM));
+        TB_CUDA(cudaFuncSetAttribute(k_f1_tc<128, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcCfg<128>::SMEM));
+        TB_CUDA(cudaFuncSetAttribute(k_b1_tc<false, 128, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     TcB1Cfg<false, 128>::SMEM));
+        TB_CUDA(cudaFuncSetAttribute(k_b1_tc<false, 128, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     TcB1Cfg<false, 128>::SMEM));
+        TB_CUDA(cudaFuncSetAttribute(k_b1_tc<true, 128, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     TcB1Cfg<true, 128>::SMEM));
+        TB_CUDA(cudaFuncSetAttribute(k_b1_tc<true, 128, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     TcB1Cfg<true, 128>::SMEM));
+        TB_CUDA(cudaFuncSetAttribute(k_b1_tc<false, 64, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     TcB1Cfg<false, 64>::SMEM));
+        TB_CUDA(cudaFuncSetAttribute(k_b1_tc<false, 64, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     TcB1Cfg<false, 64>::SMEM));
+        TB_CUDA(cudaFuncSetAttribute(k_b1_tc<true, 64, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     TcB1Cfg<true, 64>::SMEM));
+        TB_CUDA(cudaFuncSetAttribute(k_b1_tc<true, 64, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     TcB1Cfg<true, 64>::SMEM));
+        return TRIPLES_OK;
+    });
+}
+
+// Tensor maps over one call's 16-bit operands (built on the host).
+struct OperandMaps {
+    CUtensorMap tmA1, tmB1, tmA2, tmB2;             // W contraction, K-major boxes
+    CUtensorMap tmA1m, tmA2m, tmB1z[5], tmB2z[5];   // adjoint contractions, MN-major boxes
+};
+
+// The W contraction's N tile is BN = 16 * RT columns (RT occupied r values x
+// 16 z), P.f1_bn.
+static int build_operand_maps(const Plan &P, char *ws, OperandMaps &M) {
+    const uint64_t o = P.d.o, v = P.d.v;
+    const bool bf16 = P.prec == TRIPLES_PRECISION_MIXED_BF16;
+    const uint64_t dA1[5] = {(uint64_t)P.Kp8, v, o, v, 2};
+    const uint32_t bA[5] = {64, 16, 8, 1, 1};
+    const uint64_t dB1[5] = {(uint64_t)P.Kp8, v, o, o, 2};
+    const uint32_t bB[5] = {64, 16, (uint32_t)(P.f1_bn / 16), 1, 1};
+    const uint64_t dA2[5] = {(uint64_t)P.Op8, v, o, o, 2};
+    const uint64_t dB2[5] = {(uint64_t)P.Op8, v, o, v, 2};
+    int rc;
+    if ((rc = make_tmap5(&M.tmA1, ws + P.off_A1h, bf16, dA1, bA)) != TRIPLES_OK) return rc;
+    if ((rc = make_tmap5(&M.tmB1, ws + P.off_B1h, bf16, dB1, bB)) != TRIPLES_OK) return rc;
+    if ((rc = make_tmap5(&M.tmA2, ws + P.off_A2h, bf16, dA2, bA)) != TRIPLES_OK) return rc;
+    if ((rc = make_tmap5(&M.tmB2, ws + P.off_B2h, bf16, dB2, bB)) != TRIPLES_OK) return rc;
+    if (P.want_grad) {
+        const uint64_t dA1mn[5] = {(uint64_t)P.Kp8, v, o, v, 2};
+        const uint64_t dA2mn[5] = {(uint64_t)P.Op8, v, o, o, 2};
+        const uint64_t dB1mn[5] = {(uint64_t)P.Kp8, v, o, o, 2};
+        const uint64_t dB2mn[5] = {(uint64_t)P.Op8, v, o, v, 2};
+        const uint32_t bX[5] = {64, 16, 4, 1, 1};
+        if ((rc = make_tmap5(&M.tmA1m, ws + P.off_A1h, bf16, dA1mn, bX)) != TRIPLES_OK) return rc;
+        if ((rc = make_tmap5(&M.tmA2m, ws + P.off_A2h, bf16, dA2mn, bX)) != TRIPLES_OK) return rc;
+        for (int lt = 0; lt < 5; lt++) {
+            const uint32_t tz = 1u << lt;
+            const uint32_t bZ[5] = {64, tz, 64 / tz, 1, 1};
+            if ((rc = make_tmap5(&M.tmB1z[lt], ws + P.off_B1h, bf16, dB1mn, bZ)) != TRIPLES_OK) return rc;
+            if ((rc = make_tmap5(&M.tmB2z[lt], ws + P.off_B2h, bf16, dB2mn, bZ)) != TRIPLES_OK) return rc;
+        }
     }
+    return TRIPLES_OK;
+}
+
+// W-contraction parameters of one chunk (tiles ordering by ordering).
+static int f1_params(const Plan &P, const ChunkDesc &ch, char *ws, TcF1Params &T) {
+    const Dims &d = P.d;
+    Ctrl *ctrl = (Ctrl *)(ws + P.off_ctrl);
+    float *S = (float *)(ws + P.off_S);
+    T.d = d;
+    T.ch = ch;
+    T.mt_count = (d.o + 7) / 8;
+    const int rt = P.f1_bn / 16;
+    T.nt_count = (d.o + rt - 1) / rt;
+    T.cum[0] = 0;
+    for (int t = 0; t < ch.nperm; t++) T.cum[t + 1] = T.cum[t] + ch.pb[t].Ty * d.o * T.mt_count * T.nt_count;
+    T.nkb1 = (P.Kp8 + kTcBK - 1) / kTcBK;
+    T.nkb2 = (P.Op8 + kTcBK - 1) / kTcBK;
+    T.S = S;
+    T.out_scale = &ctrl->out_scale;
+    T.wmax_bits = &ctrl->wmax_bits;
+    T.err = &ctrl->err;
+    T.bf16 = P.prec == TRIPLES_PRECISION_MIXED_BF16 ? 1 : 0;
+    T.kseg = P.kseg;
+    for (int t = 0; t < 6; t++) T.tmS_ok[t] = 0;
+    for (int t = 0; t < ch.nperm; t++) {
+        const PermBlock &pb = ch.pb[t];
+        if (pb.Tx == 16 && pb.Tz == 16 && d.o >= 2) {
+            const int trc = make_tmap_stage(&T.tmS[t], S + pb.soff, d.o, pb.Tx, pb.Ty);
+            if (trc != TRIPLES_OK) return trc;
+            T.tmS_ok[t] = 1;
+        }
+    }
+    return TRIPLES_OK;
+}
+
+// Epilogue parameters of one chunk: every sub-range triple, those of three
+// distinct full 8-wide sub-ranges first (mixed precision; the persistent
+// kernel k_f2p takes them with the all-distinct occupied representatives).
+// Returns the number of those leading sub-range triples.
+template <typename StageT>
+static int f2_params(const Plan &P, const ChunkDesc &ch, char *ws, const TriplesIO &io, F2P<StageT> &F) {
+    constexpr int kSB = sizeof(StageT) == 4 ? 8 : 4;
+    const bool mixed = P.prec != TRIPLES_PRECISION_FP64;
+    Ctrl *ctrl = (Ctrl *)(ws + P.off_ctrl);
+    F.d = P.d;
+    F.ch = ch;
+    F.nsub = 0;
+    int nsb[3];
+    for (int t = 0; t < 3; t++) nsb[t] = (ch.nabc[t] + kSB - 1) / kSB;
+    F2Sub rest[kMaxSub];
+    int nrest = 0;
+    for (int sa = 0; sa < nsb[0]; sa++)
+        for (int sb = 0; sb < nsb[1]; sb++) {
+            if (ch.blk[0] == ch.blk[1] && sb > sa) continue;
+            for (int sc = 0; sc < nsb[2]; sc++) {
+                if (ch.blk[1] == ch.blk[2] && sc > sb) continue;
+                F2Sub u;
+                const int si[3] = {sa, sb, sc};
+                for (int t = 0; t < 3; t++) {
+                    u.st[t] = ch.base[t] + si[t] * kSB;
+                    int len = ch.nabc[t] - si[t] * kSB;
+                    u.len[t] = len < kSB ? len : kSB;
+                }
+                const bool simple = mixed && u.len[0] == 8 && u.len[1] == 8 && u.len[2] == 8 &&
+                                    u.st[0] != u.st[1] && u.st[1] != u.st[2] && u.st[0] != u.st[2];
+                if (simple) F.sub[F.nsub++] = u;
+                else rest[nrest++] = u;
+            }
+        }
+    const int n_simple_sub = F.nsub;
+    for (int t = 0; t < nrest; t++) F.sub[F.nsub++] = rest[t];
+    F.ijk = (int *)(ws + P.off_ijk);
+    F.mo_e = io.mo_energy; F.t1 = io.t1; F.t2 = io.t2; F.ovov = io.ovov; F.fvo = io.fvo;
+    F.S = (StageT *)(ws + P.off_S);
+    F.SW = P.want_grad ? (void *)(ws + P.off_SW) : nullptr;
+    F.split = mixed ? (P.prec == TRIPLES_PRECISION_MIXED_BF16 ? 2 : 1) : 0;
+    F.wscale = &ctrl->wscale;
+    F.ybar = io.ybar;
+    F.want_grad = P.want_grad;
+    F.e_part = (double *)(ws + P.off_epart);
+    F.n_ijk = P.n_ijk;
+    F.mo_bar = io.mo_energy_bar;
+    F.t1_bar = io.t1_bar; F.fvo_bar = io.fvo_bar; F.ovov_bar = io.ovov_bar; F.t2_bar = io.t2_bar;
+    F.rep0 = 0;
+    F.sub0 = 0;
+    F.nsub_l = F.nsub;
+    return n_simple_sub;
+}
+
+// Adjoint-contraction parameters of one chunk and kind (0: ovvv_bar, 1: t2_bar
+// ovvv term, 2: ovoo_bar, 3: t2_bar ooov term), tiles ordering by ordering.
+static int b1_params(const Plan &P, const ChunkDesc &ch, char *ws, const OperandMaps &M, int kind, TcB1Params &B) {
+    const Dims &d = P.d;
+    const uint64_t o = d.o;
+    const bool bf16 = P.prec == TRIPLES_PRECISION_MIXED_BF16;
+    Ctrl *ctrl = (Ctrl *)(ws + P.off_ctrl);
+    char *SW = ws + P.off_SW;
+    const uint32_t bK[5] = {64, 1, 16, 8, 1};   // Wbar K-major (kinds 0, 2)
+    const uint32_t bM[5] = {64, 1, 16, 4, 1};   // Wbar MN-major (kinds 1, 3)
+    B.d = d;
+    B.nperm = ch.nperm;
+    for (int t = 0; t < ch.nperm; t++) B.pb[t] = ch.pb[t];
+    B.wscale = &ctrl->wscale;
+    B.err = &ctrl->err;
+    B.bf16 = bf16 ? 1 : 0;
+    B.kseg = P.kseg;
+    B.kind = kind;
+    B.ntile_n = kind <= 1 ? (d.v + 127) / 128 : (d.o + 63) / 64;
+    B.G = (double *)(ws + (kind == 0 ? P.off_GA1 : kind == 1 ? P.off_GB1 : kind == 2 ? P.off_GA2 : P.off_GB2));
+    B.oscale = &ctrl->scale[(kind == 0 || kind == 2) ? 1 : 0];
+    B.sign = kind == 2 ? -1.0 : 1.0;
+    for (int t = 0; t < ch.nperm; t++) {
+        const PermBlock &pb = ch.pb[t];
+        const uint64_t dW[5] = {(uint64_t)pb.rzp, o, (uint64_t)pb.Tx, o, (uint64_t)(2 * pb.Ty)};
+        const int rc = make_tmap5(&B.tmA[t], SW + 2 * pb.swoff * 2, bf16, dW, (kind == 0 || kind == 2) ? bK : bM);
+        if (rc != TRIPLES_OK) return rc;
+        int lz = 0;
+        while ((1 << lz) < pb.Tz) lz++;
+        switch (kind) {
+        case 0:
+            B.tmB[t] = M.tmB1z[lz];
+            B.nbatch[t] = pb.Ty; B.ntile_m[t] = (d.o + 7) / 8;
+            B.nk_outer[t] = d.o; B.nk_inner[t] = (d.o * pb.Tz + 63) / 64;
+            break;
+        case 1:
+            B.tmB[t] = M.tmA1m;
+            B.nbatch[t] = d.o; B.ntile_m[t] = (d.o * pb.Tz + 127) / 128;
+            B.nk_outer[t] = pb.Ty; B.nk_inner[t] = (d.o + 3) / 4;
+            break;
+        case 2:
+            B.tmB[t] = M.tmB2z[lz];
+            B.nbatch[t] = d.o; B.ntile_m[t] = (d.o + 7) / 8;
+            B.nk_outer[t] = pb.Ty; B.nk_inner[t] = (d.o * pb.Tz + 63) / 64;
+            break;
+        default:
+            B.tmB[t] = M.tmA2m;
+            B.nbatch[t] = pb.Ty; B.ntile_m[t] = (d.o * pb.Tz + 127) / 128;
+            B.nk_outer[t] = d.o; B.nk_inner[t] = (d.o + 3) / 4;
+            break;
+        }
+    }
+    B.cum[0] = 0;
+    for (int t = 0; t < ch.nperm; t++) B.cum[t + 1] = B.cum[t] + B.nbatch[t] * B.ntile_m[t] * B.ntile_n;
+    return TRIPLES_OK;
+}
+
+// Per-call preparation: control block, occupied table, zeroed gradients, and
+// the operand layouts (FP64 copies, or 16-bit splits with their scales).
+template <typename StageT>
+static int prep_launches(const Plan &P, cudaStream_t st, const TriplesIO &io) {
     const Dims d = P.d;
     const bool mixed = P.prec != TRIPLES_PRECISION_FP64;
     const bool bf16 = P.prec == TRIPLES_PRECISION_MIXED_BF16;
@@ -1111,14 +1356,12 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
     double *B1 = (double *)(ws + P.off_B1);
     double *A2 = (double *)(ws + P.off_A2);
     double *B2 = (double *)(ws + P.off_B2);
-    StageT *S = (StageT *)(ws + P.off_S);
     void *SW = P.want_grad ? (void *)(ws + P.off_SW) : nullptr;
     double *GA1 = P.want_grad ? (double *)(ws + P.off_GA1) : nullptr;
     double *GB1 = P.want_grad ? (double *)(ws + P.off_GB1) : nullptr;
     double *GA2 = P.want_grad ? (double *)(ws + P.off_GA2) : nullptr;
     double *GB2 = P.want_grad ? (double *)(ws + P.off_GB2) : nullptr;
     int *ijk = (int *)(ws + P.off_ijk);
-    double *e_part = (double *)(ws + P.off_epart);
     const size_t o = d.o, v = d.v, n = d.n;
 
     TB_CUDA(cudaMemsetAsync(ctrl, 0, kCtrlBytes, st));
@@ -1148,16 +1391,7 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
         TB_KLAUNCH(P_PREP, k_prep_B2<<<grid1d((long long)v * o * v * o, 256), 256, 0, st>>>(io.t2, d, B2));
     }
 
-    // 16-bit split operands and tensor maps (tensor-core path).  The W
-    // contraction's N tile is BN = 16 * RT columns (RT occupied r values x 16 z):
-    // 256 unless 128 covers nocc with fewer padded r values (nocc % 16 in
-    // 1..8, e.g. nocc = 40: three 16-r tiles hold 48 r, five 8-r tiles 40).
-    const int f1_bn = P.f1_bn;
-    CUtensorMap tmA1, tmB1, tmA2, tmB2, tmA1m, tmA2m, tmB1z[5], tmB2z[5];
-    const uint64_t dA1mn[5] = {(uint64_t)P.Kp8, v, o, v, 2};
-    const uint64_t dA2mn[5] = {(uint64_t)P.Op8, v, o, o, 2};
-    const uint64_t dB1mn[5] = {(uint64_t)P.Kp8, v, o, o, 2};
-    const uint64_t dB2mn[5] = {(uint64_t)P.Op8, v, o, v, 2};
+    // 16-bit split operands (tensor-core path)
     if (mixed) {
         const long long npair = (long long)v * (v + 1) / 2;
         TB_KLAUNCH(P_PREP, k_absmax<<<grid1d((long long)o * v * (P.packed ? npair : (long long)v * v), 256), 256, 0, st>>>(
@@ -1190,47 +1424,67 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                 io.t2, d, P.Op8, ctrl, (__half *)(ws + P.off_B2h)));
         }
         TB_LAUNCH_CHECK();
-        {
-            const uint64_t dA1[5] = {(uint64_t)P.Kp8, v, o, v, 2};
-            const uint32_t bA[5] = {64, 16, 8, 1, 1};
-            const uint64_t dB1[5] = {(uint64_t)P.Kp8, v, o, o, 2};
-            const uint32_t bB[5] = {64, 16, (uint32_t)(f1_bn / 16), 1, 1};
-            const uint64_t dA2[5] = {(uint64_t)P.Op8, v, o, o, 2};
-            const uint64_t dB2[5] = {(uint64_t)P.Op8, v, o, v, 2};
-            int rc;
-            if ((rc = make_tmap5(&tmA1, ws + P.off_A1h, bf16, dA1, bA)) != TRIPLES_OK) return rc;
-            if ((rc = make_tmap5(&tmB1, ws + P.off_B1h, bf16, dB1, bB)) != TRIPLES_OK) return rc;
-            if ((rc = make_tmap5(&tmA2, ws + P.off_A2h, bf16, dA2, bA)) != TRIPLES_OK) return rc;
-            if ((rc = make_tmap5(&tmB2, ws + P.off_B2h, bf16, dB2, bB)) != TRIPLES_OK) return rc;
+        if (P.want_grad) TB_CUDA(cudaMemsetAsync(SW, 0, P.wbar_elems * 4, st));
+    }
+    return TRIPLES_OK;
+
+}
+
+// Gradients back to the reference layouts, and the energy out.
+static int fold_launches(const Plan &P, cudaStream_t st, const TriplesIO &io) {
+    const Dims d = P.d;
+    char *ws = (char *)io.workspace;
+    Ctrl *ctrl = (Ctrl *)(ws + P.off_ctrl);
+    const double *GA1 = (const double *)(ws + P.off_GA1), *GB1 = (const double *)(ws + P.off_GB1);
+    const double *GA2 = (const double *)(ws + P.off_GA2), *GB2 = (const double *)(ws + P.off_GB2);
+    const size_t o = d.o, v = d.v;
+    if (P.want_grad) {
+        if (P.packed) {
+            TB_KLAUNCH(P_FOLD, k_fold_ovvv_packed<<<grid1d((long long)o * v * (v * (v + 1) / 2), 256), 256, 0, st>>>(
+                GA1, d, io.ovvv_bar));
+        } else {
+            TB_KLAUNCH(P_FOLD, k_fold_ovvv_full<<<dim3((d.v + 31) / 32, (d.v + 31) / 32, (unsigned)(o * v)), dim3(32, 8), 0, st>>>(
+                GA1, d, io.ovvv_bar));
         }
-        if (P.want_grad) {
-            // second operands of the adjoint contractions (MN-major boxes)
-            const uint32_t bX[5] = {64, 16, 4, 1, 1};
-            int rc;
-            if ((rc = make_tmap5(&tmA1m, ws + P.off_A1h, bf16, dA1mn, bX)) != TRIPLES_OK) return rc;
-            if ((rc = make_tmap5(&tmA2m, ws + P.off_A2h, bf16, dA2mn, bX)) != TRIPLES_OK) return rc;
-            for (int lt = 0; lt < 5; lt++) {
-                const uint32_t tz = 1u << lt;
-                const uint32_t bZ[5] = {64, tz, 64 / tz, 1, 1};
-                if ((rc = make_tmap5(&tmB1z[lt], ws + P.off_B1h, bf16, dB1mn, bZ)) != TRIPLES_OK) return rc;
-                if ((rc = make_tmap5(&tmB2z[lt], ws + P.off_B2h, bf16, dB2mn, bZ)) != TRIPLES_OK) return rc;
-            }
-            TB_CUDA(cudaMemsetAsync(SW, 0, P.wbar_elems * 4, st));
-        }
-        const int arc = once_per_device(INIT_TC, [&]() -> int {
-            TB_CUDA(cudaFuncSetAttribute(k_f1_tc<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcCfg<256>::SMEM));
-            TB_CUDA(cudaFuncSetAttribute(k_f1_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcCfg<128>::SMEM));
-            TB_CUDA(cudaFuncSetAttribute(k_b1_tc<false, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         TcB1Cfg<false, 128>::SMEM));
-            TB_CUDA(cudaFuncSetAttribute(k_b1_tc<true, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         TcB1Cfg<true, 128>::SMEM));
-            TB_CUDA(cudaFuncSetAttribute(k_b1_tc<false, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         TcB1Cfg<false, 64>::SMEM));
-            TB_CUDA(cudaFuncSetAttribute(k_b1_tc<true, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         TcB1Cfg<true, 64>::SMEM));
-            return TRIPLES_OK;
-        });
-        if (arc != TRIPLES_OK) return arc;
+        TB_LAUNCH_CHECK();
+        TB_KLAUNCH(P_FOLD, k_fold_t2<<<grid1d((long long)o * o * v * v, 256), 256, 0, st>>>(GB1, GB2, d, io.t2_bar));
+        TB_KLAUNCH(P_FOLD, k_fold_ovoo<<<grid1d((long long)o * v * o * o, 256), 256, 0, st>>>(GA2, d, io.ovoo_bar));
+    }
+    TB_KLAUNCH(P_FOLD, k_copy_scalar<<<1, 1, 0, st>>>(&ctrl->e_acc, io.e_out));
+    return TRIPLES_OK;
+}
+
+template <typename StageT>
+static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
+    constexpr int kSB = sizeof(StageT) == 4 ? 8 : 4;   // epilogue sub-block edge
+    {
+        const int rc = setup_epilogue<StageT>();
+        if (rc != TRIPLES_OK) return rc;
+    }
+    int prc = prep_launches<StageT>(P, st, io);
+    if (prc != TRIPLES_OK) return prc;
+    const Dims d = P.d;
+    const bool mixed = P.prec != TRIPLES_PRECISION_FP64;
+    const bool bf16 = P.prec == TRIPLES_PRECISION_MIXED_BF16;
+    char *ws = (char *)io.workspace;
+    Ctrl *ctrl = (Ctrl *)(ws + P.off_ctrl);
+    double *A1 = (double *)(ws + P.off_A1);
+    double *B1 = (double *)(ws + P.off_B1);
+    double *A2 = (double *)(ws + P.off_A2);
+    double *B2 = (double *)(ws + P.off_B2);
+    StageT *S = (StageT *)(ws + P.off_S);
+    void *SW = P.want_grad ? (void *)(ws + P.off_SW) : nullptr;
+    double *GA1 = P.want_grad ? (double *)(ws + P.off_GA1) : nullptr;
+    double *GB1 = P.want_grad ? (double *)(ws + P.off_GB1) : nullptr;
+    double *GA2 = P.want_grad ? (double *)(ws + P.off_GA2) : nullptr;
+    double *GB2 = P.want_grad ? (double *)(ws + P.off_GB2) : nullptr;
+    int *ijk = (int *)(ws + P.off_ijk);
+    double *e_part = (double *)(ws + P.off_epart);
+    const int f1_bn = P.f1_bn;
+    OperandMaps M;
+    if (mixed) {
+        if ((prc = build_operand_maps(P, ws, M)) != TRIPLES_OK) return prc;
+        if ((prc = setup_tensor_cores()) != TRIPLES_OK) return prc;
     }
 
     for (int A = 0; A < P.nb; A++) {
@@ -1247,37 +1501,17 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                 // F1: raw amplitudes
                 if (mixed) {
                     TcF1Params T;
-                    T.d = d;
-                    T.ch = ch;
-                    T.mt_count = (d.o + 7) / 8;
-                    const int rt = f1_bn / 16;
-                    T.nt_count = (d.o + rt - 1) / rt;
-                    T.cum[0] = 0;
-                    for (int t = 0; t < ch.nperm; t++)
-                        T.cum[t + 1] = T.cum[t] + ch.pb[t].Ty * d.o * T.mt_count * T.nt_count;
-                    T.nkb1 = (P.Kp8 + kTcBK - 1) / kTcBK;
-                    T.nkb2 = (P.Op8 + kTcBK - 1) / kTcBK;
-                    T.S = (float *)S;
-                    T.out_scale = &ctrl->out_scale;
-                    T.wmax_bits = &ctrl->wmax_bits;
-                    T.err = &ctrl->err;
-                    T.bf16 = bf16 ? 1 : 0;
-                    T.kseg = P.kseg;
-                    for (int t = 0; t < 6; t++) T.tmS_ok[t] = 0;
-                    for (int t = 0; t < ch.nperm; t++) {
-                        const PermBlock &pb = ch.pb[t];
-                        if (pb.Tx == 16 && pb.Tz == 16 && d.o >= 2) {
-                            const int trc = make_tmap_stage(&T.tmS[t], (float *)S + pb.soff, d.o, pb.Tx, pb.Ty);
-                            if (trc != TRIPLES_OK) return trc;
-                            T.tmS_ok[t] = 1;
-                        }
-                    }
+                    const int frc = f1_params(P, ch, ws, T);
+                    if (frc != TRIPLES_OK) return frc;
                     const int tiles = T.cum[ch.nperm];
                     const int grid = tiles < num_sms() ? tiles : num_sms();
+                    const F1Maps Mf1{M.tmA1, M.tmB1, M.tmA2, M.tmB2};
                     if (f1_bn == 128)
-                        TB_KLAUNCH(P_F1, k_f1_tc<128><<<grid, kF1Threads, TcCfg<128>::SMEM, st>>>(tmA1, tmB1, tmA2, tmB2, T));
+                        TB_KLAUNCH(P_F1, (k_f1_tc<128, false><<<grid, kF1Threads, TcCfg<128>::SMEM, st>>>(
+                                             Mf1, T, nullptr, nullptr, 0)));
                     else
-                        TB_KLAUNCH(P_F1, k_f1_tc<256><<<grid, kF1Threads, TcCfg<256>::SMEM, st>>>(tmA1, tmB1, tmA2, tmB2, T));
+                        TB_KLAUNCH(P_F1, (k_f1_tc<256, false><<<grid, kF1Threads, TcCfg<256>::SMEM, st>>>(
+                                             Mf1, T, nullptr, nullptr, 0)));
                 } else {
                     GemmLaunch<double> L;
                     L.d = d;
@@ -1302,57 +1536,20 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                     // n_distinct_ijk of the table) they go to the persistent kernel k_f2p
                     // in the mixed modes, every other CTA to k_f2t.
                     F2P<StageT> F;
-                    F.d = d;
-                    F.ch = ch;
-                    F.nsub = 0;
-                    int nsb[3];
-                    for (int t = 0; t < 3; t++) nsb[t] = (ch.nabc[t] + kSB - 1) / kSB;
-                    F2Sub rest[kMaxSub];
-                    int nrest = 0;
-                    for (int sa = 0; sa < nsb[0]; sa++)
-                        for (int sb = 0; sb < nsb[1]; sb++) {
-                            if (ch.blk[0] == ch.blk[1] && sb > sa) continue;
-                            for (int sc = 0; sc < nsb[2]; sc++) {
-                                if (ch.blk[1] == ch.blk[2] && sc > sb) continue;
-                                F2Sub u;
-                                const int si[3] = {sa, sb, sc};
-                                for (int t = 0; t < 3; t++) {
-                                    u.st[t] = ch.base[t] + si[t] * kSB;
-                                    int len = ch.nabc[t] - si[t] * kSB;
-                                    u.len[t] = len < kSB ? len : kSB;
-                                }
-                                const bool simple = mixed && u.len[0] == 8 && u.len[1] == 8 && u.len[2] == 8 &&
-                                                    u.st[0] != u.st[1] && u.st[1] != u.st[2] && u.st[0] != u.st[2];
-                                if (simple) F.sub[F.nsub++] = u;
-                                else rest[nrest++] = u;
-                            }
-                        }
-                    const int n_simple_sub = F.nsub;
-                    for (int t = 0; t < nrest; t++) F.sub[F.nsub++] = rest[t];
-                    F.ijk = ijk;
-                    F.mo_e = io.mo_energy; F.t1 = io.t1; F.t2 = io.t2; F.ovov = io.ovov; F.fvo = io.fvo;
-                    F.S = S;
-                    F.SW = SW;
-                    F.split = mixed ? (bf16 ? 2 : 1) : 0;
+                    const int n_simple_sub = f2_params<StageT>(P, ch, ws, io, F);
                     if (mixed && P.want_grad)
                         TB_KLAUNCH(P_PREP, k_chunk_scale<<<1, 32, 0, st>>>(ctrl, io.mo_energy, d.o, ch.base[0], ch.nabc[0],
                                                                            ch.base[1], ch.nabc[1], ch.base[2], ch.nabc[2],
                                                                            io.ybar, bf16 ? 0 : 1, 0));
-                    F.wscale = &ctrl->wscale;
-                    F.ybar = io.ybar;
-                    F.want_grad = P.want_grad;
-                    F.e_part = e_part;
-                    F.n_ijk = P.n_ijk;
-                    F.mo_bar = io.mo_energy_bar;
-                    F.t1_bar = io.t1_bar; F.fvo_bar = io.fvo_bar; F.ovov_bar = io.ovov_bar; F.t2_bar = io.t2_bar;
                     const int nd = mixed ? n_distinct_ijk(d.o) : 0;
                     auto f2t = [&](int rep0, int nrep, int sub0, int nsub_l) -> int {
                         if (nrep <= 0 || nsub_l <= 0) return TRIPLES_OK;
                         F.rep0 = rep0;
                         F.sub0 = sub0;
                         F.nsub_l = nsub_l;
-                        TB_KLAUNCH(P_F2, (k_f2t<StageT, kSB><<<(unsigned)(nrep * nsub_l), F2Smem<kSB>::NT,
-                                                               f2_smem_bytes<StageT, kSB>(), st>>>(F)));
+                        TB_KLAUNCH(P_F2, (k_f2t<StageT, kSB, false><<<(unsigned)(nrep * nsub_l), F2Smem<kSB>::NT,
+                                                                      f2_smem_bytes<StageT, kSB>(), st>>>(
+                                             F, nullptr, nullptr, 0)));
                         return TRIPLES_OK;
                     };
                     if (nd > 0 && n_simple_sub > 0) {
@@ -1377,76 +1574,36 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                 // W-term gradients
                 if (mixed) {
                     // one launch per kind over all orderings of the chunk
-                    const uint32_t bK[5] = {64, 1, 16, 8, 1};
-                    const uint32_t bM[5] = {64, 1, 16, 4, 1};
-                    CUtensorMap wk[6], wm[6];
-                    int lzs[6];
-                    for (int t = 0; t < ch.nperm; t++) {
-                        const PermBlock &pb = ch.pb[t];
-                        const uint64_t dW[5] = {(uint64_t)pb.rzp, o, (uint64_t)pb.Tx, o, (uint64_t)(2 * pb.Ty)};
-                        void *wbase = (char *)SW + 2 * pb.swoff * 2;
-                        int rc;
-                        if ((rc = make_tmap5(&wk[t], wbase, bf16, dW, bK)) != TRIPLES_OK) return rc;
-                        if ((rc = make_tmap5(&wm[t], wbase, bf16, dW, bM)) != TRIPLES_OK) return rc;
-                        lzs[t] = 0;
-                        while ((1 << lzs[t]) < pb.Tz) lzs[t]++;
-                    }
-                    const int nsm = num_sms();
                     TcB1Params B;
-                    B.d = d;
-                    B.nperm = ch.nperm;
-                    for (int t = 0; t < ch.nperm; t++) B.pb[t] = ch.pb[t];
-                    B.wscale = &ctrl->wscale;
-                    B.err = &ctrl->err;
-                    B.bf16 = bf16 ? 1 : 0;
-                    B.kseg = P.kseg;
-                    auto grid_of = [&]() {
-                        B.cum[0] = 0;
-                        for (int t = 0; t < ch.nperm; t++)
-                            B.cum[t + 1] = B.cum[t] + B.nbatch[t] * B.ntile_m[t] * B.ntile_n;
+                    auto launch_b1 = [&](int kind) -> int {
+                        const int brc = b1_params(P, ch, ws, M, kind, B);
+                        if (brc != TRIPLES_OK) return brc;
                         const int tiles = B.cum[ch.nperm];
-                        return tiles < nsm ? tiles : nsm;
+                        const int grid = tiles < num_sms() ? tiles : num_sms();
+                        switch (kind) {
+                        case 0:
+                            TB_KLAUNCH(P_B1A, (k_b1_tc<false, 128, false><<<grid, kB1Threads, TcB1Cfg<false, 128>::SMEM, st>>>(
+                                                  B, nullptr, nullptr, 0)));
+                            break;
+                        case 1:
+                            TB_KLAUNCH(P_B1B, (k_b1_tc<true, 128, false><<<grid, kB1Threads, TcB1Cfg<true, 128>::SMEM, st>>>(
+                                                  B, nullptr, nullptr, 0)));
+                            break;
+                        case 2:
+                            TB_KLAUNCH(P_B1C, (k_b1_tc<false, 64, false><<<grid, kB1Threads, TcB1Cfg<false, 64>::SMEM, st>>>(
+                                                  B, nullptr, nullptr, 0)));
+                            break;
+                        default:
+                            TB_KLAUNCH(P_B1D, (k_b1_tc<true, 64, false><<<grid, kB1Threads, TcB1Cfg<true, 64>::SMEM, st>>>(
+                                                  B, nullptr, nullptr, 0)));
+                            break;
+                        }
+                        return TRIPLES_OK;
                     };
-                    // ovvv gradient
-                    B.kind = 0; B.ntile_n = (d.v + 127) / 128;
-                    B.G = GA1; B.oscale = &ctrl->scale[1]; B.sign = 1.0;
-                    for (int t = 0; t < ch.nperm; t++) {
-                        const PermBlock &pb = ch.pb[t];
-                        B.tmA[t] = wk[t]; B.tmB[t] = tmB1z[lzs[t]];
-                        B.nbatch[t] = pb.Ty; B.ntile_m[t] = (d.o + 7) / 8;
-                        B.nk_outer[t] = d.o; B.nk_inner[t] = (d.o * pb.Tz + 63) / 64;
+                    for (int kind = 0; kind < 4; kind++) {
+                        const int brc = launch_b1(kind);
+                        if (brc != TRIPLES_OK) return brc;
                     }
-                    TB_KLAUNCH(P_B1A, (k_b1_tc<false, 128><<<grid_of(), kB1Threads, TcB1Cfg<false, 128>::SMEM, st>>>(B)));
-                    // t2 gradient, ovvv term
-                    B.kind = 1; B.ntile_n = (d.v + 127) / 128;
-                    B.G = GB1; B.oscale = &ctrl->scale[0]; B.sign = 1.0;
-                    for (int t = 0; t < ch.nperm; t++) {
-                        const PermBlock &pb = ch.pb[t];
-                        B.tmA[t] = wm[t]; B.tmB[t] = tmA1m;
-                        B.nbatch[t] = d.o; B.ntile_m[t] = (d.o * pb.Tz + 127) / 128;
-                        B.nk_outer[t] = pb.Ty; B.nk_inner[t] = (d.o + 3) / 4;
-                    }
-                    TB_KLAUNCH(P_B1B, (k_b1_tc<true, 128><<<grid_of(), kB1Threads, TcB1Cfg<true, 128>::SMEM, st>>>(B)));
-                    // ovoo gradient
-                    B.kind = 2; B.ntile_n = (d.o + 63) / 64;
-                    B.G = GA2; B.oscale = &ctrl->scale[1]; B.sign = -1.0;
-                    for (int t = 0; t < ch.nperm; t++) {
-                        const PermBlock &pb = ch.pb[t];
-                        B.tmA[t] = wk[t]; B.tmB[t] = tmB2z[lzs[t]];
-                        B.nbatch[t] = d.o; B.ntile_m[t] = (d.o + 7) / 8;
-                        B.nk_outer[t] = pb.Ty; B.nk_inner[t] = (d.o * pb.Tz + 63) / 64;
-                    }
-                    TB_KLAUNCH(P_B1C, (k_b1_tc<false, 64><<<grid_of(), kB1Threads, TcB1Cfg<false, 64>::SMEM, st>>>(B)));
-                    // t2 gradient, ooov term
-                    B.kind = 3; B.ntile_n = (d.o + 63) / 64;
-                    B.G = GB2; B.oscale = &ctrl->scale[0]; B.sign = 1.0;
-                    for (int t = 0; t < ch.nperm; t++) {
-                        const PermBlock &pb = ch.pb[t];
-                        B.tmA[t] = wm[t]; B.tmB[t] = tmA2m;
-                        B.nbatch[t] = pb.Ty; B.ntile_m[t] = (d.o * pb.Tz + 127) / 128;
-                        B.nk_outer[t] = d.o; B.nk_inner[t] = (d.o + 3) / 4;
-                    }
-                    TB_KLAUNCH(P_B1D, (k_b1_tc<true, 64><<<grid_of(), kB1Threads, TcB1Cfg<true, 64>::SMEM, st>>>(B)));
                 } else {
                 GemmLaunch<StageT> L;
                 L.d = d;
@@ -1473,25 +1630,251 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
             }
     }
 
-    if (P.want_grad) {
-        if (P.packed) {
-            TB_KLAUNCH(P_FOLD, k_fold_ovvv_packed<<<grid1d((long long)o * v * (v * (v + 1) / 2), 256), 256, 0, st>>>(
-                GA1, d, io.ovvv_bar));
-        } else {
-            TB_KLAUNCH(P_FOLD, k_fold_ovvv_full<<<dim3((d.v + 31) / 32, (d.v + 31) / 32, (unsigned)(o * v)), dim3(32, 8), 0, st>>>(
-                GA1, d, io.ovvv_bar));
-        }
-        TB_LAUNCH_CHECK();
-        TB_KLAUNCH(P_FOLD, k_fold_t2<<<grid1d((long long)o * o * v * v, 256), 256, 0, st>>>(GB1, GB2, d, io.t2_bar));
-        TB_KLAUNCH(P_FOLD, k_fold_ovoo<<<grid1d((long long)o * v * o * o, 256), 256, 0, st>>>(GA2, d, io.ovoo_bar));
-    }
-    TB_KLAUNCH(P_FOLD, k_copy_scalar<<<1, 1, 0, st>>>(&ctrl->e_acc, io.e_out));
-    return TRIPLES_OK;
+    return fold_launches(P, st, io);
 }
 
 int run_triples(const Plan &P, cudaStream_t st, const TriplesIO &io) {
     if (P.prec == TRIPLES_PRECISION_FP64) return run_impl<double>(P, st, io);
     return run_impl<float>(P, st, io);
+}
+
+// ---------------------------------------------------------------------------
+// batched calls: many problems of uneven size.  Every problem keeps its own
+// workspace (operands, one chunk's staging, gradient accumulators); chunk
+// step c launches each kernel kind ONCE over the c-th chunk of every problem
+// that has one (tiles / CTAs numbered problem after problem, parameters in
+// job tables built on the host when the batch is created and stored after
+// the problems' workspaces).  Mixed precision only; an FP64 batch runs the
+// problems one after another.
+// ---------------------------------------------------------------------------
+struct BatchStep {
+    size_t f1_jobs[2], f1_start[2];   // [0]: W-contraction N tile 256, [1]: 128
+    int f1_n[2], f1_tiles[2];
+    size_t aux;                       // ChunkAux per problem of the step
+    int naux;
+    size_t f2_jobs, f2_start;
+    int f2_ctas;
+    size_t b1_jobs[4], b1_start[4];   // per adjoint kind
+    int b1_tiles[4];
+};
+
+struct Batch {
+    int prec = 0, nprob = 0;
+    char *ws = nullptr;
+    std::vector<Plan> plans;
+    std::vector<TriplesIO> ios;
+    std::vector<size_t> ws_off;
+    std::vector<BatchStep> steps;
+    size_t tables_off = 0, total = 0;
+};
+
+static void batch_chunks(const Plan &P, std::vector<ChunkDesc> &out) {
+    out.clear();
+    for (int A = 0; A < P.nb; A++)
+        for (int B = 0; B <= A; B++)
+            for (int C = 0; C <= B; C++) {
+                ChunkDesc ch;
+                make_chunk(P.d, A, B, C, ch);
+                out.push_back(ch);
+            }
+}
+
+// Plans, workspace offsets and (with image != nullptr) the job tables of a
+// batch; B.ws must then be the device workspace the tables point into.
+static int batch_build(Batch &B, int prec, int nprob, const triples_problem *probs, double ybar,
+                       std::vector<char> *image) {
+    if (nprob < 1 || !probs) return TRIPLES_ERR_INVALID_ARGUMENT;
+    B.prec = prec;
+    B.nprob = nprob;
+    B.plans.assign(nprob, Plan{});
+    B.ios.assign(nprob, TriplesIO{});
+    B.ws_off.assign(nprob, 0);
+    size_t off = 0;
+    for (int p = 0; p < nprob; p++) {
+        const triples_problem &q = probs[p];
+        triples_options opt{};
+        opt.block_size = q.block_size;
+        opt.tile_n = q.tile_n;
+        const int rc = make_plan(prec, q.nocc, q.nvir, q.ovvv_packed, 1, B.plans[p], 0, &opt);
+        if (rc != TRIPLES_OK) return rc;
+        B.ws_off[p] = off;
+        off = align256(off + B.plans[p].total);
+        TriplesIO &io = B.ios[p];
+        io.mo_energy = q.mo_energy; io.t1 = q.t1; io.t2 = q.t2; io.ovoo = q.ovoo; io.ovov = q.ovov;
+        io.ovvv = q.ovvv; io.fvo = q.fvo; io.ybar = ybar; io.e_out = q.e_out;
+        io.mo_energy_bar = q.mo_energy_bar; io.t1_bar = q.t1_bar; io.t2_bar = q.t2_bar; io.ovoo_bar = q.ovoo_bar;
+        io.ovov_bar = q.ovov_bar; io.ovvv_bar = q.ovvv_bar; io.fvo_bar = q.fvo_bar;
+        io.workspace = B.ws ? B.ws + B.ws_off[p] : nullptr;
+        if (image && (!io.mo_energy || !io.t1 || !io.t2 || !io.ovoo || !io.ovov || !io.ovvv || !io.fvo || !io.e_out ||
+                      !io.mo_energy_bar || !io.t1_bar || !io.t2_bar || !io.ovoo_bar || !io.ovov_bar ||
+                      !io.ovvv_bar || !io.fvo_bar))
+            return TRIPLES_ERR_INVALID_ARGUMENT;
+    }
+    B.tables_off = off;
+    B.steps.clear();
+    if (prec == TRIPLES_PRECISION_FP64) {
+        B.total = off;
+        return TRIPLES_OK;
+    }
+    std::vector<std::vector<ChunkDesc>> chunks(nprob);
+    std::vector<OperandMaps> maps(image ? nprob : 0);
+    size_t nsteps = 0;
+    for (int p = 0; p < nprob; p++) {
+        batch_chunks(B.plans[p], chunks[p]);
+        if (chunks[p].size() > nsteps) nsteps = chunks[p].size();
+        if (image) {
+            const int rc = build_operand_maps(B.plans[p], B.ws + B.ws_off[p], maps[p]);
+            if (rc != TRIPLES_OK) return rc;
+        }
+    }
+    // table layout: per step, 256-byte aligned arrays
+    size_t t = 0;
+    auto take = [&](size_t bytes) {
+        const size_t at = t;
+        t = align256(t + bytes);
+        return at;
+    };
+    B.steps.resize(nsteps);
+    for (size_t c = 0; c < nsteps; c++) {
+        BatchStep &S = B.steps[c];
+        std::vector<int> who, who_bn[2];
+        for (int p = 0; p < nprob; p++)
+            if (c < chunks[p].size()) {
+                who.push_back(p);
+                who_bn[B.plans[p].f1_bn == 256 ? 0 : 1].push_back(p);
+            }
+        const int n = (int)who.size();
+        for (int g = 0; g < 2; g++) {
+            S.f1_n[g] = (int)who_bn[g].size();
+            S.f1_jobs[g] = take(sizeof(F1Job) * S.f1_n[g]);
+            S.f1_start[g] = take(sizeof(int) * (S.f1_n[g] + 1));
+        }
+        S.naux = n;
+        S.aux = take(sizeof(ChunkAux) * n);
+        S.f2_jobs = take(sizeof(F2P<float>) * n);
+        S.f2_start = take(sizeof(int) * (n + 1));
+        for (int k = 0; k < 4; k++) {
+            S.b1_jobs[k] = take(sizeof(TcB1Params) * n);
+            S.b1_start[k] = take(sizeof(int) * (n + 1));
+        }
+        if (!image) continue;
+        if (image->size() < t) image->resize(t);
+        char *img = image->data();
+        for (int g = 0; g < 2; g++) {
+            int *start = (int *)(img + S.f1_start[g]);
+            start[0] = 0;
+            for (int j = 0; j < S.f1_n[g]; j++) {
+                const int p = who_bn[g][j];
+                F1Job job;
+                std::memset(&job, 0, sizeof(job));
+                const OperandMaps &M = maps[p];
+                job.m = F1Maps{M.tmA1, M.tmB1, M.tmA2, M.tmB2};
+                const int rc = f1_params(B.plans[p], chunks[p][c], B.ws + B.ws_off[p], job.P);
+                if (rc != TRIPLES_OK) return rc;
+                std::memcpy(img + S.f1_jobs[g] + sizeof(F1Job) * j, &job, sizeof(job));
+                start[j + 1] = start[j] + job.P.cum[job.P.ch.nperm];
+            }
+            S.f1_tiles[g] = start[S.f1_n[g]];
+        }
+        int *f2s = (int *)(img + S.f2_start);
+        f2s[0] = 0;
+        int *b1s[4];
+        for (int k = 0; k < 4; k++) {
+            b1s[k] = (int *)(img + S.b1_start[k]);
+            b1s[k][0] = 0;
+        }
+        for (int j = 0; j < n; j++) {
+            const int p = who[j];
+            const Plan &P = B.plans[p];
+            const ChunkDesc &ch = chunks[p][c];
+            char *wsp = B.ws + B.ws_off[p];
+            F2P<float> F;
+            std::memset(&F, 0, sizeof(F));
+            f2_params<float>(P, ch, wsp, B.ios[p], F);   // one segment: every representative, every sub-range triple
+            std::memcpy(img + S.f2_jobs + sizeof(F) * j, &F, sizeof(F));
+            f2s[j + 1] = f2s[j] + P.n_ijk * F.nsub;
+            ChunkAux A;
+            std::memset(&A, 0, sizeof(A));
+            A.ctrl = (Ctrl *)(wsp + P.off_ctrl);
+            A.mo_e = B.ios[p].mo_energy;
+            A.e_part = (const double *)(wsp + P.off_epart);
+            A.ybar = ybar;
+            A.o = P.d.o;
+            A.a0 = ch.base[0]; A.na = ch.nabc[0];
+            A.b0 = ch.base[1]; A.nb = ch.nabc[1];
+            A.c0 = ch.base[2]; A.nc = ch.nabc[2];
+            A.n_part = P.n_ijk * F.nsub;
+            std::memcpy(img + S.aux + sizeof(A) * j, &A, sizeof(A));
+            for (int k = 0; k < 4; k++) {
+                TcB1Params Bp;
+                std::memset(&Bp, 0, sizeof(Bp));
+                const int rc = b1_params(P, ch, wsp, maps[p], k, Bp);
+                if (rc != TRIPLES_OK) return rc;
+                std::memcpy(img + S.b1_jobs[k] + sizeof(Bp) * j, &Bp, sizeof(Bp));
+                b1s[k][j + 1] = b1s[k][j] + Bp.cum[ch.nperm];
+            }
+        }
+        S.f2_ctas = f2s[n];
+        for (int k = 0; k < 4; k++) S.b1_tiles[k] = b1s[k][n];
+    }
+    if (image) image->resize(t);
+    B.total = B.tables_off + t;
+    return TRIPLES_OK;
+}
+
+static int run_batch(const Batch &B, cudaStream_t st) {
+    if (B.prec == TRIPLES_PRECISION_FP64) {
+        for (int p = 0; p < B.nprob; p++) {
+            const int rc = run_impl<double>(B.plans[p], st, B.ios[p]);
+            if (rc != TRIPLES_OK) return rc;
+        }
+        return TRIPLES_OK;
+    }
+    int rc;
+    if ((rc = setup_epilogue<float>()) != TRIPLES_OK) return rc;
+    if ((rc = setup_tensor_cores()) != TRIPLES_OK) return rc;
+    for (int p = 0; p < B.nprob; p++)
+        if ((rc = prep_launches<float>(B.plans[p], st, B.ios[p])) != TRIPLES_OK) return rc;
+    const char *tab = B.ws + B.tables_off;
+    const int nsm = num_sms();
+    const int scaled = B.prec == TRIPLES_PRECISION_MIXED_BF16 ? 0 : 1;
+    const F1Maps M0{};
+    const TcF1Params T0{};
+    const TcB1Params B0{};
+    const F2P<float> F0{};
+    auto cap = [&](int n) { return n < nsm ? n : nsm; };
+    for (const BatchStep &S : B.steps) {
+        const F1Job *f1j[2] = {(const F1Job *)(tab + S.f1_jobs[0]), (const F1Job *)(tab + S.f1_jobs[1])};
+        const int *f1s[2] = {(const int *)(tab + S.f1_start[0]), (const int *)(tab + S.f1_start[1])};
+        if (S.f1_n[0] > 0)
+            TB_KLAUNCH(P_F1, (k_f1_tc<256, true><<<cap(S.f1_tiles[0]), kF1Threads, TcCfg<256>::SMEM, st>>>(
+                                 M0, T0, f1j[0], f1s[0], S.f1_n[0])));
+        if (S.f1_n[1] > 0)
+            TB_KLAUNCH(P_F1, (k_f1_tc<128, true><<<cap(S.f1_tiles[1]), kF1Threads, TcCfg<128>::SMEM, st>>>(
+                                 M0, T0, f1j[1], f1s[1], S.f1_n[1])));
+        const ChunkAux *aux = (const ChunkAux *)(tab + S.aux);
+        TB_KLAUNCH(P_PREP, k_chunk_scale_batch<<<S.naux, 32, 0, st>>>(aux, scaled));
+        TB_KLAUNCH(P_F2, (k_f2t<float, 8, true><<<S.f2_ctas, F2Smem<8>::NT, f2_smem_bytes<float, 8>(), st>>>(
+                             F0, (const F2P<float> *)(tab + S.f2_jobs), (const int *)(tab + S.f2_start), S.naux)));
+        TB_KLAUNCH(P_F2, k_energy_sum_batch<<<S.naux, 256, 0, st>>>(aux));
+        const TcB1Params *bj[4];
+        const int *bs[4];
+        for (int k = 0; k < 4; k++) {
+            bj[k] = (const TcB1Params *)(tab + S.b1_jobs[k]);
+            bs[k] = (const int *)(tab + S.b1_start[k]);
+        }
+        TB_KLAUNCH(P_B1A, (k_b1_tc<false, 128, true><<<cap(S.b1_tiles[0]), kB1Threads, TcB1Cfg<false, 128>::SMEM, st>>>(
+                              B0, bj[0], bs[0], S.naux)));
+        TB_KLAUNCH(P_B1B, (k_b1_tc<true, 128, true><<<cap(S.b1_tiles[1]), kB1Threads, TcB1Cfg<true, 128>::SMEM, st>>>(
+                              B0, bj[1], bs[1], S.naux)));
+        TB_KLAUNCH(P_B1C, (k_b1_tc<false, 64, true><<<cap(S.b1_tiles[2]), kB1Threads, TcB1Cfg<false, 64>::SMEM, st>>>(
+                              B0, bj[2], bs[2], S.naux)));
+        TB_KLAUNCH(P_B1D, (k_b1_tc<true, 64, true><<<cap(S.b1_tiles[3]), kB1Threads, TcB1Cfg<true, 64>::SMEM, st>>>(
+                              B0, bj[3], bs[3], S.naux)));
+    }
+    for (int p = 0; p < B.nprob; p++)
+        if ((rc = fold_launches(B.plans[p], st, B.ios[p])) != TRIPLES_OK) return rc;
+    return TRIPLES_OK;
 }
 
 void profile_enable(int on) {
@@ -1839,6 +2222,67 @@ int triples_check_device_status(void *stream, const void *workspace) {
     }
     return c.err ? TRIPLES_ERR_DEVICE_TIMEOUT : TRIPLES_OK;
 }
+
+// ---- batched calls ----
+struct triples_batch {
+    tb::Batch b;
+};
+
+size_t triples_batch_workspace_size(int precision, int nprob, const triples_problem *probs) {
+    tb::Batch B;
+    if (tb::batch_build(B, precision, nprob, probs, 1.0, nullptr) != TRIPLES_OK) return 0;
+    return B.total;
+}
+
+int triples_batch_create(int precision, int nprob, const triples_problem *probs, double ybar, void *workspace,
+                         size_t workspace_bytes, triples_batch **batch) {
+    if (!batch) return TRIPLES_ERR_INVALID_ARGUMENT;
+    *batch = nullptr;
+    if (!workspace) return TRIPLES_ERR_WORKSPACE;
+    {
+        // the workspace must hold the batch before any table points into it
+        tb::Batch sizing;
+        const int rc = tb::batch_build(sizing, precision, nprob, probs, ybar, nullptr);
+        if (rc != TRIPLES_OK) return rc;
+        if (workspace_bytes < sizing.total) return TRIPLES_ERR_WORKSPACE;
+    }
+    triples_batch *h = new (std::nothrow) triples_batch;
+    if (!h) return TRIPLES_ERR_INVALID_ARGUMENT;
+    h->b.ws = (char *)workspace;
+    std::vector<char> image;
+    int rc = tb::batch_build(h->b, precision, nprob, probs, ybar, &image);
+    if (rc == TRIPLES_OK && !image.empty()) {
+        const cudaError_t e = cudaMemcpy(h->b.ws + h->b.tables_off, image.data(), image.size(), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            tb::set_last_cuda_error((int)e);
+            rc = TRIPLES_ERR_CUDA;
+        }
+    }
+    if (rc != TRIPLES_OK) {
+        delete h;
+        return rc;
+    }
+    *batch = h;
+    return TRIPLES_OK;
+}
+
+int triples_batch_run(triples_batch *batch, void *stream) {
+    if (!batch) return TRIPLES_ERR_INVALID_ARGUMENT;
+    return tb::run_batch(batch->b, (cudaStream_t)stream);
+}
+
+int triples_batch_check_device_status(triples_batch *batch, void *stream) {
+    if (!batch) return TRIPLES_ERR_INVALID_ARGUMENT;
+    int status = TRIPLES_OK;
+    for (int p = 0; p < batch->b.nprob; p++) {
+        const int rc = triples_check_device_status(stream, batch->b.ws + batch->b.ws_off[p]);
+        if (rc == TRIPLES_ERR_CUDA) return rc;
+        if (rc != TRIPLES_OK) status = rc;
+    }
+    return status;
+}
+
+void triples_batch_destroy(triples_batch *batch) { delete batch; }
 
 const char *triples_status_string(int status) {
     switch (status) {

@@ -132,3 +132,38 @@ def test_options_are_per_call_and_validated():
     rc = lib.triples_energy_vjp_ex(null, 0, 5, 19, 1, *([null] * 7), 1.0, 0, None, ctypes.c_void_p(256),
                                    1 << 30, ctypes.c_void_p(256), *([null] * 7))
     assert rc == 1
+
+
+def _batch_problems(shapes):
+    arr = (_lib.Problem * len(shapes))()
+    for i, (o, v) in enumerate(shapes):
+        arr[i].nocc, arr[i].nvir, arr[i].ovvv_packed = o, v, 1
+    return arr
+
+
+def test_batch_workspace_covers_every_problem_and_the_job_tables():
+    lib = _lib.load()
+    shapes = [(4, 20), (6, 27), (5, 33), (12, 80)]
+    arr = _batch_problems(shapes)
+    for prec in (0, 1, 2):
+        total = lib.triples_batch_workspace_size(prec, len(shapes), arr)
+        singles = sum(lib.triples_workspace_size(prec, o, v, 1, 1) for o, v in shapes)
+        assert total >= singles
+        if prec > 0:   # mixed modes add the job tables of the chunk steps
+            assert total > singles
+    assert lib.triples_batch_workspace_size(1, 0, arr) == 0                 # no problems
+    bad = _batch_problems([(0, 20)])
+    assert lib.triples_batch_workspace_size(1, 1, bad) == 0                 # nocc < 1
+    assert lib.triples_batch_workspace_size(7, len(shapes), arr) == 0       # bad precision
+
+
+def test_batch_create_rejects_bad_arguments_before_any_cuda_call():
+    lib = _lib.load()
+    arr = _batch_problems([(4, 20)])
+    handle = ctypes.c_void_p()
+    assert lib.triples_batch_create(1, 1, arr, 1.0, None, 0, ctypes.byref(handle)) == 2     # no workspace
+    assert lib.triples_batch_create(1, 1, arr, 1.0, ctypes.c_void_p(256), 8, ctypes.byref(handle)) == 2  # too small
+    assert lib.triples_batch_create(1, 1, arr, 1.0, ctypes.c_void_p(256), 1 << 40, None) == 1      # no handle slot
+    assert handle.value is None
+    assert lib.triples_batch_run(None, None) == 1
+    lib.triples_batch_destroy(None)

@@ -776,6 +776,11 @@ def main():
         dom = max(classes, key=lambda k: prof[k][0])
         roof = dict(classes[dom])
         roof["traffic"] = traffic_tab.get(dom)
+        bpa = traffic_tab.get(dom + "_bytes_per_amplitude")
+        if roof["traffic"] is None and bpa is not None:
+            # measured DRAM bytes per raw amplitude (ncu, smaller chunk) x this step's amplitudes, per launch
+            roof["traffic"] = bpa * elem * n_steps / roof["launches"]
+            roof["traffic_note"] = "%.1f DRAM bytes per raw amplitude (ncu) scaled to this launch" % bpa
         roof["peak_note"] = hnote if roof["bound"] == "hbm" else tnote
         roof["classes"] = {k: {kk: (round(vv, 4) if isinstance(vv, float) else vv) for kk, vv in c.items()
                                if kk in ("bound", "achieved", "frac", "frac_emulated", "share")}

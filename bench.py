@@ -348,7 +348,8 @@ def run_accuracy(args, o, v, naux):
         t1 = torch.cuda.Event(enable_timing=True)
         t0.record(stream)
         e, g = triples.energy_vjp(*xs, ybar=1.0, precision=prec, device=dev, block_size=tv,
-                                  chunk_range=(a0 * s, a1 * s))
+                                  chunk_range=(a0 * s, a1 * s),
+                                  accumulation_segment=0 if prec == "fp64" else args.accumulation_segment)
         t1.record(stream)
         torch.cuda.synchronize()
         out = float(e), g, t0.elapsed_time(t1) / 1e3
@@ -373,6 +374,7 @@ def run_accuracy(args, o, v, naux):
         return float((a - b).abs().max() / max(float(b.abs().max()), 1e-300))
 
     out = {"workload": args.workload, "nocc": o, "nvir": v, "naux": naux, "scale": args.scale,
+           "accumulation_segment": args.accumulation_segment,
            "e_fp64": e64, "fp64_seconds": t64, "fp64_block": tv64, "mixed_block": tvm or 16}
     if args.slice:
         frac = triples.chunk_fraction(v, a0, a1)
@@ -567,6 +569,8 @@ def main():
                          "timed in both precisions (FP64 vs mixed on identical work)")
     ap.add_argument("--fp64-block", type=int, default=16, choices=[4, 8, 16],
                     help="with --accuracy: virtual block size of the FP64 run (8 or 4 shrink its FP64 staging)")
+    ap.add_argument("--accumulation-segment", type=int, default=0,
+                    help="mixed precision: 64-wide K blocks per FP32 tensor-core accumulation segment (0: library default)")
     ap.add_argument("--mixed-block", type=int, default=16, choices=[4, 8, 16],
                     help="with --accuracy: virtual block size of the mixed-precision runs")
     ap.add_argument("--no-bf16", action="store_true", help="with --accuracy: skip the bf16 mode")
@@ -632,7 +636,8 @@ def main():
             dist.barrier()
 
     def step():
-        e, g = triples.energy_vjp(*dev_args, ybar=1.0, precision=args.precision, device=dev, check=False)
+        e, g = triples.energy_vjp(*dev_args, ybar=1.0, precision=args.precision, device=dev, check=False,
+                                  accumulation_segment=args.accumulation_segment)
         return e, g
 
     # first warm-up step (one-time set-up included) sizes the plan; every rank
@@ -715,7 +720,8 @@ def main():
         e0.record()
         for _ in range(n_e2e):
             dev_in = [a.to(dev, non_blocking=True) for a in host_in]
-            ee, gg = triples.energy_vjp(*dev_in, ybar=1.0, precision=args.precision, device=dev, check=False)
+            ee, gg = triples.energy_vjp(*dev_in, ybar=1.0, precision=args.precision, device=dev, check=False,
+                                        accumulation_segment=args.accumulation_segment)
             e_host.copy_(ee, non_blocking=True)
             for k in keys:
                 grads_host[k].copy_(gg[k], non_blocking=True)

@@ -71,18 +71,43 @@ struct F2Smem {
     static constexpr int SX = SB;
     static constexpr int SY = (SB == 8) ? 69 : SB * SB + 1;
     static constexpr int REG = SY * SB;
+    // W tile (y, x, z) at y*SYW + x*SX + z: 8-byte aligned rows for the
+    // 8-byte cp.async copies of the FP32 staging (SB = 8); item results keep SY
+    static constexpr int SYW = (SB == 8) ? 70 : SY;
+    static constexpr int REGW = SYW * SB;
     static constexpr int NV = 3 * SB;
     static constexpr int NVP = NV + 1;
     static constexpr int TAB = 6 * NV * NVP;
     static constexpr int ITEMS = SB * SB * SB;
     static constexpr int NT = (SB == 8) ? 256 : ITEMS;     // threads per CTA
     static constexpr int IPT = ITEMS / NT;                  // items per thread
-    static_assert(12 * REG <= 36 * REG, "item results overlay the W tile");
+    static_assert(12 * REG <= 36 * REGW, "item results overlay the W tile");
 };
 
 template <typename StageT, int SB>
 __host__ __device__ constexpr size_t f2_smem_bytes() {
-    return sizeof(StageT) * (36 * F2Smem<SB>::REG + 2 * F2Smem<SB>::TAB + 2 * 3 * F2Smem<SB>::NV);
+    return sizeof(StageT) * (36 * F2Smem<SB>::REGW + 2 * F2Smem<SB>::TAB + 2 * 3 * F2Smem<SB>::NV);
+}
+
+// 4- and 8-byte asynchronous copies global -> shared (L1-allocating, L2
+// evict-first hint: the staging is streamed once); src_bytes < size
+// zero-fills the rest of the destination without reading past src_bytes.
+__device__ __forceinline__ uint64_t f2_policy_evict_first() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ void f2_cp_async(void *smem_dst, const void *gsrc, int size, int src_bytes,
+                                            uint64_t pol) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
+    if (size == 8)
+        asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], 8, %2, %3;" ::"r"(d), "l"(gsrc),
+                     "r"(src_bytes), "l"(pol)
+                     : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], 4, %2, %3;" ::"r"(d), "l"(gsrc),
+                     "r"(src_bytes), "l"(pol)
+                     : "memory");
 }
 
 __host__ __device__ constexpr inline int pair_index(int sp, int sq) { return 2 * sp + (sq > sp ? sq - 1 : sq); }
@@ -252,11 +277,12 @@ __global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4)
     constexpr int NT = C::NT, IPT = C::IPT;
     constexpr int REG = C::REG, NV = C::NV, NVP = C::NVP;
     constexpr int SX = C::SX, SY = C::SY;
+    constexpr int REGW = C::REGW, SYW = C::SYW;
     constexpr int NW = NT / 32;
     extern __shared__ __align__(16) uint8_t f2_smem[];
     StageT *sW = reinterpret_cast<StageT *>(f2_smem);
     StageT *sG = sW;                      // item results [12][REG] (padded) once W is consumed
-    StageT *tOV = sW + 36 * REG;
+    StageT *tOV = sW + 36 * REGW;
     StageT *tT2 = tOV + C::TAB;
     StageT *tT1 = tT2 + C::TAB;
     StageT *tFV = tT1 + 3 * NV;
@@ -338,7 +364,30 @@ __global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4)
     //      LB runs are fetched before any is stored, so their latencies overlap ----
     // distinct sub-ranges: the tables need only the blocks of two different ranges
     const bool distinct_rng = (cs[1] == 1 && cs[2] == 2);
-    {
+    if constexpr (sizeof(StageT) == 4 && SB == 8) {
+        // FP32 staging: four lanes per 32-byte run, 8-byte cp.async (two 4-byte
+        // copies where the run is not 8-byte aligned), zero-filled past the run
+        const uint64_t pol = f2_policy_evict_first();
+        const int npiece = nreg * SB * SB * 4;
+        for (int e = tid; e < npiece; e += NT) {
+            const int run = e >> 2, c = e & 3;
+            const int reg = run / (SB * SB), yy = (run / SB) % SB, xx = run % SB;
+            const int *rd = s_rd[reg];
+            if (xx < rd[3] && yy < rd[4]) {
+                const int n = rd[5] - 2 * c;   // valid values of this 2-value piece (<= 0: none)
+                const StageT *run0 = P.S + s_gb[reg] + (long long)yy * s_gs[reg][0] + (long long)xx * s_gs[reg][1];
+                const StageT *src = n > 0 ? run0 + 2 * c : run0;   // nothing is read when n <= 0
+                StageT *dst = sW + reg * REGW + yy * SYW + xx * SX + 2 * c;
+                if (n >= 2 && (reinterpret_cast<uintptr_t>(src) & 7) == 0) {
+                    f2_cp_async(dst, src, 8, 8, pol);
+                } else {
+                    f2_cp_async(dst, src, 4, n >= 1 ? 4 : 0, pol);
+                    f2_cp_async(dst + 1, n >= 2 ? src + 1 : src, 4, n >= 2 ? 4 : 0, pol);
+                }
+            }
+        }
+        asm volatile("cp.async.wait_all;" ::: "memory");
+    } else {
         constexpr int LB = 3;
         const int nrun = nreg * SB * SB;
         for (int e0 = tid; e0 < nrun; e0 += LB * NT) {
@@ -357,7 +406,7 @@ __global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4)
                         lzs[u] = rd[5];
                         ld_run(b[u], P.S + s_gb[reg] + (long long)yy * s_gs[reg][0] + (long long)xx * s_gs[reg][1],
                                lzs[u]);
-                        dst[u] = sW + reg * REG + yy * SY + xx * SX;
+                        dst[u] = sW + reg * REGW + yy * SYW + xx * SX;
                     }
                 }
             }
@@ -447,7 +496,7 @@ __global__ void __launch_bounds__(F2Smem<SB>::NT, (SB == 8) ? 2 : 4)
                     int pp[3], pt[3];
                     perm_of(pi, pp);
                     perm_of(tau, pt);
-                    sw += (double)sW[pat.reg[pi * 6 + tau] * REG + loc[pp[1]] * SY + loc[pp[0]] * SX + loc[pp[2]]];
+                    sw += (double)sW[pat.reg[pi * 6 + tau] * REGW + loc[pp[1]] * SYW + loc[pp[0]] * SX + loc[pp[2]]];
                     const int pair = pair_index(pt[0], pt[1]);
                     const int xl = vl[pp[0]], yl = vl[pp[1]], zl = vl[pp[2]];
                     sv += tOV[(pair * NV + xl) * NVP + yl] * tT1[pt[2] * NV + zl] +

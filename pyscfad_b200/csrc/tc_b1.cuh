@@ -43,10 +43,13 @@ struct TcB1Params {
     double sign;
     int *err;
     int bf16;
-    int kseg;               // K blocks per accumulation segment (summed in FP64)
+    int kseg;               // K blocks per TMEM accumulation segment
 };
 
 constexpr int kB1Threads = 320;   // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
+// K segments summed in FP32 before the run goes into the FP64 gradient: runs of
+// K <= 512 * 64 keep the rounding of the sum well below the fp16 split error
+constexpr int kB1RunSegments = 512;
 
 template <bool A_MN, int BN>
 struct TcB1Cfg {
@@ -298,11 +301,46 @@ __global__ void __launch_bounds__(kB1Threads, 1)
             const PermBlock &pb = P.pb[tau];
             const int Tz = pb.Tz;
             const int nk = P.nk_outer[tau] * P.nk_inner[tau];
-            double accd[HC];
+            const double sc = BATCH ? P.sign / ((*P.wscale) * (*P.oscale)) : sc0;
+            long long roff = -1;
+            if (P.kind == 0 || P.kind == 2) {
+                const int p = mt * 8 + row / 16, x = row % 16;
+                if (p < o && x < pb.Tx) {
+                    if (P.kind == 0)
+                        roff = ((((long long)pb.Y0 + b) * o + p) * v + pb.X0 + x) * Kp;
+                    else
+                        roff = (((long long)b * o + p) * v + pb.X0 + x) * o;
+                }
+            } else {
+                const int rz = mt * 128 + row;
+                if (rz < o * Tz) {
+                    const int r = rz / Tz, z = rz % Tz;
+                    if (P.kind == 1)
+                        roff = (((long long)b * o + r) * v + pb.Z0 + z) * Kp;
+                    else
+                        roff = ((((long long)pb.Y0 + b) * o + r) * v + pb.Z0 + z) * o;
+                }
+            }
+            const int ncol = (P.kind <= 1) ? v : o;
+            const int c0 = nt * BN + half * HC;
+            float acc[HC];
 #pragma unroll
-            for (int j = 0; j < HC; j++) accd[j] = 0.0;
-            // segments in pairs: the two partials are added in FP32 (one rounding),
-            // then once into the FP64 sum
+            for (int j = 0; j < HC; j++) acc[j] = 0.f;
+            // G += sc * acc, then acc = 0: the FP64 sum of a run of at most
+            // kB1RunSegments FP32-summed segments
+            auto flush = [&]() {
+                if (roff >= 0) {
+#pragma unroll
+                    for (int j = 0; j < HC; j++) {
+                        const int col = c0 + j;
+                        if (col < ncol) atomicAdd(&P.G[roff + col], sc * (double)acc[j]);
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < HC; j++) acc[j] = 0.f;
+            };
+            // segments in pairs, added into the FP32 run sum; every kB1RunSegments
+            // segments the run goes into G in FP64
             const int nseg = (nk + P.kseg - 1) / P.kseg;
             for (int s0 = 0; s0 < nseg; s0 += 2, seg += 2) {
                 const bool two = s0 + 1 < nseg;
@@ -325,7 +363,7 @@ __global__ void __launch_bounds__(kB1Threads, 1)
 #pragma unroll
                     for (int j = 0; j < 8; j++) {
                         const float sum = two ? __uint_as_float(va[j]) + __uint_as_float(vb[j]) : __uint_as_float(va[j]);
-                        accd[c * 8 + j] += (double)sum;
+                        acc[c * 8 + j] += sum;
                     }
                 }
                 tc_fence_before();
@@ -335,37 +373,10 @@ __global__ void __launch_bounds__(kB1Threads, 1)
                     if (two) mbar_arrive(&tempty[accB]);
                 }
                 if (!two) seg -= 1;   // an odd tail used one accumulator
+                if ((s0 + 2) % kB1RunSegments == 0 && s0 + 2 < nseg) flush();
             }
             if (!ok) break;
-            const double sc = BATCH ? P.sign / ((*P.wscale) * (*P.oscale)) : sc0;
-            long long roff = -1;
-            if (P.kind == 0 || P.kind == 2) {
-                const int p = mt * 8 + row / 16, x = row % 16;
-                if (p < o && x < pb.Tx) {
-                    if (P.kind == 0)
-                        roff = ((((long long)pb.Y0 + b) * o + p) * v + pb.X0 + x) * Kp;
-                    else
-                        roff = (((long long)b * o + p) * v + pb.X0 + x) * o;
-                }
-            } else {
-                const int rz = mt * 128 + row;
-                if (rz < o * Tz) {
-                    const int r = rz / Tz, z = rz % Tz;
-                    if (P.kind == 1)
-                        roff = (((long long)b * o + r) * v + pb.Z0 + z) * Kp;
-                    else
-                        roff = ((((long long)pb.Y0 + b) * o + r) * v + pb.Z0 + z) * o;
-                }
-            }
-            const int ncol = (P.kind <= 1) ? v : o;
-            if (roff >= 0) {
-                const int c0 = nt * BN + half * HC;
-#pragma unroll
-                for (int j = 0; j < HC; j++) {
-                    const int col = c0 + j;
-                    if (col < ncol) atomicAdd(&P.G[roff + col], sc * accd[j]);
-                }
-            }
+            flush();
         }
     }
     tc_fence_before();

@@ -1,7 +1,8 @@
-// Chunk epilogue, common case: one occupied representative i > j > k and
-// three distinct, full 8-wide virtual sub-ranges (a work item).  Same math
-// and the same outputs as k_f2t (f2.cuh), which keeps every other case
-// (repeated occupied indices, coinciding or short sub-ranges, the FP64 mode):
+// Chunk epilogue, common case: one occupied representative i > j > k (or,
+// DEG, i = j > k / i > j = k) and three distinct, full 8-wide virtual
+// sub-ranges (a work item).  Same math and the same outputs as k_f2t (f2.cuh),
+// which keeps every other case (i = j = k, coinciding or short sub-ranges, the
+// FP64 mode):
 //
 //   WW(s) = sum_tau w(tau(ijk), tau(s abc)),  VV(s) likewise from v,
 //   X = WW + VV/2,  Z = r3(X),  E += 2 sum_s WW Z / D,
@@ -12,6 +13,12 @@
 // pairs (sub-range ordering pi, occupied ordering rho), region pi*6 + rho,
 // and each raw amplitude belongs to one orbit item and one ordering s, so
 // every index map is a compile-time constant once the (s, tau) loops unroll.
+// With two equal occupied indices (DEG) the occupied orderings rho and
+// rho' = (the swap of the two equal slots) o rho name the same raw amplitudes:
+// both regions are loaded (the same staging data twice), every sum over tau
+// is then the one of k_f2t, the orbit weight n_ijk n_abc / 18 is 1 instead of
+// 2, and the region of the smaller rho writes Wbar and the V-term gradients of
+// both orderings s(pi, rho) + s(pi, rho') while the other writes nothing.
 //
 // Persistent and software-pipelined: one CTA of 512 threads per SM walks the
 // work items w = blockIdx.x + k*grid.  The W tile of item k+1 (36 regions x
@@ -107,6 +114,13 @@ __device__ __forceinline__ void f2p_split8(const float (&w)[8], float scale, uin
 
 __device__ __forceinline__ int sel3(int a, int b, int c, int i) { return i == 0 ? a : (i == 1 ? b : c); }
 
+// f2p_sof(PI, rho) for a run-time rho, from compile-time constants
+template <int PI>
+__device__ __forceinline__ int f2p_sof_rt(int rho) {
+    return (rho == 0) ? f2p_sof(PI, 0) : (rho == 1) ? f2p_sof(PI, 1) : (rho == 2) ? f2p_sof(PI, 2)
+         : (rho == 3) ? f2p_sof(PI, 3) : (rho == 4) ? f2p_sof(PI, 4) : f2p_sof(PI, 5);
+}
+
 
 struct F2pSmem {
     using C = F2pTile;
@@ -171,12 +185,13 @@ __device__ __forceinline__ F2pRegion f2p_region_desc(const F2P<float> &P, int i0
 // rho): Wbar hi/lo out (16-byte halves of the 32-byte sectors whose other
 // half comes from the item with the other 8-wide half of this z block,
 // scheduled next to it), V-term gradients in (row sums per run, column sums
-// over the warp's 32 runs).
-template <int H, int PI>
+// over the warp's 32 runs).  DEG: the item results of ordering rho2 (the same
+// raw amplitudes) are added first.
+template <int H, int PI, bool DEG>
 __device__ __forceinline__ void f2p_run(const F2P<float> &P, const float2 *sG, const float2 *tOT,
                                         const float *tT1, const float *tFV, int i0, int i1, int i2,
-                                        int st0, int st1, int st2, int rho, int lane, int run, long long wbase, int ws0,
-                                        int ws1, long long half, float wscf) {
+                                        int st0, int st1, int st2, int rho, int rho2, int lane, int run,
+                                        long long wbase, int ws0, int ws1, long long half, float wscf) {
     using C = F2pTile;
     constexpr int pp0 = (PI >> 1), pp1 = (PI & 1) ? ((pp0 == 2) ? 1 : 2) : ((pp0 == 0) ? 1 : 0);
     constexpr int pp2 = 3 - pp0 - pp1;
@@ -185,8 +200,7 @@ __device__ __forceinline__ void f2p_run(const F2P<float> &P, const float2 *sG, c
     const int pt0 = rho >> 1;
     const int pt1 = (rho & 1) ? ((pt0 == 2) ? 1 : 2) : ((pt0 == 0) ? 1 : 0);
     const int pt2 = 3 - pt0 - pt1;
-    const int s = (rho == 0) ? f2p_sof(PI, 0) : (rho == 1) ? f2p_sof(PI, 1) : (rho == 2) ? f2p_sof(PI, 2)
-                : (rho == 3) ? f2p_sof(PI, 3) : (rho == 4) ? f2p_sof(PI, 4) : f2p_sof(PI, 5);
+    const int s = f2p_sof_rt<PI>(rho);
     const int p = sel3(i0, i1, i2, pt0), q = sel3(i0, i1, i2, pt1), r = sel3(i0, i1, i2, pt2);
     const int o = P.d.o, v = P.d.v;
     const int yy = run >> 3, xx = run & 7;
@@ -197,6 +211,15 @@ __device__ __forceinline__ void f2p_run(const F2P<float> &P, const float2 *sG, c
         const float2 gv = g[z * str[pp2]];
         wb[z] = gv.x;
         vb[z] = gv.y;
+    }
+    if constexpr (DEG) {
+        const float2 *g2 = sG + f2p_sof_rt<PI>(rho2) * C::PLANE + xx * str[pp0] + yy * str[pp1];
+#pragma unroll
+        for (int z = 0; z < 8; z++) {
+            const float2 gv = g2[z * str[pp2]];
+            wb[z] += gv.x;
+            vb[z] += gv.y;
+        }
     }
     uint4 hi, lo;
     f2p_split8<H>(wb, wscf, hi, lo);
@@ -229,10 +252,13 @@ __device__ __forceinline__ void f2p_run(const F2P<float> &P, const float2 *sG, c
     }
 }
 
-template <int H>   // 1: fp16 hi/lo, 2: bf16 hi/lo
+// H: 1 fp16 hi/lo, 2 bf16 hi/lo.  DEG: every work item has exactly two equal
+// occupied indices (i = j > k or i > j = k); otherwise all three are distinct.
+template <int H, bool DEG>
 __global__ void __launch_bounds__(F2pSmem::NT, 1)
     k_f2p(const __grid_constant__ F2P<float> P, int nitems) {
     using C = F2pTile;
+    constexpr double CF = DEG ? 1.0 : 2.0;   // orbit weight n_ijk n_abc / 18
     constexpr int NT = F2pSmem::NT, NW = F2pSmem::NW;
     extern __shared__ __align__(16) uint8_t f2p_smem[];
     float *sWb = reinterpret_cast<float *>(f2p_smem);   // W buffers [2][36 regions]
@@ -439,10 +465,10 @@ __global__ void __launch_bounds__(F2pSmem::NT, 1)
             double esum = 0.0;
 #pragma unroll
             for (int s = 0; s < 6; s++) esum += WW[s] * Z[s];
-            e_loc = 2.0 * esum * rD;   // orbit weight n_ijk n_abc / 18 = 2
+            e_loc = CF * esum * rD;
             if (P.want_grad) {
-                const double g0 = 2.0 * P.ybar * rD;
-                const double ddi = -2.0 * P.ybar * esum * rD * rD;
+                const double g0 = CF * P.ybar * rD;
+                const double ddi = -CF * P.ybar * esum * rD * rD;
 #pragma unroll
                 for (int s = 0; s < 6; s++)
                     gres[s] = make_float2((float)(g0 * (Z[s] + RW[s])), (float)(g0 * 0.5 * RW[s]));
@@ -529,10 +555,18 @@ __global__ void __launch_bounds__(F2pSmem::NT, 1)
         for (int hr = NW - 1 - warp; hr < 72; hr += NW) {
             const int reg = hr >> 1, part = hr & 1;
             const int pi = reg / 6, rho = reg % 6;
+            int rho2 = rho;
+            if constexpr (DEG) {
+                // the ordering with the two equal occupied slots swapped (perm 2
+                // swaps slots 0 and 1, perm 1 slots 1 and 2)
+                rho2 = perm_compose(ik == jk ? 2 : 1, rho);
+                if (rho2 < rho) continue;   // written by the region of rho2
+            }
             const int run = (part << 5) + lane;
             const F2pRegion &rg = s_reg[c][reg];
-#define F2P_RUN(PIV) \
-    f2p_run<H, PIV>(P, sG, tOT, tT1, tFV, ik, jk, kk, st0, st1, st2, rho, lane, run, rg.wb, rg.ws0, rg.ws1, rg.half, wscf)
+#define F2P_RUN(PIV)                                                                                                \
+    f2p_run<H, PIV, DEG>(P, sG, tOT, tT1, tFV, ik, jk, kk, st0, st1, st2, rho, rho2, lane, run, rg.wb, rg.ws0, rg.ws1, \
+                         rg.half, wscf)
             switch (pi) {
             case 0: F2P_RUN(0); break;
             case 1: F2P_RUN(1); break;

@@ -1124,8 +1124,10 @@ static int setup_epilogue() {
         TB_CUDA(cudaFuncSetAttribute(k_f2t<StageT, kSB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)f2_smem_bytes<StageT, kSB>()));
         if (sizeof(StageT) == 4) {
-            TB_CUDA(cudaFuncSetAttribute(k_f2p<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F2pSmem::BYTES));
-            TB_CUDA(cudaFuncSetAttribute(k_f2p<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F2pSmem::BYTES));
+            TB_CUDA(cudaFuncSetAttribute(k_f2p<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F2pSmem::BYTES));
+            TB_CUDA(cudaFuncSetAttribute(k_f2p<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F2pSmem::BYTES));
+            TB_CUDA(cudaFuncSetAttribute(k_f2p<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F2pSmem::BYTES));
+            TB_CUDA(cudaFuncSetAttribute(k_f2p<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F2pSmem::BYTES));
         }
         F2Pattern pats[kF2Patterns];
         f2_build_patterns(pats);
@@ -1532,9 +1534,11 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                 } else {
                     // F2: energy (+ adjoint of the raw amplitudes).  Sub-range
                     // triples of three distinct full 8-wide sub-ranges come first;
-                    // with the all-distinct occupied representatives (the first
-                    // n_distinct_ijk of the table) they go to the persistent kernel k_f2p
-                    // in the mixed modes, every other CTA to k_f2t.
+                    // in the mixed modes they go to the persistent kernel k_f2p with
+                    // the all-distinct occupied representatives (the first
+                    // n_distinct_ijk of the table) and, in a second launch, with the
+                    // representatives i = j > k and i > j = k that follow them; every
+                    // other item (i = j = k, the remaining sub-range triples) to k_f2t.
                     F2P<StageT> F;
                     const int n_simple_sub = f2_params<StageT>(P, ch, ws, io, F);
                     if (mixed && P.want_grad)
@@ -1542,6 +1546,7 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                                                                            ch.base[1], ch.nabc[1], ch.base[2], ch.nabc[2],
                                                                            io.ybar, bf16 ? 0 : 1, 0));
                     const int nd = mixed ? n_distinct_ijk(d.o) : 0;
+                    const int n2 = mixed ? d.o * (d.o - 1) : 0;   // i = j > k, then i > j = k
                     auto f2t = [&](int rep0, int nrep, int sub0, int nsub_l) -> int {
                         if (nrep <= 0 || nsub_l <= 0) return TRIPLES_OK;
                         F.rep0 = rep0;
@@ -1552,22 +1557,35 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                                              F, nullptr, nullptr, 0)));
                         return TRIPLES_OK;
                     };
-                    if (nd > 0 && n_simple_sub > 0) {
-                        F.rep0 = 0;
+                    // k_f2p over the representatives [rep0, rep0 + nrep) and the
+                    // leading n_simple_sub sub-range triples
+                    auto f2p = [&](int rep0, int nrep, bool deg) -> int {
+                        if (nrep <= 0 || n_simple_sub <= 0) return TRIPLES_OK;
+                        F.rep0 = rep0;
                         F.sub0 = 0;
                         F.nsub_l = n_simple_sub;
                         F2P<float> Ff;
                         std::memcpy(&Ff, &F, sizeof(F));   // StageT = float in the mixed modes
-                        const int nitems = nd * n_simple_sub;
+                        const int nitems = nrep * n_simple_sub;
                         const unsigned nb = (unsigned)(nitems < num_sms() ? nitems : num_sms());
-                        if (bf16)
-                            TB_KLAUNCH(P_F2, (k_f2p<2><<<nb, F2pSmem::NT, F2pSmem::BYTES, st>>>(Ff, nitems)));
-                        else
-                            TB_KLAUNCH(P_F2, (k_f2p<1><<<nb, F2pSmem::NT, F2pSmem::BYTES, st>>>(Ff, nitems)));
-                    }
+                        if (deg) {
+                            if (bf16)
+                                TB_KLAUNCH(P_F2, (k_f2p<2, true><<<nb, F2pSmem::NT, F2pSmem::BYTES, st>>>(Ff, nitems)));
+                            else
+                                TB_KLAUNCH(P_F2, (k_f2p<1, true><<<nb, F2pSmem::NT, F2pSmem::BYTES, st>>>(Ff, nitems)));
+                        } else {
+                            if (bf16)
+                                TB_KLAUNCH(P_F2, (k_f2p<2, false><<<nb, F2pSmem::NT, F2pSmem::BYTES, st>>>(Ff, nitems)));
+                            else
+                                TB_KLAUNCH(P_F2, (k_f2p<1, false><<<nb, F2pSmem::NT, F2pSmem::BYTES, st>>>(Ff, nitems)));
+                        }
+                        return TRIPLES_OK;
+                    };
                     int frc;
-                    if ((frc = f2t(0, nd, n_simple_sub, F.nsub - n_simple_sub)) != TRIPLES_OK) return frc;
-                    if ((frc = f2t(nd, P.n_ijk - nd, 0, F.nsub)) != TRIPLES_OK) return frc;
+                    if ((frc = f2p(0, nd, false)) != TRIPLES_OK) return frc;
+                    if ((frc = f2p(nd, n2, true)) != TRIPLES_OK) return frc;
+                    if ((frc = f2t(0, nd + n2, n_simple_sub, F.nsub - n_simple_sub)) != TRIPLES_OK) return frc;
+                    if ((frc = f2t(nd + n2, P.n_ijk - nd - n2, 0, F.nsub)) != TRIPLES_OK) return frc;
                     TB_KLAUNCH(P_F2, k_f2_energy_sum<<<1, 256, 0, st>>>(e_part, P.n_ijk * F.nsub, &ctrl->e_acc));
                 }
                 if (!P.want_grad) continue;

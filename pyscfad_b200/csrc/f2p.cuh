@@ -1,5 +1,5 @@
 // Chunk epilogue, common case: one occupied representative i > j > k (or,
-// DEG, i = j > k / i > j = k) and three distinct, full 8-wide virtual
+// DEG = 1 / 2, i = j > k / i > j = k) and three distinct, full 8-wide virtual
 // sub-ranges (a work item).  Same math and the same outputs as k_f2t (f2.cuh),
 // which keeps every other case (i = j = k, coinciding or short sub-ranges, the
 // FP64 mode):
@@ -15,10 +15,10 @@
 // every index map is a compile-time constant once the (s, tau) loops unroll.
 // With two equal occupied indices (DEG) the occupied orderings rho and
 // rho' = (the swap of the two equal slots) o rho name the same raw amplitudes:
-// both regions are loaded (the same staging data twice), every sum over tau
-// is then the one of k_f2t, the orbit weight n_ijk n_abc / 18 is 1 instead of
-// 2, and the region of the smaller rho writes Wbar and the V-term gradients of
-// both orderings s(pi, rho) + s(pi, rho') while the other writes nothing.
+// only the region of the smaller of the two is loaded (18 regions) and read
+// for both, so every sum over tau is the one of k_f2t; the orbit weight
+// n_ijk n_abc / 18 is 1 instead of 2; and that region writes Wbar and the
+// V-term gradients of both orderings, s(pi, rho) + s(pi, rho').
 //
 // Persistent and software-pipelined: one CTA of 512 threads per SM walks the
 // work items w = blockIdx.x + k*grid.  The W tile of item k+1 (36 regions x
@@ -114,6 +114,18 @@ __device__ __forceinline__ void f2p_split8(const float (&w)[8], float scale, uin
 
 __device__ __forceinline__ int sel3(int a, int b, int c, int i) { return i == 0 ? a : (i == 1 ? b : c); }
 
+// DEG = 1 (i = j): ordering 2 swaps the values 0 and 1 of an occupied
+// ordering; DEG = 2 (j = k): ordering 1 swaps 1 and 2.  The partner of rho
+// names the same occupied triple; the three rho below their partner are
+// {0, 1, 4} and {0, 2, 3}.
+__host__ __device__ constexpr int f2p_partner(int deg, int rho) { return perm_compose(deg == 1 ? 2 : 1, rho); }
+__host__ __device__ constexpr int f2p_lead(int deg, int rho) {
+    return f2p_partner(deg, rho) < rho ? f2p_partner(deg, rho) : rho;
+}
+__host__ __device__ constexpr int f2p_act(int deg, int k) { return k == 0 ? 0 : (deg == 1 ? (k == 1 ? 1 : 4) : (k == 1 ? 2 : 3)); }
+static_assert(f2p_partner(1, 0) == 2 && f2p_partner(1, 1) == 3 && f2p_partner(1, 4) == 5, "i = j partners");
+static_assert(f2p_partner(2, 0) == 1 && f2p_partner(2, 2) == 4 && f2p_partner(2, 3) == 5, "j = k partners");
+
 // f2p_sof(PI, rho) for a run-time rho, from compile-time constants
 template <int PI>
 __device__ __forceinline__ int f2p_sof_rt(int rho) {
@@ -187,7 +199,7 @@ __device__ __forceinline__ F2pRegion f2p_region_desc(const F2P<float> &P, int i0
 // scheduled next to it), V-term gradients in (row sums per run, column sums
 // over the warp's 32 runs).  DEG: the item results of ordering rho2 (the same
 // raw amplitudes) are added first.
-template <int H, int PI, bool DEG>
+template <int H, int PI, int DEG>
 __device__ __forceinline__ void f2p_run(const F2P<float> &P, const float2 *sG, const float2 *tOT,
                                         const float *tT1, const float *tFV, int i0, int i1, int i2,
                                         int st0, int st1, int st2, int rho, int rho2, int lane, int run,
@@ -212,7 +224,7 @@ __device__ __forceinline__ void f2p_run(const F2P<float> &P, const float2 *sG, c
         wb[z] = gv.x;
         vb[z] = gv.y;
     }
-    if constexpr (DEG) {
+    if constexpr (DEG != 0) {
         const float2 *g2 = sG + f2p_sof_rt<PI>(rho2) * C::PLANE + xx * str[pp0] + yy * str[pp1];
 #pragma unroll
         for (int z = 0; z < 8; z++) {
@@ -252,13 +264,14 @@ __device__ __forceinline__ void f2p_run(const F2P<float> &P, const float2 *sG, c
     }
 }
 
-// H: 1 fp16 hi/lo, 2 bf16 hi/lo.  DEG: every work item has exactly two equal
-// occupied indices (i = j > k or i > j = k); otherwise all three are distinct.
-template <int H, bool DEG>
+// H: 1 fp16 hi/lo, 2 bf16 hi/lo.  DEG 0: i > j > k; 1: i = j > k; 2: i > j = k
+// (every work item of a launch).
+template <int H, int DEG>
 __global__ void __launch_bounds__(F2pSmem::NT, 1)
     k_f2p(const __grid_constant__ F2P<float> P, int nitems) {
     using C = F2pTile;
     constexpr double CF = DEG ? 1.0 : 2.0;   // orbit weight n_ijk n_abc / 18
+    constexpr int NREG = DEG ? 18 : 36;      // distinct regions (loaded, written back)
     constexpr int NT = F2pSmem::NT, NW = F2pSmem::NW;
     extern __shared__ __align__(16) uint8_t f2p_smem[];
     float *sWb = reinterpret_cast<float *>(f2p_smem);   // W buffers [2][36 regions]
@@ -355,9 +368,10 @@ __global__ void __launch_bounds__(F2pSmem::NT, 1)
     auto issue_copies = [&](int b) {
         float *sW = sWb + b * F2pSmem::WTILE;
 #pragma unroll 2
-        for (int e = tid; e < 36 * 64 * 4; e += NT) {
+        for (int e = tid; e < NREG * 64 * 4; e += NT) {
             const int run = e >> 2, c = e & 3;
-            const int reg = run >> 6, yy = (run >> 3) & 7, xx = run & 7;
+            const int dreg = run >> 6, yy = (run >> 3) & 7, xx = run & 7;
+            const int reg = DEG ? (dreg / 3) * 6 + f2p_act(DEG, dreg % 3) : dreg;
             const float *src =
                 P.S + s_lgb[reg] + (long long)yy * s_lgs[reg][0] + (long long)xx * s_lgs[reg][1] + 2 * c;
             cp_async8(sW + reg * C::REG + yy * C::SY + xx * C::SX + 2 * c, src, pol);
@@ -443,7 +457,8 @@ __global__ void __launch_bounds__(F2pSmem::NT, 1)
                     int pp[3] = {0, 0, 0};
                     perm_of(pi, pp);
                     const int spair = pair_index(pp[0], pp[1]);
-                    const float w = sW[(pi * 6 + tau) * C::REG + woff[pi]];
+                    const int rw = DEG ? f2p_lead(DEG, tau) : tau;   // the loaded region of (pi, tau)
+                    const float w = sW[(pi * 6 + rw) * C::REG + woff[pi]];
                     const float2 ot = tOT[(pair * 6 + spair) * C::TBLK + toff[pi]];
                     WW[s] += (double)w;
                     VV[s] = fmaf(ot.x, t1r[pt[2]][pp[2]], fmaf(ot.y, fvr[pt[2]][pp[2]], VV[s]));
@@ -552,16 +567,11 @@ __global__ void __launch_bounds__(F2pSmem::NT, 1)
         //      did the set-up above, so they take the shorter share) ----
         const float2 *sG = reinterpret_cast<const float2 *>(sWb + c * F2pSmem::WTILE);
 #pragma unroll 1
-        for (int hr = NW - 1 - warp; hr < 72; hr += NW) {
-            const int reg = hr >> 1, part = hr & 1;
-            const int pi = reg / 6, rho = reg % 6;
-            int rho2 = rho;
-            if constexpr (DEG) {
-                // the ordering with the two equal occupied slots swapped (perm 2
-                // swaps slots 0 and 1, perm 1 slots 1 and 2)
-                rho2 = perm_compose(ik == jk ? 2 : 1, rho);
-                if (rho2 < rho) continue;   // written by the region of rho2
-            }
+        for (int hr = NW - 1 - warp; hr < 2 * NREG; hr += NW) {
+            const int dreg = hr >> 1, part = hr & 1;
+            const int pi = DEG ? dreg / 3 : dreg / 6, rho = DEG ? f2p_act(DEG, dreg % 3) : dreg % 6;
+            const int reg = pi * 6 + rho;
+            const int rho2 = DEG ? f2p_partner(DEG, rho) : rho;
             const int run = (part << 5) + lane;
             const F2pRegion &rg = s_reg[c][reg];
 #define F2P_RUN(PIV)                                                                                                \

@@ -1124,10 +1124,12 @@ static int setup_epilogue() {
         TB_CUDA(cudaFuncSetAttribute(k_f2t<StageT, kSB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)f2_smem_bytes<StageT, kSB>()));
         if (sizeof(StageT) == 4) {
-            TB_CUDA(cudaFuncSetAttribute(k_f2p<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F2pSmem::BYTES));
-            TB_CUDA(cudaFuncSetAttribute(k_f2p<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F2pSmem::BYTES));
-            TB_CUDA(cudaFuncSetAttribute(k_f2p<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F2pSmem::BYTES));
-            TB_CUDA(cudaFuncSetAttribute(k_f2p<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F2pSmem::BYTES));
+            TB_CUDA(cudaFuncSetAttribute(k_f2p<1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F2pSmem::BYTES));
+            TB_CUDA(cudaFuncSetAttribute(k_f2p<2, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F2pSmem::BYTES));
+            TB_CUDA(cudaFuncSetAttribute(k_f2p<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F2pSmem::BYTES));
+            TB_CUDA(cudaFuncSetAttribute(k_f2p<2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F2pSmem::BYTES));
+            TB_CUDA(cudaFuncSetAttribute(k_f2p<1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F2pSmem::BYTES));
+            TB_CUDA(cudaFuncSetAttribute(k_f2p<2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F2pSmem::BYTES));
         }
         F2Pattern pats[kF2Patterns];
         f2_build_patterns(pats);
@@ -1546,7 +1548,7 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                                                                            ch.base[1], ch.nabc[1], ch.base[2], ch.nabc[2],
                                                                            io.ybar, bf16 ? 0 : 1, 0));
                     const int nd = mixed ? n_distinct_ijk(d.o) : 0;
-                    const int n2 = mixed ? d.o * (d.o - 1) : 0;   // i = j > k, then i > j = k
+                    const int np = mixed ? d.o * (d.o - 1) / 2 : 0;   // i = j > k, then as many i > j = k
                     auto f2t = [&](int rep0, int nrep, int sub0, int nsub_l) -> int {
                         if (nrep <= 0 || nsub_l <= 0) return TRIPLES_OK;
                         F.rep0 = rep0;
@@ -1559,7 +1561,7 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                     };
                     // k_f2p over the representatives [rep0, rep0 + nrep) and the
                     // leading n_simple_sub sub-range triples
-                    auto f2p = [&](int rep0, int nrep, bool deg) -> int {
+                    auto f2p = [&](int rep0, int nrep, int deg) -> int {
                         if (nrep <= 0 || n_simple_sub <= 0) return TRIPLES_OK;
                         F.rep0 = rep0;
                         F.sub0 = 0;
@@ -1568,24 +1570,26 @@ static int run_impl(const Plan &P, cudaStream_t st, const TriplesIO &io) {
                         std::memcpy(&Ff, &F, sizeof(F));   // StageT = float in the mixed modes
                         const int nitems = nrep * n_simple_sub;
                         const unsigned nb = (unsigned)(nitems < num_sms() ? nitems : num_sms());
-                        if (deg) {
-                            if (bf16)
-                                TB_KLAUNCH(P_F2, (k_f2p<2, true><<<nb, F2pSmem::NT, F2pSmem::BYTES, st>>>(Ff, nitems)));
-                            else
-                                TB_KLAUNCH(P_F2, (k_f2p<1, true><<<nb, F2pSmem::NT, F2pSmem::BYTES, st>>>(Ff, nitems)));
+#define TB_F2P(HV, DV) TB_KLAUNCH(P_F2, (k_f2p<HV, DV><<<nb, F2pSmem::NT, F2pSmem::BYTES, st>>>(Ff, nitems)))
+                        if (deg == 1) {
+                            if (bf16) TB_F2P(2, 1);
+                            else TB_F2P(1, 1);
+                        } else if (deg == 2) {
+                            if (bf16) TB_F2P(2, 2);
+                            else TB_F2P(1, 2);
                         } else {
-                            if (bf16)
-                                TB_KLAUNCH(P_F2, (k_f2p<2, false><<<nb, F2pSmem::NT, F2pSmem::BYTES, st>>>(Ff, nitems)));
-                            else
-                                TB_KLAUNCH(P_F2, (k_f2p<1, false><<<nb, F2pSmem::NT, F2pSmem::BYTES, st>>>(Ff, nitems)));
+                            if (bf16) TB_F2P(2, 0);
+                            else TB_F2P(1, 0);
                         }
+#undef TB_F2P
                         return TRIPLES_OK;
                     };
                     int frc;
-                    if ((frc = f2p(0, nd, false)) != TRIPLES_OK) return frc;
-                    if ((frc = f2p(nd, n2, true)) != TRIPLES_OK) return frc;
-                    if ((frc = f2t(0, nd + n2, n_simple_sub, F.nsub - n_simple_sub)) != TRIPLES_OK) return frc;
-                    if ((frc = f2t(nd + n2, P.n_ijk - nd - n2, 0, F.nsub)) != TRIPLES_OK) return frc;
+                    if ((frc = f2p(0, nd, 0)) != TRIPLES_OK) return frc;
+                    if ((frc = f2p(nd, np, 1)) != TRIPLES_OK) return frc;
+                    if ((frc = f2p(nd + np, np, 2)) != TRIPLES_OK) return frc;
+                    if ((frc = f2t(0, nd + 2 * np, n_simple_sub, F.nsub - n_simple_sub)) != TRIPLES_OK) return frc;
+                    if ((frc = f2t(nd + 2 * np, P.n_ijk - nd - 2 * np, 0, F.nsub)) != TRIPLES_OK) return frc;
                     TB_KLAUNCH(P_F2, k_f2_energy_sum<<<1, 256, 0, st>>>(e_part, P.n_ijk * F.nsub, &ctrl->e_acc));
                 }
                 if (!P.want_grad) continue;

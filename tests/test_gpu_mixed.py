@@ -98,12 +98,13 @@ def test_mixed_odd_shapes_vs_oracle(o, v):
 
 
 @pytest.mark.parametrize("precision", ["mixed", "mixed_bf16"])
-@pytest.mark.parametrize("o,v,seed", [(10, 48, 51), (6, 64, 52)])
+@pytest.mark.parametrize("o,v,seed", [(10, 48, 51), (6, 64, 52), (3, 48, 53), (2, 40, 54)])
 def test_lean_epilogue_shapes_vs_fp64(precision, o, v, seed):
-    """Shapes where most epilogue blocks take the lean all-distinct kernel
-    (i > j > k, three distinct full 8-wide sub-ranges) and the rest the
+    """Shapes where most epilogue blocks take the persistent kernel (three
+    distinct full 8-wide sub-ranges; i > j > k, or i = j > k / i > j = k,
+    which dominate at nocc 3 and are all there is at nocc 2) and the rest the
     generic one: the mixed result against the FP64 path on the same inputs,
-    with its oracle check at the smaller shape."""
+    with its oracle check at the smaller shapes."""
     inp = make_inputs(o, v, 3 * (o + v), seed=seed, fvo_sigma=1e-3)
     e64, g64 = _run(inp, True, "fp64")
     e, g = _run(inp, True, precision)

@@ -339,9 +339,9 @@ __global__ void k_prep_B2(const double *__restrict__ t2, Dims d, double *__restr
 // 16-bit split operands for the tensor-core path
 // ---------------------------------------------------------------------------
 // Occupied representatives i >= j >= k: first the o(o-1)(o-2)/6 with
-// i > j > k (combinatorial order), then i == j > k, i > j == k and
-// i == j == k, so the epilogue can give the all-distinct ones their own
-// kernel with one contiguous range of blocks.
+// i > j > k (combinatorial order), then the o(o-1)/2 with i == j > k, as
+// many with i > j == k, and the o with i == j == k, so that each pattern the
+// persistent epilogue takes (the first three) is one contiguous range.
 __host__ __device__ inline int n_distinct_ijk(int o) { return o * (o - 1) * (o - 2) / 6; }
 
 __global__ void k_ijk_table(int o, int *ijk) {
@@ -1238,7 +1238,7 @@ static int f1_params(const Plan &P, const ChunkDesc &ch, char *ws, TcF1Params &T
 
 // Epilogue parameters of one chunk: every sub-range triple, those of three
 // distinct full 8-wide sub-ranges first (mixed precision; the persistent
-// kernel k_f2p takes them with the all-distinct occupied representatives).
+// kernel k_f2p takes them with every occupied representative but i == j == k).
 // Returns the number of those leading sub-range triples.
 template <typename StageT>
 static int f2_params(const Plan &P, const ChunkDesc &ch, char *ws, const TriplesIO &io, F2P<StageT> &F) {
